@@ -1,0 +1,461 @@
+#!/usr/bin/env python
+"""bench.py — per-format FP32 SpMV sweep on B200 (the reference's per-format
+benchmark, src/spmv_all.cpp:196-250, on synthetic matrices of the named
+shapes).
+
+One step = one y += A x launch of every format kernel on its matrix:
+
+  stencil27   3D 27-point stencil 128^3 (2,097,152 rows, 55,742,968 nnz):  DIA, BDIA
+  powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR-merge, CSR-vector,
+              CSR-scalar, COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32
+  blocks4x4   500,000 block rows x 8 dense 4x4 blocks (2,000,000 rows, 64M nnz):  BELL, SBELL, BCSR
+
+value = sum of useful flops (2 nnz per SpMV) / sum of kernel times, GFLOP/s.
+Kernel times are CUDA events on the launching stream; every matrix is larger
+than the 126 MB L2 and the formats run back to back, so no explicit flush.
+
+--impl reference: the reference's own serial csr_spmv (include/spmv_serial.h
+:198-217, compiled from its sources into oracle/_ref; the C restatement in
+oracle/ where that build is absent), single thread, on the same matrices.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMV GFLOP/s (per-format FP32 sweep)"
+UNIT = "GFLOP/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--small", action="store_true", help="scaled-down matrices (quick check)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--only", default="", help="comma list of format keys to run (debugging)")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Workload
+# ---------------------------------------------------------------------------
+def hyb_width(lengths: np.ndarray) -> int:
+    """ELL width of the ELL+COO split: the largest K such that at least a
+    third of the rows (and at least 4096) have K or more nonzeros."""
+    need = max(4096, len(lengths) // 3)
+    hist = np.bincount(lengths)
+    at_least = np.cumsum(hist[::-1])[::-1]
+    ks = np.nonzero(at_least >= need)[0]
+    return int(max(1, ks.max())) if ks.size else 1
+
+
+def split_hyb(coo_arrays, k):
+    """Rows' first k entries -> ELL part, the rest -> COO tail (both sorted)."""
+    h, w, r, c, v = coo_arrays
+    start = np.searchsorted(r, r, side="left")
+    pos = np.arange(r.size) - start
+    head = pos < k
+    return (h, w, r[head], c[head], v[head]), (h, w, r[~head], c[~head], v[~head])
+
+
+def build_workload(small: bool):
+    from clspmv_mic_b200 import formats as F
+    from clspmv_mic_b200 import synth
+
+    if small:
+        sten, pl, blk = synth.stencil_27pt(32), synth.powerlaw(1 << 15, maxlen=2000), synth.block_rows(8000, 8)
+    else:
+        sten, pl, blk = synth.stencil_27pt(128), synth.powerlaw(1 << 20), synth.block_rows(500_000, 8)
+    mats = {"stencil27": sten, "powerlaw": pl, "blocks4x4": blk}
+    items = []
+
+    def add(key, mat, host, kw=None, part_of=None):
+        h, w = mats[mat][0], mats[mat][1]
+        items.append(dict(key=key, matrix=mat, host=host, kw=kw or {}, rows=h, cols=w, nnz=int(host.nnz),
+                          stored=host.stored_bytes(), part_of=part_of))
+
+    coo = F.coo_matrix(*sten)
+    add("dia", "stencil27", F.coo2dia(coo))
+    add("bdia", "stencil27", F.coo2bdia(coo))
+    del coo
+
+    coo = F.coo_matrix(*pl)
+    csr = F.coo2csr(coo)
+    add("csr_merge", "powerlaw", csr, {"variant": "merge"})
+    add("csr_vector", "powerlaw", csr, {"variant": "vector"})
+    add("csr_scalar", "powerlaw", csr, {"variant": "scalar"})
+    add("coo", "powerlaw", coo)
+    lengths = np.diff(csr.array("csr_row_ptr"))
+    k = hyb_width(lengths)
+    ell_part, coo_tail = split_hyb(pl, k)
+    add("ell", "powerlaw", F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell")
+    add("ell_tail_coo", "powerlaw", F.coo_matrix(*coo_tail), part_of="ell")
+    add("sell32", "powerlaw", F.coo2sell(coo, 32))
+
+    coo = F.coo_matrix(*blk)
+    add("bell", "blocks4x4", F.coo2b4ell(coo, 4, 4))
+    add("sbell", "blocks4x4", F.coo2sbell(coo, 4, 4, 32))
+    add("bcsr", "blocks4x4", F.coo2b4csr(coo, 4, 4))
+    return mats, items, {"ell_width": k}
+
+
+def algorithmic_bytes(it) -> int:
+    """Arrays the kernel must stream (values, indices, pointers, padding),
+    plus x read once and y read and written once."""
+    return int(it["stored"] + 4 * it["cols"] + 8 * it["rows"])
+
+
+def format_flops(it) -> int:
+    return 2 * it["nnz"]
+
+
+# ---------------------------------------------------------------------------
+# Clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"clspmv_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes from committed ncu summaries
+    (profiles/ncu_traffic.txt: `<format key> <bytes per launch> ...`)."""
+    out = {}
+    p = ROOT / "profiles" / "ncu_traffic.txt"
+    if p.exists():
+        for line in p.read_text().splitlines():
+            t = line.split()
+            if len(t) >= 2 and not line.startswith("#"):
+                try:
+                    out[t[0]] = float(t[1])
+                except ValueError:
+                    pass
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's serial csr_spmv
+# ---------------------------------------------------------------------------
+def cpu_csr_seconds(mats, budget_s: float = 15.0):
+    """Best-of-k single-thread csr_spmv per matrix (compiled reference when
+    available). Returns (sum of best times, flops, kind, sample text)."""
+    from clspmv_mic_b200 import formats as F
+    from clspmv_mic_b200 import synth
+    from oracle import oracle as O
+    use_ref = O.ref() is not None
+    kind = "reference" if use_ref else "port"
+    total_t, total_f, desc = 0.0, 0, []
+    per = budget_s / len(mats)
+    for name, arrs in mats.items():
+        coo = F.coo_matrix(*arrs)
+        csr = F.coo2csr(coo)
+        x = synth.x_vector(arrs[1])
+        best, n, t_start = float("inf"), 0, time.perf_counter()
+        while n < 3 or (time.perf_counter() - t_start < per and n < 50):
+            y = np.zeros(arrs[0], np.float32)
+            t0 = time.perf_counter()
+            (O.spmv_ref if use_ref else O.spmv_port)(csr, x, y)
+            best = min(best, time.perf_counter() - t0)
+            n += 1
+        total_t += best
+        total_f += 2 * csr.nnz
+        desc.append(f"{name} best of {n}")
+    return total_t, total_f, kind, "csr_spmv on " + ", ".join(desc) + ", 1 thread"
+
+
+# ---------------------------------------------------------------------------
+# Arms
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from clspmv_mic_b200 import synth  # noqa: F401
+    mats = {}
+    if args.small:
+        from clspmv_mic_b200 import synth as S
+        mats = {"stencil27": S.stencil_27pt(32), "powerlaw": S.powerlaw(1 << 15, maxlen=2000),
+                "blocks4x4": S.block_rows(8000, 8)}
+    else:
+        from clspmv_mic_b200 import synth as S
+        mats = {"stencil27": S.stencil_27pt(128), "powerlaw": S.powerlaw(1 << 20), "blocks4x4": S.block_rows(500_000, 8)}
+    from clspmv_mic_b200 import formats as F
+    from oracle import oracle as O
+    use_ref = O.ref() is not None
+    fn = O.spmv_ref if use_ref else O.spmv_port
+    prepared = []
+    for name, arrs in mats.items():
+        csr = F.coo2csr(F.coo_matrix(*arrs))
+        prepared.append((csr, synth.x_vector(arrs[1]), arrs[0]))
+    flops = sum(2 * c.nnz for c, _, _ in prepared)
+
+    def step():
+        for csr, x, h in prepared:
+            fn(csr, x, np.zeros(h, np.float32))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = flops / dt / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "csr_spmv (the reference's serial CPU path) over stencil27 128^3, powerlaw 2^20, "
+                               "blocks4x4 500k x 8" + (" (small)" if args.small else ""), "parallelism": "1 thread"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference" if use_ref else "port",
+                         "sample": f"{args.steps} steps of csr_spmv over the three matrices"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    from clspmv_mic_b200 import formats as F
+    from clspmv_mic_b200 import synth
+
+    world, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mats, items, meta = build_workload(args.small)
+    if args.only:
+        keep = set(args.only.split(","))
+        items = [it for it in items if it["key"] in keep]
+
+    stream = torch.cuda.Stream(device=dev)
+    xs, ys = {}, {}
+    for name, arrs in mats.items():
+        xs[name] = torch.from_numpy(synth.x_vector(arrs[1])).to(dev)
+    for it in items:
+        it["dev"] = F.DeviceMatrix(it["host"], device=dev)
+        ys[it["key"]] = torch.zeros(it["rows"], dtype=torch.float32, device=dev)
+        if it["host"].fmt == "csr" and it["kw"].get("variant") == "merge":
+            it["dev"].merge_plan(stream)
+        it.pop("host")
+    torch.cuda.synchronize()
+
+    K = len(items)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(K + 1)] for _ in range(args.steps)]
+
+    def step(i=None):
+        with torch.cuda.stream(stream):
+            for j, it in enumerate(items):
+                if i is not None:
+                    ev[i][j].record(stream)
+                it["dev"].spmv(xs[it["matrix"]], ys[it["key"]], 1.0, 1.0, stream=stream, **it["kw"])
+            if i is not None:
+                ev[i][K].record(stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = F.launch_count()
+    t_all0 = torch.cuda.Event(enable_timing=True)
+    t_all1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_all0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    t_all1.record(stream)
+    torch.cuda.synchronize()
+    launches = F.launch_count() - launches0
+    total_ms = t_all0.elapsed_time(t_all1)
+    per_kernel_ms = np.array([[ev[i][j].elapsed_time(ev[i][j + 1]) for j in range(K)] for i in range(args.steps)])
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        torch.distributed.barrier()
+
+    # e2e through the public API with host buffers: per kernel, pinned x
+    # copied in and y read back on the same stream, inside the timed region.
+    h2d = d2h = 0
+    hx = {name: torch.from_numpy(synth.x_vector(a[1])).pin_memory() for name, a in mats.items()}
+    hy = {it["key"]: torch.zeros(it["rows"], dtype=torch.float32).pin_memory() for it in items}
+    dx = {it["key"]: torch.empty(it["cols"], dtype=torch.float32, device=dev) for it in items}
+    for it in items:
+        h2d += 4 * it["cols"]
+        d2h += 4 * it["rows"]
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for it in items:
+                dx[it["key"]].copy_(hx[it["matrix"]], non_blocking=True)
+                it["dev"].spmv(dx[it["key"]], ys[it["key"]], 1.0, 1.0, stream=stream, **it["kw"])
+                hy[it["key"]].copy_(ys[it["key"]], non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # the ELL part and its COO tail together carry the matrix's flops once
+    flops_step = sum(format_flops(it) for it in items if it["part_of"] is None) + \
+        sum(format_flops(it) for it in items if it["part_of"] == "ell")
+    ms_per_step = total_ms / args.steps
+    value = flops_step * world / (ms_per_step * 1e-3) / 1e9
+    e2e_value = flops_step * world / (e2e_ms * 1e-3) / 1e9
+
+    peak, peak_kind = hbm_peak()
+    med = np.median(per_kernel_ms, axis=0)
+    mean = per_kernel_ms.mean(axis=0)
+    formats = {}
+    for j, it in enumerate(items):
+        ab = algorithmic_bytes(it)
+        useful = 12 * it["nnz"] + 4 * it["cols"] + 8 * it["rows"]
+        formats[it["key"]] = {
+            "matrix": it["matrix"], "ms": round(float(med[j]), 5), "gflops": round(format_flops(it) / (med[j] * 1e-3) / 1e9, 2),
+            "gbs": round(ab / (med[j] * 1e-3) / 1e9, 1), "frac": round(ab / (med[j] * 1e-3) / 1e9 / peak, 3),
+            "alg_bytes": ab, "useful_bytes": useful, "nnz": it["nnz"], "rows": it["rows"],
+        }
+    dom = int(np.argmax(mean))
+    dom_it = items[dom]
+    ab = algorithmic_bytes(dom_it)
+    achieved = ab / (mean[dom] * 1e-3) / 1e9
+    traffic = ncu_traffic().get(dom_it["key"])
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {
+            "workload": "per-format FP32 sweep: stencil27 128^3 -> DIA,BDIA; powerlaw 2^20 Zipf(2.0) mean 16 "
+                        "-> CSR(merge,vector,scalar),COO,ELL(K)+COO tail,SELL-32; 4x4 blocks 500k x 8 -> "
+                        "BELL,SBELL,BCSR" + (" (SMALL)" if args.small else ""),
+            "global_batch": 1, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "l2": "no flush: every matrix exceeds the 126 MB L2 and the formats run back to back",
+            "ell_width": meta["ell_width"],
+        },
+        "roofline": {"bound": "hbm", "kernel": dom_it["key"], "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                     "traffic": traffic, "alg_bytes_per_launch": ab},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": round(e2e_ms, 4)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "formats": formats,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)
+        line["cpu_baseline"] = {"value": round(f_cpu / t_cpu / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

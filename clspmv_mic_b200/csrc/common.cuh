@@ -1,0 +1,225 @@
+// common.cuh — load/store helpers and argument blocks shared by the SpMV
+// tile functions (sm_100a only).
+//
+// Every format is written as a CTA-level tile function
+//     template <...> __device__ void <fmt>_tile(const <Fmt>Args&, int tile, char* smem)
+// for a fixed block of kBlock threads. A per-format __global__ wrapper runs
+// one tile per CTA; the fused Cocktail kernel maps CTA ranges to the tiles of
+// several formats, so all tile functions share the block size and take their
+// shared memory from the caller.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clspmv {
+
+constexpr int kBlock = 256;      // threads per CTA for every SpMV tile
+constexpr int kWarp = 32;
+
+// ---------------------------------------------------------------------------
+// Cache-policy loads. Matrix arrays are streamed once per SpMV: they are read
+// through the non-coherent path without L1 allocation and marked evict-first
+// in L2, so that x (reused by many rows) keeps its L2 lines. x is read with
+// an evict-last policy for the same reason.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ float4 ld_stream_f4(const float* p, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int4 ld_stream_i4(const int* p, uint64_t pol)
+{
+    int4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream_f(const float* p, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream_i(const int* p, uint64_t pol)
+{
+    int v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+// Loads for thread-per-row walks (CSR scalar / vector): consecutive loads
+// of one thread share sectors, so these keep the L1 allocation.
+__device__ __forceinline__ float ld_l1_f(const float* p, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_l1_i(const int* p, uint64_t pol)
+{
+    int v;
+    asm volatile("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ld_l1_f4(const float* p, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int4 ld_l1_i4(const int* p, uint64_t pol)
+{
+    int4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+// x gathers: read-only path, L1 allocation kept (neighbouring rows share
+// lines), evict-last in L2.
+__device__ __forceinline__ float ld_x(const float* p, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ld_x4(const float* p, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+
+// y update. ATOMIC is used when another CTA (or another Cocktail part) may
+// add to the same row; otherwise the row belongs to this thread alone.
+template <bool ATOMIC>
+__device__ __forceinline__ void y_update(float* y, long long row, float alpha, float beta, float acc)
+{
+    if (ATOMIC) {
+        atomicAdd(y + row, alpha * acc);
+    } else {
+        float old = beta == 0.0f ? 0.0f : beta * y[row];
+        y[row] = old + alpha * acc;
+    }
+}
+
+__device__ __forceinline__ float dot4(float4 a, float4 b, float acc)
+{
+    acc = fmaf(a.x, b.x, acc);
+    acc = fmaf(a.y, b.y, acc);
+    acc = fmaf(a.z, b.z, acc);
+    acc = fmaf(a.w, b.w, acc);
+    return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Argument blocks (device pointers + sizes), one per format.
+// ---------------------------------------------------------------------------
+struct DiaArgs {
+    int rows, cols, ndiag, len;       // len = dia_length_aligned (multiple of 4)
+    const int* offsets;
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct BdiaArgs {
+    int rows, cols, nband, len;
+    const int* offsets;               // first offset of each band
+    const int* bptr;                  // nband + 1
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct EllArgs {
+    int rows, ell_num, len;           // len = ell_height_aligned (multiple of 4)
+    const int* col;
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct SellArgs {
+    int rows, slice_height, nslice;
+    const int* slice_ptr;
+    const int* col;
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct CsrArgs {
+    int rows, nnz;
+    const int* row_ptr;
+    const int* col;
+    const float* val;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct CooArgs {
+    int nnz;
+    const int* row;
+    const int* col;
+    const float* val;
+    const float* x;
+    float* y;
+    float alpha;
+};
+
+struct B4ellArgs {
+    int rows, cols, nbrow, ellnum, len, f4;   // len = height_aligned, f4 = float4_aligned
+    const int* col;                           // float4 units
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct SbellArgs {
+    int rows, cols, nbrow, nslice, slice_height;
+    const int* slice_ptr;
+    const int* col;
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+struct B4csrArgs {
+    int rows, cols, nbrow, len;               // len = aligned_size
+    const int* row_ptr;
+    const int* col;
+    const float* data;
+    const float* x;
+    float* y;
+    float alpha, beta;
+};
+
+}  // namespace clspmv

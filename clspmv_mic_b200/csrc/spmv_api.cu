@@ -1,0 +1,383 @@
+// spmv_api.cu — extern "C" compute and residency entry points of
+// libclspmv_b200.so: argument checks, template dispatch, launches.
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include "clspmv_b200.h"
+#include "kernels.cuh"
+#include "api_internal.h"
+
+using namespace clspmv;
+
+namespace clspmv {
+
+static thread_local std::string g_last_cuda_error;
+static std::atomic<long long> g_launches{0};
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return CLSPMV_OK;
+    g_last_cuda_error = cudaGetErrorString(e);
+    return CLSPMV_ERR_CUDA;
+}
+
+int after_launch(int n)
+{
+    g_launches += n;
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace clspmv
+
+namespace {
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+inline cudaStream_t S(clspmv_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+inline unsigned grid_for(long long units, long long per_cta) { return (unsigned)((units + per_cta - 1) / per_cta); }
+
+// ---------------------------------------------------------------------------
+// __global__ wrappers: one tile per CTA.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_scale(float* y, int n, float beta)
+{
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < n) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
+}
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_dia(DiaArgs a)
+{
+    __shared__ __align__(16) char smem[kDiaSmemBytes];
+    dia_tile<A>(a, blockIdx.x, smem);
+}
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgs a)
+{
+    __shared__ __align__(16) char smem[kBdiaSmemBytes];
+    bdia_tile<A>(a, blockIdx.x, smem);
+}
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_ell(EllArgs a) { ell_tile<A>(a, blockIdx.x, nullptr); }
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_sell(SellArgs a) { sell_tile<A>(a, blockIdx.x, nullptr); }
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_sell_scalar(SellArgs a) { sell_tile_scalar<A>(a, blockIdx.x, nullptr); }
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_tile<A>(a, blockIdx.x, nullptr); }
+
+template <int T, bool A>
+__global__ void __launch_bounds__(kBlock) k_csr_vector(CsrArgs a) { csr_vector_tile<T, A>(a, blockIdx.x, nullptr); }
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_csr_merge(CsrArgs a, const int* __restrict__ tc)
+{
+    extern __shared__ __align__(16) char dsmem[];
+    csr_merge_tile<A>(a, tc, blockIdx.x, dsmem);
+}
+
+__global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, const int* __restrict__ row_ptr, int* tc, int ntiles)
+{
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t > ntiles) return;
+    csr_merge_search(rows, nnz, row_ptr, (long long)t * kMergeTile, tc + 2 * t);
+}
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_coo(CooArgs a) { coo_tile<A>(a, blockIdx.x, nullptr); }
+
+template <int BW4, int BH, bool A>
+__global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgs a) { b4ell_tile<BW4, BH, A>(a, blockIdx.x, nullptr); }
+
+template <int BW4, int BH, bool A>
+__global__ void __launch_bounds__(kBlock) k_sbell(SbellArgs a) { sbell_tile<BW4, BH, A>(a, blockIdx.x, nullptr); }
+
+template <int BW4, int BH, int T, bool A>
+__global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgs a) { b4csr_tile<BW4, BH, T, A>(a, blockIdx.x, nullptr); }
+
+// ---------------------------------------------------------------------------
+// Shape dispatch helpers.
+// ---------------------------------------------------------------------------
+template <int V> using ic = std::integral_constant<int, V>;
+
+// Calls f(ic<bwidth/4>, ic<bheight>) for the 8 block shapes of the
+// reference ({1,2,4,8} x {4,8}, include/matrix_storage.h:241).
+template <class F>
+int dispatch_block(unsigned bw, unsigned bh, F&& f)
+{
+    if (bw == 4) {
+        switch (bh) {
+            case 1: return f(ic<1>{}, ic<1>{});
+            case 2: return f(ic<1>{}, ic<2>{});
+            case 4: return f(ic<1>{}, ic<4>{});
+            case 8: return f(ic<1>{}, ic<8>{});
+        }
+    } else if (bw == 8) {
+        switch (bh) {
+            case 1: return f(ic<2>{}, ic<1>{});
+            case 2: return f(ic<2>{}, ic<2>{});
+            case 4: return f(ic<2>{}, ic<4>{});
+            case 8: return f(ic<2>{}, ic<8>{});
+        }
+    }
+    return CLSPMV_ERR_UNSUPPORTED;
+}
+
+// Calls f(ic<T>) for T in {1, 2, 4, 8, 16, 32}.
+template <class F>
+int dispatch_lanes(int t, F&& f)
+{
+    switch (t) {
+        case 1: return f(ic<1>{});
+        case 2: return f(ic<2>{});
+        case 4: return f(ic<4>{});
+        case 8: return f(ic<8>{});
+        case 16: return f(ic<16>{});
+        case 32: return f(ic<32>{});
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int pow2_lanes(double mean, int lo, int hi)
+{
+    int t = lo;
+    while (t < hi && t < mean) t <<= 1;
+    return t;
+}
+
+int prescale(float* y, int n, float beta, cudaStream_t st)
+{
+    if (beta == 1.0f || n == 0) return CLSPMV_OK;
+    k_scale<<<grid_for(n, kBlock), kBlock, 0, st>>>(y, n, beta);
+    return after_launch(1);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Compute entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* clspmv_version(void) { return "clspmv_b200 0.1 sm_100a"; }
+
+const char* clspmv_status_string(int s)
+{
+    switch (s) {
+        case CLSPMV_OK: return "ok";
+        case CLSPMV_ERR_ARG: return "invalid argument";
+        case CLSPMV_ERR_ALLOC: return "allocation failed";
+        case CLSPMV_ERR_UNSUPPORTED: return "unsupported shape";
+        case CLSPMV_ERR_CUDA: return "CUDA error";
+        case CLSPMV_ERR_REFUSED: return "refused by the format's size rule";
+        case CLSPMV_ERR_ALIGN: return "misaligned pointer or length";
+        case CLSPMV_ERR_NOT_SORTED: return "COO input is not sorted by (row, col)";
+        case CLSPMV_ERR_TIMEOUT: return "bounded device wait timed out";
+    }
+    return "unknown status";
+}
+
+const char* clspmv_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
+
+long long clspmv_launch_count(void) { return g_launches.load(); }
+
+int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->dia_num > 0 && (!m->dia_offsets || !m->dia_data)) return CLSPMV_ERR_ARG;
+    if ((m->dia_length_aligned & 3) || !aligned16(m->dia_data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
+    DiaArgs a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, m->dia_data, x, y, alpha, beta};
+    k_dia<false><<<grid_for(rows, kDiaRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    return after_launch(1);
+}
+
+int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data)) return CLSPMV_ERR_ARG;
+    if ((m->bdia_length_aligned & 3) || !aligned16(m->bdia_data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
+    BdiaArgs a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, m->bdia_data, x, y, alpha, beta};
+    k_bdia<false><<<grid_for(rows, kBdiaRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    return after_launch(1);
+}
+
+int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->ell_num > 0 && (!m->ell_col_id || !m->ell_data)) return CLSPMV_ERR_ARG;
+    if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned16(m->ell_data) || rows > m->ell_height_aligned)
+        return CLSPMV_ERR_ALIGN;
+    EllArgs a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, m->ell_data, x, y, alpha, beta};
+    k_ell<false><<<grid_for(rows, kEllRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    return after_launch(1);
+}
+
+int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y || !m->sell_slice_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    const int sh = (int)m->sell_slice_height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
+    SellArgs a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data, x, y, alpha, beta};
+    if ((sh & 3) == 0 && aligned16(m->sell_col_id) && aligned16(m->sell_data)) {
+        const long long quads = (long long)m->sell_slice_num * (sh / 4);
+        k_sell<false><<<grid_for(quads, kBlock), kBlock, 0, S(stream)>>>(a);
+    } else {
+        k_sell_scalar<false><<<grid_for(rows, kBlock), kBlock, 0, S(stream)>>>(a);
+    }
+    return after_launch(1);
+}
+
+int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
+    k_csr_scalar<false><<<grid_for(rows, kBlock), kBlock, 0, S(stream)>>>(a);
+    return after_launch(1);
+}
+
+int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, clspmv_stream_t stream)
+{
+    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
+    if (tpr == 0) tpr = pow2_lanes((double)m->matinfo.nnz / rows, 2, 32);
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
+    const unsigned grid = grid_for((long long)rows * tpr, kBlock);
+    cudaStream_t st = S(stream);
+    return dispatch_lanes(tpr, [&](auto t) {
+        k_csr_vector<decltype(t)::value, false><<<grid, kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int clspmv_csr_merge_tiles(int rows, int nnz)
+{
+    if (rows < 0 || nnz < 0) return -1;
+    return (int)(((long long)rows + nnz + kMergeTile - 1) / kMergeTile);
+}
+
+int clspmv_csr_merge_plan(const clspmv_csr_f32* m, int* tc, clspmv_stream_t stream)
+{
+    if (!m || !tc || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int ntiles = clspmv_csr_merge_tiles(m->matinfo.height, m->matinfo.nnz);
+    if (ntiles < 0) return CLSPMV_ERR_ARG;
+    k_csr_merge_plan<<<grid_for((long long)ntiles + 1, kBlock), kBlock, 0, S(stream)>>>(
+        m->matinfo.height, m->matinfo.nnz, m->csr_row_ptr, tc, ntiles);
+    return after_launch(1);
+}
+
+int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !tc || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    cudaStream_t st = S(stream);
+    int rc = prescale(y, rows, beta, st);
+    if (rc) return rc;
+    const int ntiles = clspmv_csr_merge_tiles(rows, m->matinfo.nnz);
+    static bool attr_set = false;
+    if (!attr_set) {
+        rc = cuda_status(cudaFuncSetAttribute(k_csr_merge<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMergeSmemBytes));
+        if (rc) return rc;
+        attr_set = true;
+    }
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, 1.0f};
+    k_csr_merge<false><<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
+    return after_launch(1);
+}
+
+int clspmv_coo_spmv_f32(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    cudaStream_t st = S(stream);
+    int rc = prescale(y, rows, beta, st);
+    if (rc) return rc;
+    if (m->matinfo.nnz <= 0) return CLSPMV_OK;
+    if (!m->coo_row_id || !m->coo_col_id || !m->coo_data) return CLSPMV_ERR_ARG;
+    CooArgs a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, m->coo_data, x, y, alpha};
+    k_coo<false><<<grid_for(m->matinfo.nnz, kCooTileNnz), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+}  // extern "C"
+
+
+extern "C" {
+
+int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->b4ell_row_num <= 0) return CLSPMV_OK;
+    if (!m->b4ell_col_id || !m->b4ell_data) return CLSPMV_ERR_ARG;
+    if ((m->b4ell_float4_aligned & 3) || !aligned16(m->b4ell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->b4ell_row_num * m->b4ell_bheight < rows || m->b4ell_float4_aligned < 4 * m->b4ell_row_num) return CLSPMV_ERR_ARG;
+    const B4ellArgs a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
+                      m->b4ell_float4_aligned, m->b4ell_col_id, m->b4ell_data, x, y, alpha, beta};
+    cudaStream_t st = S(stream);
+    return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
+        k_b4ell<decltype(bw4)::value, decltype(bh)::value, false><<<grid_for(a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->sbell_row_num <= 0) return CLSPMV_OK;
+    if (!m->sbell_slice_ptr || !m->sbell_col_id || !m->sbell_data || m->sbell_slice_height == 0) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->sbell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
+    const SbellArgs a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
+                      m->sbell_slice_ptr, m->sbell_col_id, m->sbell_data, x, y, alpha, beta};
+    cudaStream_t st = S(stream);
+    return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
+        k_sbell<decltype(bw4)::value, decltype(bh)::value, false><<<grid_for(a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->b4csr_row_num <= 0) return CLSPMV_OK;
+    if (!m->b4csr_row_ptr || !m->b4csr_col_id || !m->b4csr_data) return CLSPMV_ERR_ARG;
+    if ((m->b4csr_aligned_size & 3) || !aligned16(m->b4csr_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->b4csr_row_num * m->b4csr_bheight < rows) return CLSPMV_ERR_ARG;
+    const B4csrArgs a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
+                      m->b4csr_row_ptr, m->b4csr_col_id, m->b4csr_data, x, y, alpha, beta};
+    cudaStream_t st = S(stream);
+    const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num, 1, 32);
+    return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
+        return dispatch_lanes(lanes, [&](auto t) {
+            constexpr int T = decltype(t)::value;
+            k_b4csr<decltype(bw4)::value, decltype(bh)::value, T, false>
+                <<<grid_for((long long)a.nbrow * T, kBlock), kBlock, 0, st>>>(a);
+            return after_launch(1);
+        });
+    });
+}
+
+}  // extern "C"

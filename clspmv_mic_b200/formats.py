@@ -1,0 +1,276 @@
+"""Host and device matrices in the reference's storage formats.
+
+The converters are the library's own C++ (include/matrix_storage.h of this
+repository), reached through the C ABI; their names follow the reference
+(coo2csr, coo2dia, ... of include/matrix_storage.h in clSpMV), and they
+return HostMatrix objects whose numpy arrays are views of the library-owned
+buffers. DeviceMatrix copies a HostMatrix into device memory (torch tensors,
+used purely as allocations) and runs the CUDA SpMV through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import FORMATS, check, lib
+
+GPU_ALIGNMENT = 32       # include/constant.h:17 of the reference
+SELL_GROUP_SIZE = 128    # include/constant.h:42
+WARPSIZE = 32            # include/constant.h:21
+BLOCK_SHAPES = [(bh, bw) for bw in (4, 8) for bh in (1, 2, 4, 8)]   # src/spmv_bell.cpp:362-363 order
+
+
+class HostMatrix:
+    """A format struct whose arrays live in host memory.
+
+    `owner` is "lib" when the arrays were malloc'ed by the library (released
+    with clspmv_free_<fmt>_f32), otherwise the numpy arrays are kept alive
+    here."""
+
+    def __init__(self, fmt: str, struct, keep=None, lib_owned: bool = False):
+        self.fmt = fmt
+        self.struct = struct
+        self._keep = keep
+        self._lib_owned = lib_owned
+
+    def __del__(self):
+        if getattr(self, "_lib_owned", False):
+            try:
+                getattr(lib(), f"clspmv_free_{self.fmt}_f32")(C.byref(self.struct))
+            except Exception:
+                pass
+            self._lib_owned = False
+
+    # -- views -------------------------------------------------------------
+    def array(self, field: str) -> np.ndarray:
+        for f, dt, n in FORMATS[self.fmt][1]:
+            if f == field:
+                count = int(n(self.struct))
+                ptr = getattr(self.struct, field)
+                if count <= 0 or not ptr:
+                    return np.zeros(0, dtype=dt)
+                ctype = C.c_int if dt == np.int32 else C.c_float
+                return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count,))
+        raise KeyError(field)
+
+    def arrays(self) -> dict:
+        return {f: self.array(f) for f, _, _ in FORMATS[self.fmt][1]}
+
+    def scalars(self) -> dict:
+        out = {}
+        for name, _ in self.struct._fields_:
+            if name == "matinfo":
+                mi = self.struct.matinfo
+                out.update(width=mi.width, height=mi.height, nnz=mi.nnz)
+            elif not any(name == f for f, _, _ in FORMATS[self.fmt][1]):
+                out[name] = int(getattr(self.struct, name))
+        return out
+
+    @property
+    def shape(self):
+        return (self.struct.matinfo.height, self.struct.matinfo.width)
+
+    @property
+    def nnz(self) -> int:
+        return self.struct.matinfo.nnz
+
+    def stored_bytes(self) -> int:
+        return int(sum(a.nbytes for a in self.arrays().values()))
+
+    def copy(self) -> "HostMatrix":
+        """Deep copy into numpy-owned arrays."""
+        arrays = {k: np.array(v, copy=True) for k, v in self.arrays().items()}
+        return from_arrays(self.fmt, self.scalars(), arrays)
+
+
+def from_arrays(fmt: str, scalars: dict, arrays: dict) -> HostMatrix:
+    """Builds a HostMatrix whose struct points at the given numpy arrays."""
+    struct_t, spec = FORMATS[fmt]
+    s = struct_t()
+    keep = {}
+    s.matinfo.width = int(scalars.get("width", 0))
+    s.matinfo.height = int(scalars.get("height", 0))
+    s.matinfo.nnz = int(scalars.get("nnz", 0))
+    for name, _ in struct_t._fields_:
+        if name in scalars and name not in ("width", "height", "nnz"):
+            setattr(s, name, int(scalars[name]))
+    for field, dt, _ in spec:
+        a = np.ascontiguousarray(arrays[field], dtype=dt)
+        if a.size == 0:
+            a = np.zeros(4, dtype=dt)   # non-null pointer for empty arrays
+        keep[field] = a
+        setattr(s, field, a.ctypes.data)
+    return HostMatrix(fmt, s, keep=keep)
+
+
+def coo_matrix(height: int, width: int, row_id, col_id, data) -> HostMatrix:
+    """COO matrix (coo_matrix<int,float>, include/matrix_storage.h:141-152)."""
+    row_id = np.ascontiguousarray(row_id, dtype=np.int32)
+    col_id = np.ascontiguousarray(col_id, dtype=np.int32)
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    if not (row_id.shape == col_id.shape == data.shape):
+        raise ValueError("row_id, col_id and data must have the same length")
+    return from_arrays("coo", dict(width=width, height=height, nnz=row_id.size),
+                       dict(coo_row_id=row_id, coo_col_id=col_id, coo_data=data))
+
+
+# ---------------------------------------------------------------------------
+# Converters (names as in the reference's matrix_storage.h)
+# ---------------------------------------------------------------------------
+def if_sorted_coo(coo: HostMatrix) -> bool:
+    return bool(lib().clspmv_is_sorted_coo_f32(C.byref(coo.struct)))
+
+
+def sort_coo(coo: HostMatrix) -> HostMatrix:
+    check(lib().clspmv_sort_coo_f32(C.byref(coo.struct)), "sort_coo")
+    return coo
+
+
+def _convert(fmt: str, cname: str, coo: HostMatrix, *args) -> HostMatrix:
+    out = FORMATS[fmt][0]()
+    status = getattr(lib(), cname)(C.byref(coo.struct), C.byref(out), *args)
+    m = HostMatrix(fmt, out, lib_owned=(status == _abi.OK))
+    check(status, cname)
+    return m
+
+
+def coo2csr(coo):
+    return _convert("csr", "clspmv_coo2csr_f32", coo)
+
+
+def coo2dia(coo, alignment=GPU_ALIGNMENT):
+    return _convert("dia", "clspmv_coo2dia_f32", coo, alignment)
+
+
+def coo2bdia(coo, alignment=GPU_ALIGNMENT):
+    return _convert("bdia", "clspmv_coo2bdia_f32", coo, alignment)
+
+
+def coo2ell(coo, alignment=GPU_ALIGNMENT, ellnum=0):
+    return _convert("ell", "clspmv_coo2ell_f32", coo, alignment, ellnum)
+
+
+def coo2sell(coo, slice_height=WARPSIZE):
+    return _convert("sell", "clspmv_coo2sell_f32", coo, slice_height)
+
+
+def coo2bcsr(coo, bwidth, bheight, alignment=GPU_ALIGNMENT):
+    return _convert("bcsr", "clspmv_coo2bcsr_f32", coo, bwidth, bheight, alignment)
+
+
+def coo2b4csr(coo, bwidth, bheight, alignment=GPU_ALIGNMENT):
+    return _convert("b4csr", "clspmv_coo2b4csr_f32", coo, bwidth, bheight, alignment)
+
+
+def coo2bell(coo, bwidth, bheight, alignment=GPU_ALIGNMENT, ellnum=0):
+    return _convert("bell", "clspmv_coo2bell_f32", coo, bwidth, bheight, alignment, ellnum)
+
+
+def coo2b4ell(coo, bwidth, bheight, alignment=GPU_ALIGNMENT, ellnum=0):
+    return _convert("b4ell", "clspmv_coo2b4ell_f32", coo, bwidth, bheight, alignment, ellnum)
+
+
+def coo2sbell(coo, bwidth, bheight, slice_height=WARPSIZE):
+    return _convert("sbell", "clspmv_coo2sbell_f32", coo, bwidth, bheight, slice_height)
+
+
+def pad_csr(csr: HostMatrix, alignment: int) -> HostMatrix:
+    out = FORMATS["csr"][0]()
+    status = lib().clspmv_pad_csr_f32(C.byref(csr.struct), C.byref(out), alignment)
+    m = HostMatrix("csr", out, lib_owned=(status == _abi.OK))
+    check(status, "pad_csr")
+    return m
+
+
+def to_coo(m: HostMatrix) -> HostMatrix:
+    """Inverse conversion <fmt>2coo (row-sorted output)."""
+    out = FORMATS["coo"][0]()
+    status = getattr(lib(), f"clspmv_{m.fmt}2coo_f32")(C.byref(m.struct), C.byref(out))
+    res = HostMatrix("coo", out, lib_owned=(status == _abi.OK))
+    check(status, f"{m.fmt}2coo")
+    return res
+
+
+# ---------------------------------------------------------------------------
+# Device residency and SpMV
+# ---------------------------------------------------------------------------
+_SPMV = {
+    "coo": "clspmv_coo_spmv_f32",
+    "dia": "clspmv_dia_spmv_f32",
+    "bdia": "clspmv_bdia_spmv_f32",
+    "ell": "clspmv_ell_spmv_f32",
+    "sell": "clspmv_sell_spmv_f32",
+    "b4ell": "clspmv_b4ell_spmv_f32",
+    "sbell": "clspmv_sbell_spmv_f32",
+    "b4csr": "clspmv_b4csr_spmv_f32",
+}
+CSR_VARIANTS = ("merge", "vector", "scalar")
+
+
+def _stream_handle(stream) -> Optional[int]:
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+class DeviceMatrix:
+    """A format struct whose arrays are device copies (torch allocations)."""
+
+    def __init__(self, host: HostMatrix, device="cuda"):
+        import torch
+        if host.fmt in ("bcsr", "bell"):
+            raise ValueError(f"{host.fmt} is a host-only format; use b4csr / b4ell on the device")
+        self.fmt = host.fmt
+        self.struct = type(host.struct).from_buffer_copy(host.struct)
+        self.tensors = {}
+        for field, arr in host.arrays().items():
+            if arr.size:
+                t = torch.from_numpy(arr).to(device)   # host view -> one device copy
+            else:
+                t = torch.zeros(4, dtype=torch.float32 if arr.dtype == np.float32 else torch.int32, device=device)
+            self.tensors[field] = t
+            setattr(self.struct, field, t.data_ptr())
+        self.shape = host.shape
+        self.nnz = host.nnz
+        self.stored_bytes = host.stored_bytes()
+        self._plan = None
+
+    def merge_plan(self, stream=None):
+        """Tile coordinates for the merge-path CSR kernel (computed once)."""
+        import torch
+        if self._plan is None:
+            ntiles = lib().clspmv_csr_merge_tiles(self.shape[0], self.nnz)
+            plan = torch.empty(2 * (ntiles + 1), dtype=torch.int32, device=self.tensors["csr_row_ptr"].device)
+            check(lib().clspmv_csr_merge_plan(C.byref(self.struct), plan.data_ptr(), _stream_handle(stream)), "csr_merge_plan")
+            self._plan = plan
+        return self._plan
+
+    def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None, variant: str = "merge",
+             threads_per_row: int = 0) -> None:
+        """y <- alpha * A x + beta * y on the device (asynchronous on `stream`)."""
+        L = lib()
+        s = _stream_handle(stream)
+        if self.fmt == "csr":
+            if variant == "merge":
+                plan = self.merge_plan(stream)
+                check(L.clspmv_csr_merge_spmv_f32(C.byref(self.struct), plan.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                                  alpha, beta, s), "csr_merge_spmv")
+            elif variant == "vector":
+                check(L.clspmv_csr_vector_spmv_f32(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta,
+                                                   threads_per_row, s), "csr_vector_spmv")
+            elif variant == "scalar":
+                check(L.clspmv_csr_scalar_spmv_f32(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s),
+                      "csr_scalar_spmv")
+            else:
+                raise ValueError(variant)
+            return
+        name = _SPMV[self.fmt]
+        check(getattr(L, name)(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s), name)
+
+
+def launch_count() -> int:
+    return int(lib().clspmv_launch_count())

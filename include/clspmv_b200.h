@@ -1,0 +1,331 @@
+/*
+ * clspmv_b200.h — C ABI of the B200 SpMV library (libclspmv_b200.so).
+ *
+ * Plain C: no CUDA or torch types appear here. Device pointers are plain
+ * pointers, streams are passed as `clspmv_stream_t` (a cudaStream_t cast to
+ * void*; NULL means the legacy default stream).
+ *
+ * Semantics of every SpMV entry point: y <- alpha * A * x + beta * y, FP32
+ * values, int32 indices. The reference clSpMV kernels all compute
+ * y <- A*x + y (they read `result` before accumulating, e.g.
+ * kernels/spmv_ell.cl:7, kernels/spmv_coo.cl:43), which is alpha = beta = 1.
+ * beta == 0 never reads y (BLAS convention).
+ *
+ * The format structs below are layout-identical to the reference's C++
+ * templates instantiated with dimType = offsetType = int, dataType = float
+ * (include/matrix_storage.h:15-365 of clSpMV), so a `coo_matrix<int,float>*`
+ * may be passed where a `clspmv_coo_f32*` is expected. The same struct type is
+ * used for host copies (converter outputs) and device copies (upload outputs):
+ * only where the pointers point differs.
+ *
+ * Every function returns a clspmv_status (0 = success) and never exits the
+ * process; the reference instead calls exit(1) from CHECKERROR
+ * (include/oclcommon.h:11).
+ */
+#ifndef CLSPMV_B200_H
+#define CLSPMV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* clspmv_stream_t;
+
+typedef enum {
+    CLSPMV_OK = 0,
+    CLSPMV_ERR_ARG = 1,         /* null pointer, negative size, bad shape     */
+    CLSPMV_ERR_ALLOC = 2,       /* host or device allocation failed           */
+    CLSPMV_ERR_UNSUPPORTED = 3, /* block shape / slice height not supported   */
+    CLSPMV_ERR_CUDA = 4,        /* a CUDA runtime call failed                 */
+    CLSPMV_ERR_REFUSED = 5,     /* the reference converter refuses this input */
+    CLSPMV_ERR_ALIGN = 6,       /* pointer or aligned length not 16-byte able */
+    CLSPMV_ERR_NOT_SORTED = 7,  /* COO input must be sorted by (row, col)     */
+    CLSPMV_ERR_TIMEOUT = 8      /* a bounded device wait ran out              */
+} clspmv_status;
+
+/* Reference constants (include/constant.h:7-45 of clSpMV). */
+#define CLSPMV_GPU_ALIGNMENT 32
+#define CLSPMV_COO_ALIGNMENT 32
+#define CLSPMV_MAX_MEM_OBJ 268435456
+#define CLSPMV_MAX_DIA_NUM 128
+#define CLSPMV_MAX_BAND_NUM 31
+#define CLSPMV_MAX_BAND_WIDTH 128
+#define CLSPMV_WARPSIZE 32
+#define CLSPMV_SELL_GROUP_SIZE 128
+
+/* matrixInfo<int>: include/matrix_storage.h:15-25 */
+typedef struct { int width; int height; int nnz; } clspmv_matinfo;
+
+/* coo_matrix<int,float>: include/matrix_storage.h:141-152 */
+typedef struct {
+    clspmv_matinfo matinfo;
+    int* coo_row_id; int* coo_col_id; float* coo_data;
+} clspmv_coo_f32;
+
+/* csr_matrix<int,float>: include/matrix_storage.h:155-166 */
+typedef struct {
+    clspmv_matinfo matinfo;
+    int* csr_row_ptr; int* csr_col_id; float* csr_data;
+} clspmv_csr_f32;
+
+/* dia_matrix<int,int,float>: include/matrix_storage.h:30-47.
+ * dia_data[d * dia_length_aligned + row] holds A[row, row + dia_offsets[d]]. */
+typedef struct {
+    clspmv_matinfo matinfo;
+    int dia_num; int dia_length; int dia_length_aligned;
+    int* dia_offsets; float* dia_data;
+} clspmv_dia_f32;
+
+/* bdia_matrix<int,int,float>: include/matrix_storage.h:72-94 */
+typedef struct {
+    clspmv_matinfo matinfo;
+    int bdia_band_num; int bdia_length; int bdia_length_aligned;
+    int* bdia_offsets; int* bdia_bptr; float* bdia_data;
+} clspmv_bdia_f32;
+
+/* ell_matrix<int,float>: include/matrix_storage.h:96-111 (column major) */
+typedef struct {
+    clspmv_matinfo matinfo;
+    int ell_num; int ell_height_aligned;
+    int* ell_col_id; float* ell_data;
+} clspmv_ell_f32;
+
+/* sell_matrix<int,float>: include/matrix_storage.h:122-137 */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int sell_slice_height; int sell_slice_num;
+    int* sell_slice_ptr; int* sell_col_id; float* sell_data;
+} clspmv_sell_f32;
+
+/* bcsr_matrix<int,float>: include/matrix_storage.h:178-199 (host only) */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int bcsr_bwidth; unsigned int bcsr_bheight;
+    int bcsr_row_num; int bcsr_aligned_size; int bcsr_block_num;
+    int* bcsr_row_ptr; int* bcsr_col_id; float* bcsr_data;
+} clspmv_bcsr_f32;
+
+/* bell_matrix<int,float>: include/matrix_storage.h:215-236 (host only) */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int bell_bwidth; unsigned int bell_bheight;
+    int bell_row_num; int bell_block_num; int bell_height_aligned; int bell_float4_aligned;
+    int* bell_col_id; float* bell_data;
+} clspmv_bell_f32;
+
+/* b4csr_matrix<int,float>: include/matrix_storage.h:266-287 ("BCSR" on the GPU).
+ * Column ids in float4 units; data plane (w4, h) holds one float4 per block:
+ * b4csr_data[w4*aligned*bh + h*aligned + 4*block + w]. */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int b4csr_bwidth; unsigned int b4csr_bheight;
+    int b4csr_row_num; int b4csr_aligned_size; int b4csr_block_num;
+    int* b4csr_row_ptr; int* b4csr_col_id; float* b4csr_data;
+} clspmv_b4csr_f32;
+
+/* b4ell_matrix<int,float>: include/matrix_storage.h:311-332 ("BELL" on the GPU) */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int b4ell_bwidth; unsigned int b4ell_bheight;
+    int b4ell_row_num; int b4ell_block_num; int b4ell_height_aligned; int b4ell_float4_aligned;
+    int* b4ell_col_id; float* b4ell_data;
+} clspmv_b4ell_f32;
+
+/* sbell_matrix<int,float>: include/matrix_storage.h:344-365 */
+typedef struct {
+    clspmv_matinfo matinfo;
+    unsigned int sbell_bwidth; unsigned int sbell_bheight; unsigned int sbell_slice_height;
+    int sbell_slice_num; int sbell_row_num;
+    int* sbell_slice_ptr; int* sbell_col_id; float* sbell_data;
+} clspmv_sbell_f32;
+
+/* ------------------------------------------------------------------------ */
+/* Library                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Version string, e.g. "clspmv_b200 0.1 sm_100a". */
+const char* clspmv_version(void);
+/* Human readable text for a status code. */
+const char* clspmv_status_string(int status);
+/* Last CUDA error text seen by the library on this thread ("" if none). */
+const char* clspmv_last_cuda_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Host converters. Outputs are malloc'ed; release with clspmv_free_<fmt>.   */
+/* Byte-identical to the reference converters on sorted COO input.          */
+/* ------------------------------------------------------------------------ */
+
+/* sort_coo: include/matrix_storage.h:744-815 (row-major (row, col) order). */
+int clspmv_sort_coo_f32(clspmv_coo_f32* mat);
+/* if_sorted_coo: include/matrix_storage.h:731-741. Returns 1 if sorted. */
+int clspmv_is_sorted_coo_f32(const clspmv_coo_f32* mat);
+/* coo2csr: include/matrix_storage.h:1268-1307 */
+int clspmv_coo2csr_f32(const clspmv_coo_f32* src, clspmv_csr_f32* dst);
+/* pad_csr: src/util.cpp:31-72 (rows padded to a multiple of `alignment`
+ * with the last column id and 0.0f). */
+int clspmv_pad_csr_f32(const clspmv_csr_f32* src, clspmv_csr_f32* dst, int alignment);
+/* coo2dia: include/matrix_storage.h:936-1014. CLSPMV_ERR_REFUSED when the
+ * reference refuses (padded size rule at :972). */
+int clspmv_coo2dia_f32(const clspmv_coo_f32* src, clspmv_dia_f32* dst, int alignment);
+/* coo2bdia: include/matrix_storage.h:1184-1236 */
+int clspmv_coo2bdia_f32(const clspmv_coo_f32* src, clspmv_bdia_f32* dst, int alignment);
+/* coo2ell: include/matrix_storage.h:1339-1394. ellnum == 0 -> max row length.
+ * CLSPMV_ERR_ARG when a row is longer than a given ellnum (reference
+ * assert at :1379); CLSPMV_ERR_REFUSED when aligned_height*ellnum exceeds
+ * INT_MAX (the reference overflows int there). */
+int clspmv_coo2ell_f32(const clspmv_coo_f32* src, clspmv_ell_f32* dst, int alignment, int ellnum);
+/* coo2sell: include/matrix_storage.h:1397-1513 */
+int clspmv_coo2sell_f32(const clspmv_coo_f32* src, clspmv_sell_f32* dst, unsigned int slice_height);
+/* coo2bcsr: include/matrix_storage.h:1593-1737 */
+int clspmv_coo2bcsr_f32(const clspmv_coo_f32* src, clspmv_bcsr_f32* dst,
+                        unsigned int bwidth, unsigned int bheight, int alignment);
+/* coo2b4csr: include/matrix_storage.h:1740-1897 (refusal cap at :1863) */
+int clspmv_coo2b4csr_f32(const clspmv_coo_f32* src, clspmv_b4csr_f32* dst,
+                         unsigned int bwidth, unsigned int bheight, int alignment);
+/* coo2bell: include/matrix_storage.h:1940-2006 */
+int clspmv_coo2bell_f32(const clspmv_coo_f32* src, clspmv_bell_f32* dst,
+                        unsigned int bwidth, unsigned int bheight, int alignment, int ellnum);
+/* coo2b4ell: include/matrix_storage.h:2008-2200 (refusal cap at :2141) */
+int clspmv_coo2b4ell_f32(const clspmv_coo_f32* src, clspmv_b4ell_f32* dst,
+                         unsigned int bwidth, unsigned int bheight, int alignment, int ellnum);
+/* coo2sbell: include/matrix_storage.h:2202-2409 (refusal cap at :2350) */
+int clspmv_coo2sbell_f32(const clspmv_coo_f32* src, clspmv_sbell_f32* dst,
+                         unsigned int bwidth, unsigned int bheight, unsigned int slice_height);
+
+/* Inverse converters (allocate dst arrays). csr2coo :1238-1266, dia2coo
+ * :825-863, bdia2coo :1136-1181, ell2coo :1309-1337, bcsr2coo :1545-1589,
+ * bell2coo :1900-1938. The b4csr/b4ell/sbell inverses have no reference
+ * counterpart; they exist for round-trip checks of the block layouts. */
+int clspmv_csr2coo_f32(const clspmv_csr_f32* src, clspmv_coo_f32* dst);
+int clspmv_dia2coo_f32(const clspmv_dia_f32* src, clspmv_coo_f32* dst);
+int clspmv_bdia2coo_f32(const clspmv_bdia_f32* src, clspmv_coo_f32* dst);
+int clspmv_ell2coo_f32(const clspmv_ell_f32* src, clspmv_coo_f32* dst);
+int clspmv_bcsr2coo_f32(const clspmv_bcsr_f32* src, clspmv_coo_f32* dst);
+int clspmv_bell2coo_f32(const clspmv_bell_f32* src, clspmv_coo_f32* dst);
+int clspmv_b4csr2coo_f32(const clspmv_b4csr_f32* src, clspmv_coo_f32* dst);
+int clspmv_b4ell2coo_f32(const clspmv_b4ell_f32* src, clspmv_coo_f32* dst);
+int clspmv_sbell2coo_f32(const clspmv_sbell_f32* src, clspmv_coo_f32* dst);
+
+/* free_*: include/matrix_storage.h:529-652. Frees the arrays and nulls them. */
+void clspmv_free_coo_f32(clspmv_coo_f32* m);
+void clspmv_free_csr_f32(clspmv_csr_f32* m);
+void clspmv_free_dia_f32(clspmv_dia_f32* m);
+void clspmv_free_bdia_f32(clspmv_bdia_f32* m);
+void clspmv_free_ell_f32(clspmv_ell_f32* m);
+void clspmv_free_sell_f32(clspmv_sell_f32* m);
+void clspmv_free_bcsr_f32(clspmv_bcsr_f32* m);
+void clspmv_free_bell_f32(clspmv_bell_f32* m);
+void clspmv_free_b4csr_f32(clspmv_b4csr_f32* m);
+void clspmv_free_b4ell_f32(clspmv_b4ell_f32* m);
+void clspmv_free_sbell_f32(clspmv_sbell_f32* m);
+
+/* ------------------------------------------------------------------------ */
+/* Device residency. upload: cudaMalloc + copy of every array of `host`     */
+/* into `dev` (scalars copied). device_free: cudaFree of those arrays.      */
+/* Replaces the ALLOCATE_GPU_READ uploads of the per-format drivers         */
+/* (include/oclcommon.h:13-38) and the cpy_<fmt>_mat helpers of             */
+/* src/spmv_cocktail.cpp:304-1009.                                          */
+/* ------------------------------------------------------------------------ */
+int clspmv_upload_coo_f32(const clspmv_coo_f32* host, clspmv_coo_f32* dev);
+int clspmv_upload_csr_f32(const clspmv_csr_f32* host, clspmv_csr_f32* dev);
+int clspmv_upload_dia_f32(const clspmv_dia_f32* host, clspmv_dia_f32* dev);
+int clspmv_upload_bdia_f32(const clspmv_bdia_f32* host, clspmv_bdia_f32* dev);
+int clspmv_upload_ell_f32(const clspmv_ell_f32* host, clspmv_ell_f32* dev);
+int clspmv_upload_sell_f32(const clspmv_sell_f32* host, clspmv_sell_f32* dev);
+int clspmv_upload_b4csr_f32(const clspmv_b4csr_f32* host, clspmv_b4csr_f32* dev);
+int clspmv_upload_b4ell_f32(const clspmv_b4ell_f32* host, clspmv_b4ell_f32* dev);
+int clspmv_upload_sbell_f32(const clspmv_sbell_f32* host, clspmv_sbell_f32* dev);
+int clspmv_device_free_coo_f32(clspmv_coo_f32* dev);
+int clspmv_device_free_csr_f32(clspmv_csr_f32* dev);
+int clspmv_device_free_dia_f32(clspmv_dia_f32* dev);
+int clspmv_device_free_bdia_f32(clspmv_bdia_f32* dev);
+int clspmv_device_free_ell_f32(clspmv_ell_f32* dev);
+int clspmv_device_free_sell_f32(clspmv_sell_f32* dev);
+int clspmv_device_free_b4csr_f32(clspmv_b4csr_f32* dev);
+int clspmv_device_free_b4ell_f32(clspmv_b4ell_f32* dev);
+int clspmv_device_free_sbell_f32(clspmv_sbell_f32* dev);
+
+/* ------------------------------------------------------------------------ */
+/* Compute entry points (device structs, device x and y).                    */
+/* x has matinfo.width entries, y has matinfo.height entries; both 16-byte  */
+/* aligned. All launches are asynchronous on `stream`.                      */
+/* ------------------------------------------------------------------------ */
+
+/* CSR, thread per row. Replaces gpu_csr_sc_pm / _u4 / _float4_noif
+ * (kernels/spmv_csr_scalar.cl:5-209), driver src/spmv_csr_scalar.cpp:670-713.
+ * Rows padded by pad_csr(.., 4) take the 128-bit load path automatically. */
+int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* dev, const float* x, float* y,
+                               float alpha, float beta, clspmv_stream_t stream);
+
+/* CSR, `threads_per_row` lanes per row (1,2,4,8,16,32; 0 = chosen from the
+ * mean row length) with a shuffle reduction. Replaces gpu_csr_ve_slm_pm_fs /
+ * gpu_csr_ve_reduction_fs (kernels/spmv_csr_vector.cl:4-191), driver
+ * src/spmv_csr_vector.cpp:619-664. */
+int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* dev, const float* x, float* y,
+                               float alpha, float beta, int threads_per_row,
+                               clspmv_stream_t stream);
+
+/* CSR, nnz-balanced merge-path tiles: every CTA gets the same number of
+ * (rows + nonzeros), so power-law rows cost the same as regular ones.
+ * `tile_coord` is a device array of 2*(ntiles+1) ints made by
+ * clspmv_csr_merge_plan (rows finished, nonzeros consumed at each tile
+ * start). This is the CSR kernel the autotuner and the Cocktail runtime use. */
+int clspmv_csr_merge_tiles(int rows, int nnz);
+int clspmv_csr_merge_plan(const clspmv_csr_f32* dev, int* tile_coord, clspmv_stream_t stream);
+int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* dev, const int* tile_coord,
+                              const float* x, float* y, float alpha, float beta,
+                              clspmv_stream_t stream);
+
+/* COO, single-pass warp segmented reduction (row-sorted input). Replaces the
+ * two-pass gpu_coo_s1/gpu_coo_s2 (kernels/spmv_coo.cl:4-217), driver
+ * src/spmv_coo.cpp:17-353. */
+int clspmv_coo_spmv_f32(const clspmv_coo_f32* dev, const float* x, float* y,
+                        float alpha, float beta, clspmv_stream_t stream);
+
+/* DIA. Replaces gpu_dia{,_v4,_tx,_v4_tx} (kernels/spmv_dia.cl:4-170),
+ * driver src/spmv_dia.cpp:366-395. x is not padded: out-of-range columns
+ * are predicated off instead of read from an extended vector. */
+int clspmv_dia_spmv_f32(const clspmv_dia_f32* dev, const float* x, float* y,
+                        float alpha, float beta, clspmv_stream_t stream);
+
+/* BDIA with a shared-memory x window per band. Replaces gpu_bdia* variants
+ * (kernels/spmv_bdia.cl:4-283), driver src/spmv_bdia.cpp:413-441. */
+int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* dev, const float* x, float* y,
+                         float alpha, float beta, clspmv_stream_t stream);
+
+/* ELL (column major), 4 rows per thread with 128-bit loads. Replaces
+ * gpu_ell{,_v4,_tx,_v4_tx} (kernels/spmv_ell.cl:4-104). */
+int clspmv_ell_spmv_f32(const clspmv_ell_f32* dev, const float* x, float* y,
+                        float alpha, float beta, clspmv_stream_t stream);
+
+/* SELL, any slice height that is a multiple of 4 (32 and 128 in the
+ * reference). Replaces gpu_sell_warp / gpu_sell_group (kernels/spmv_sell.cl). */
+int clspmv_sell_spmv_f32(const clspmv_sell_f32* dev, const float* x, float* y,
+                         float alpha, float beta, clspmv_stream_t stream);
+
+/* BELL = b4ell, block shapes {1,2,4,8} x {4,8}. Replaces the 32 kernels of
+ * kernels/spmv_bell.cl, driver src/spmv_bell.cpp:345-399. */
+int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* dev, const float* x, float* y,
+                          float alpha, float beta, clspmv_stream_t stream);
+
+/* SBELL, slice of `sbell_slice_height` block rows (32 in the reference).
+ * Replaces the 16 kernels of kernels/spmv_sbell.cl. */
+int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* dev, const float* x, float* y,
+                          float alpha, float beta, clspmv_stream_t stream);
+
+/* BCSR = b4csr, block shapes {1,2,4,8} x {4,8}. Replaces the 16 kernels of
+ * kernels/spmv_bcsr.cl, driver src/spmv_bcsr.cpp:224-278. */
+int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* dev, const float* x, float* y,
+                          float alpha, float beta, clspmv_stream_t stream);
+
+/* Number of kernels this library launched since load (all entry points). */
+long long clspmv_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLSPMV_B200_H */
