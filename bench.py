@@ -3,12 +3,17 @@
 benchmark, src/spmv_all.cpp:196-250, on synthetic matrices of the named
 shapes).
 
-One step = one y += A x launch of every format kernel on its matrix:
+One step = one y += A x launch of each of the nine formats on its matrix,
+with the format's best kernel (the reference's drivers likewise report the
+best variant per format, e.g. src/spmv_csr_vector.cpp:649-656):
 
   stencil27   3D 27-point stencil 128^3 (2,097,152 rows, 55,742,968 nnz):  DIA, BDIA
-  powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR-merge, CSR-vector,
-              CSR-scalar, COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32
+  powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR (merge-path kernel),
+              COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32
   blocks4x4   500,000 block rows x 8 dense 4x4 blocks (2,000,000 rows, 64M nnz):  BELL, SBELL, BCSR
+
+The CSR-vector and CSR-scalar kernels (the reference's two CSR drivers) are
+timed separately and reported under "variants".
 
 value = sum of useful flops (2 nnz per SpMV) / sum of kernel times, GFLOP/s.
 Kernel times are CUDA events on the launching stream; every matrix is larger
@@ -73,45 +78,63 @@ def split_hyb(coo_arrays, k):
     return (h, w, r[head], c[head], v[head]), (h, w, r[~head], c[~head], v[~head])
 
 
-def build_workload(small: bool):
+VARIANT_KEYS = {"csr_vector", "csr_scalar"}
+FORMAT_KEYS = {"stencil27": ["dia", "bdia"],
+               "powerlaw": ["csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32"],
+               "blocks4x4": ["bell", "sbell", "bcsr"]}
+
+
+def build_workload(small: bool, only=None):
+    """Host matrices of the sweep; `only` restricts it to some format keys
+    (and builds only the matrices they need)."""
     from clspmv_mic_b200 import formats as F
     from clspmv_mic_b200 import synth
 
-    if small:
-        sten, pl, blk = synth.stencil_27pt(32), synth.powerlaw(1 << 15, maxlen=2000), synth.block_rows(8000, 8)
-    else:
-        sten, pl, blk = synth.stencil_27pt(128), synth.powerlaw(1 << 20), synth.block_rows(500_000, 8)
-    mats = {"stencil27": sten, "powerlaw": pl, "blocks4x4": blk}
+    want = set(only) if only else {k for ks in FORMAT_KEYS.values() for k in ks}
+    if "ell" in want or "ell_tail_coo" in want:
+        want |= {"ell", "ell_tail_coo"}
+    gens = {
+        "stencil27": (lambda: synth.stencil_27pt(32)) if small else (lambda: synth.stencil_27pt(128)),
+        "powerlaw": (lambda: synth.powerlaw(1 << 15, maxlen=2000)) if small else (lambda: synth.powerlaw(1 << 20)),
+        "blocks4x4": (lambda: synth.block_rows(8000, 8)) if small else (lambda: synth.block_rows(500_000, 8)),
+    }
+    mats = {name: gen() for name, gen in gens.items() if want & set(FORMAT_KEYS[name])}
     items = []
+    meta = {"ell_width": None}
 
-    def add(key, mat, host, kw=None, part_of=None):
+    def add(key, mat, make, kw=None, part_of=None):
+        if key not in want:
+            return
+        host = make()
         h, w = mats[mat][0], mats[mat][1]
         items.append(dict(key=key, matrix=mat, host=host, kw=kw or {}, rows=h, cols=w, nnz=int(host.nnz),
                           stored=host.stored_bytes(), part_of=part_of))
 
-    coo = F.coo_matrix(*sten)
-    add("dia", "stencil27", F.coo2dia(coo))
-    add("bdia", "stencil27", F.coo2bdia(coo))
-    del coo
-
-    coo = F.coo_matrix(*pl)
-    csr = F.coo2csr(coo)
-    add("csr_merge", "powerlaw", csr, {"variant": "merge"})
-    add("csr_vector", "powerlaw", csr, {"variant": "vector"})
-    add("csr_scalar", "powerlaw", csr, {"variant": "scalar"})
-    add("coo", "powerlaw", coo)
-    lengths = np.diff(csr.array("csr_row_ptr"))
-    k = hyb_width(lengths)
-    ell_part, coo_tail = split_hyb(pl, k)
-    add("ell", "powerlaw", F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell")
-    add("ell_tail_coo", "powerlaw", F.coo_matrix(*coo_tail), part_of="ell")
-    add("sell32", "powerlaw", F.coo2sell(coo, 32))
-
-    coo = F.coo_matrix(*blk)
-    add("bell", "blocks4x4", F.coo2b4ell(coo, 4, 4))
-    add("sbell", "blocks4x4", F.coo2sbell(coo, 4, 4, 32))
-    add("bcsr", "blocks4x4", F.coo2b4csr(coo, 4, 4))
-    return mats, items, {"ell_width": k}
+    if "stencil27" in mats:
+        coo = F.coo_matrix(*mats["stencil27"])
+        add("dia", "stencil27", lambda: F.coo2dia(coo))
+        add("bdia", "stencil27", lambda: F.coo2bdia(coo))
+    if "powerlaw" in mats:
+        pl = mats["powerlaw"]
+        coo = F.coo_matrix(*pl)
+        csr = F.coo2csr(coo)
+        add("csr_merge", "powerlaw", lambda: csr, {"variant": "merge"})
+        add("csr_vector", "powerlaw", lambda: csr, {"variant": "vector"})
+        add("csr_scalar", "powerlaw", lambda: csr, {"variant": "scalar"})
+        add("coo", "powerlaw", lambda: coo)
+        if "ell" in want:
+            k = hyb_width(np.diff(csr.array("csr_row_ptr")))
+            meta["ell_width"] = k
+            ell_part, coo_tail = split_hyb(pl, k)
+            add("ell", "powerlaw", lambda: F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell")
+            add("ell_tail_coo", "powerlaw", lambda: F.coo_matrix(*coo_tail), part_of="ell")
+        add("sell32", "powerlaw", lambda: F.coo2sell(coo, 32))
+    if "blocks4x4" in mats:
+        coo = F.coo_matrix(*mats["blocks4x4"])
+        add("bell", "blocks4x4", lambda: F.coo2b4ell(coo, 4, 4))
+        add("sbell", "blocks4x4", lambda: F.coo2sbell(coo, 4, 4, 32))
+        add("bcsr", "blocks4x4", lambda: F.coo2b4csr(coo, 4, 4))
+    return mats, items, meta
 
 
 def algorithmic_bytes(it) -> int:
@@ -306,10 +329,7 @@ def run_ours(args):
     world, rank, local = dist_init(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    mats, items, meta = build_workload(args.small)
-    if args.only:
-        keep = set(args.only.split(","))
-        items = [it for it in items if it["key"] in keep]
+    mats, items, meta = build_workload(args.small, args.only.split(",") if args.only else None)
 
     stream = torch.cuda.Stream(device=dev)
     xs, ys = {}, {}
@@ -323,6 +343,8 @@ def run_ours(args):
         it.pop("host")
     torch.cuda.synchronize()
 
+    variants = [it for it in items if it["key"] in VARIANT_KEYS]
+    items = [it for it in items if it["key"] not in VARIANT_KEYS]
     K = len(items)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(K + 1)] for _ in range(args.steps)]
 
@@ -413,6 +435,25 @@ def run_ours(args):
             "gbs": round(ab / (med[j] * 1e-3) / 1e9, 1), "frac": round(ab / (med[j] * 1e-3) / 1e9 / peak, 3),
             "alg_bytes": ab, "useful_bytes": useful, "nnz": it["nnz"], "rows": it["rows"],
         }
+    # the CSR-vector / CSR-scalar variants, outside the timed step
+    variant_stats = {}
+    for it in variants:
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                it["dev"].spmv(xs[it["matrix"]], ys[it["key"]], 1.0, 1.0, stream=stream, **it["kw"])
+            v0 = torch.cuda.Event(enable_timing=True)
+            v1 = torch.cuda.Event(enable_timing=True)
+            reps = max(3, min(10, args.steps))
+            v0.record(stream)
+            for _ in range(reps):
+                it["dev"].spmv(xs[it["matrix"]], ys[it["key"]], 1.0, 1.0, stream=stream, **it["kw"])
+            v1.record(stream)
+        torch.cuda.synchronize()
+        ms = v0.elapsed_time(v1) / reps
+        ab = algorithmic_bytes(it)
+        variant_stats[it["key"]] = {"matrix": it["matrix"], "ms": round(ms, 5),
+                                    "gflops": round(format_flops(it) / (ms * 1e-3) / 1e9, 2),
+                                    "gbs": round(ab / (ms * 1e-3) / 1e9, 1), "frac": round(ab / (ms * 1e-3) / 1e9 / peak, 3)}
     dom = int(np.argmax(mean))
     dom_it = items[dom]
     ab = algorithmic_bytes(dom_it)
@@ -438,6 +479,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
         "formats": formats,
+        "variants": variant_stats,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)

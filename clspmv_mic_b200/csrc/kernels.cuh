@@ -1,16 +1,26 @@
-// kernels.cuh — CTA tile functions of every storage format (sm_100a).
+// kernels.cuh — CTA-level SpMV work functions of every storage format
+// (sm_100a).
 //
-// All tiles compute  y[r] <- alpha * (A x)[r] + beta * y[r]  for the rows they
-// own. With ATOMIC = true they instead add alpha * (A x)[r] with atomicAdd
-// (beta must then have been applied beforehand); the Cocktail runtime uses
-// that mode because several parts add into the same y.
+// All functions compute  y[r] <- alpha * (A x)[r] + beta * y[r]  for the rows
+// they own. With ATOMIC = true they add alpha * (A x)[r] with red.global.add
+// instead (beta must then have been applied beforehand); the Cocktail runtime
+// uses that mode because several parts add into the same y, and the
+// load-balanced kernels (CSR merge, COO, SELL) use it for rows that straddle
+// two CTAs.
+//
+// Work distribution: a launch has `ncta` CTAs; CTA `cta` owns one contiguous,
+// equal share of the format's units (rows, block rows, slice columns,
+// nonzeros) and walks it in passes of one block of threads. Equal shares keep
+// every CTA busy to the end of the launch (no partial last wave), and the
+// functions take (cta, ncta) explicitly so that the fused Cocktail kernel can
+// give each part its own range of CTAs.
 //
 // The reference's kernels (kernels/*.cl of clSpMV) run one work-item per row
-// or per block row and rely on the texture path for x. Here the matrix arrays
+// or block row and read x through the texture path. Here the matrix arrays
 // are read with 128-bit, fully coalesced, L1-bypassing evict-first loads in
 // each format's native layout; x is gathered through L1 with an evict-last
-// L2 policy; banded formats stage their x window in shared memory; CSR-vector
-// and COO reduce with warp shuffles.
+// L2 policy; BDIA stages its x window in shared memory; CSR-vector, COO and
+// SELL reduce with warp shuffles.
 #pragma once
 #include <climits>
 #include "common.cuh"
@@ -19,9 +29,7 @@ namespace clspmv {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// ---------------------------------------------------------------------------
 // x as float4 at a float index c (c % 4 == 0), zero past `cols`.
-// ---------------------------------------------------------------------------
 __device__ __forceinline__ float4 load_x4_guarded(const float* x, int c, int cols, uint64_t pol)
 {
     if (c + 3 < cols) return ld_x4(x + c, pol);
@@ -37,114 +45,218 @@ __device__ __forceinline__ float x_or_zero(const float* x, int c, int cols, uint
     return (unsigned)c < (unsigned)cols ? ld_x(x + c, pol) : 0.f;
 }
 
+// Equal contiguous share [b, e) of `units` for CTA `cta` of `ncta`, with
+// share boundaries on multiples of `quantum`.
+__device__ __forceinline__ void cta_share(long long units, int quantum, int cta, int ncta, long long& b, long long& e)
+{
+    long long per = (units + ncta - 1) / ncta;
+    per = (per + quantum - 1) / quantum * quantum;
+    b = min(units, per * cta);
+    e = min(units, b + per);
+}
+
+template <bool ATOMIC>
+__device__ __forceinline__ void y_put4(const float* acc, long long row0, long long e, float* y, float alpha, float beta)
+{
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        if (row0 + i < e) y_update<ATOMIC>(y, row0 + i, alpha, beta, acc[i]);
+}
+
 // ---------------------------------------------------------------------------
 // DIA (kernels/spmv_dia.cl:4-170): 4 consecutive rows per thread, one
-// 128-bit load of dia_data per diagonal; diagonal offsets staged in shared
-// memory 256 at a time (the reference keeps <= MAX_DIA_NUM in __local).
+// 128-bit load of dia_data per diagonal; offsets staged in shared memory 256
+// at a time (the reference keeps <= MAX_DIA_NUM offsets in __local).
 // ---------------------------------------------------------------------------
-constexpr int kDiaRowsPerTile = kBlock * 4;
+constexpr int kDiaRowsPerPass = kBlock * 4;
 constexpr int kDiaSmemBytes = kBlock * sizeof(int);
 
 template <bool ATOMIC>
-__device__ __forceinline__ void dia_tile(const DiaArgs& a, int tile, char* smem)
+__device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, char* smem)
 {
     int* s_off = reinterpret_cast<int*>(smem);
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int row0 = tile * kDiaRowsPerTile + threadIdx.x * 4;
-    const bool active = row0 < a.rows;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
-    for (int d0 = 0; d0 < a.ndiag; d0 += kBlock) {
-        const int nd = min(kBlock, a.ndiag - d0);
+    long long b, e;
+    cta_share(a.rows, 4, cta, ncta, b, e);
+    const bool single_chunk = a.ndiag <= kBlock;
+    if (single_chunk) {
+        if (threadIdx.x < a.ndiag) s_off[threadIdx.x] = a.offsets[threadIdx.x];
         __syncthreads();
-        if (threadIdx.x < nd) s_off[threadIdx.x] = a.offsets[d0 + threadIdx.x];
-        __syncthreads();
-        if (active) {
-            const float* dp = a.data + (size_t)d0 * a.len + row0;
+    }
+    for (long long pass = b; pass < e; pass += kDiaRowsPerPass) {
+        const long long row0 = pass + threadIdx.x * 4;
+        const bool active = row0 < e;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int d0 = 0; d0 < a.ndiag; d0 += kBlock) {
+            const int nd = min(kBlock, a.ndiag - d0);
+            if (!single_chunk) {
+                __syncthreads();
+                if (threadIdx.x < nd) s_off[threadIdx.x] = a.offsets[d0 + threadIdx.x];
+                __syncthreads();
+            }
+            if (active) {
+                const float* dp = a.data + (size_t)d0 * a.len + row0;
 #pragma unroll 4
-            for (int k = 0; k < nd; k++) {
-                const int c = row0 + s_off[k];
-                const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
-                float x0, x1, x2, x3;
-                if (c >= 0 && c + 3 < a.cols) {
-                    x0 = ld_x(a.x + c, pl);
-                    x1 = ld_x(a.x + c + 1, pl);
-                    x2 = ld_x(a.x + c + 2, pl);
-                    x3 = ld_x(a.x + c + 3, pl);
-                } else {
-                    x0 = x_or_zero(a.x, c, a.cols, pl);
-                    x1 = x_or_zero(a.x, c + 1, a.cols, pl);
-                    x2 = x_or_zero(a.x, c + 2, a.cols, pl);
-                    x3 = x_or_zero(a.x, c + 3, a.cols, pl);
+                for (int k = 0; k < nd; k++) {
+                    const int c = (int)row0 + s_off[k];
+                    const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
+                    float x0, x1, x2, x3;
+                    if (c >= 0 && c + 3 < a.cols) {
+                        x0 = ld_x(a.x + c, pl);
+                        x1 = ld_x(a.x + c + 1, pl);
+                        x2 = ld_x(a.x + c + 2, pl);
+                        x3 = ld_x(a.x + c + 3, pl);
+                    } else {
+                        x0 = x_or_zero(a.x, c, a.cols, pl);
+                        x1 = x_or_zero(a.x, c + 1, a.cols, pl);
+                        x2 = x_or_zero(a.x, c + 2, a.cols, pl);
+                        x3 = x_or_zero(a.x, c + 3, a.cols, pl);
+                    }
+                    acc[0] = fmaf(v.x, x0, acc[0]);
+                    acc[1] = fmaf(v.y, x1, acc[1]);
+                    acc[2] = fmaf(v.z, x2, acc[2]);
+                    acc[3] = fmaf(v.w, x3, acc[3]);
                 }
-                acc0 = fmaf(v.x, x0, acc0);
-                acc1 = fmaf(v.y, x1, acc1);
-                acc2 = fmaf(v.z, x2, acc2);
-                acc3 = fmaf(v.w, x3, acc3);
             }
         }
-    }
-    if (active) {
-        y_update<ATOMIC>(a.y, row0, a.alpha, a.beta, acc0);
-        if (row0 + 1 < a.rows) y_update<ATOMIC>(a.y, row0 + 1, a.alpha, a.beta, acc1);
-        if (row0 + 2 < a.rows) y_update<ATOMIC>(a.y, row0 + 2, a.alpha, a.beta, acc2);
-        if (row0 + 3 < a.rows) y_update<ATOMIC>(a.y, row0 + 3, a.alpha, a.beta, acc3);
+        if (active) y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
     }
 }
 
 // ---------------------------------------------------------------------------
 // BDIA (kernels/spmv_bdia.cl:4-283): per band, the x window
-// [tile_row0 + offset, tile_row0 + offset + 1024 + width - 1) is staged in
+// [pass_row0 + offset, pass_row0 + offset + 1024 + width - 1) is staged in
 // shared memory once and every diagonal of the band reads it with a shifted
 // index, kept in a 4-register sliding window. Bands wider than kBdiaChunk
 // diagonals are processed kBdiaChunk diagonals at a time.
 // ---------------------------------------------------------------------------
-constexpr int kBdiaRowsPerTile = kBlock * 4;
+constexpr int kBdiaRowsPerPass = kBlock * 4;
 constexpr int kBdiaChunk = 128;
-constexpr int kBdiaSmemBytes = (kBdiaRowsPerTile + kBdiaChunk) * sizeof(float);
+constexpr int kBdiaSmemBytes = (kBdiaRowsPerPass + kBdiaChunk) * sizeof(float);
+constexpr int kBdiaWinMaxSmem = 100 * 1024;   // two window sets at most
 
 template <bool ATOMIC>
-__device__ __forceinline__ void bdia_tile(const BdiaArgs& a, int tile, char* smem)
+__device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, char* smem)
 {
     float* s_x = reinterpret_cast<float*>(smem);
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int rbase = tile * kBdiaRowsPerTile;
+    long long b, e;
+    cta_share(a.rows, 4, cta, ncta, b, e);
     const int l0 = threadIdx.x * 4;
-    const int row0 = rbase + l0;
-    const bool active = row0 < a.rows;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
-    for (int b = 0; b < a.nband; b++) {
-        const int dbeg = a.bptr[b], dend = a.bptr[b + 1];
-        const int boff = a.offsets[b];
-        for (int j0 = 0; j0 < dend - dbeg; j0 += kBdiaChunk) {
-            const int nj = min(kBdiaChunk, dend - dbeg - j0);
-            const int wbase = rbase + boff + j0;
-            const int wlen = kBdiaRowsPerTile + nj - 1;
-            __syncthreads();
-            for (int t = threadIdx.x; t < wlen; t += kBlock) s_x[t] = x_or_zero(a.x, wbase + t, a.cols, pl);
-            __syncthreads();
-            if (active) {
-                const float* dp = a.data + (size_t)(dbeg + j0) * a.len + row0;
-                float w0 = s_x[l0], w1 = s_x[l0 + 1], w2 = s_x[l0 + 2];
+    for (long long pass = b; pass < e; pass += kBdiaRowsPerPass) {
+        const long long row0 = pass + l0;
+        const bool active = row0 < e;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int bd = 0; bd < a.nband; bd++) {
+            const int dbeg = a.bptr[bd], dend = a.bptr[bd + 1];
+            const int boff = a.offsets[bd];
+            for (int j0 = 0; j0 < dend - dbeg; j0 += kBdiaChunk) {
+                const int nj = min(kBdiaChunk, dend - dbeg - j0);
+                const long long wbase = pass + boff + j0;
+                const int wlen = kBdiaRowsPerPass + nj - 1;
+                __syncthreads();
+                for (int t = threadIdx.x; t < wlen; t += kBlock) {
+                    const long long c = wbase + t;
+                    s_x[t] = (c >= 0 && c < a.cols) ? ld_x(a.x + c, pl) : 0.f;
+                }
+                __syncthreads();
+                if (active) {
+                    const float* dp = a.data + (size_t)(dbeg + j0) * a.len + row0;
+                    float w0 = s_x[l0], w1 = s_x[l0 + 1], w2 = s_x[l0 + 2];
 #pragma unroll 4
-                for (int j = 0; j < nj; j++) {
-                    const float w3 = s_x[l0 + j + 3];
+                    for (int j = 0; j < nj; j++) {
+                        const float w3 = s_x[l0 + j + 3];
+                        const float4 v = ld_stream_f4(dp + (size_t)j * a.len, pe);
+                        acc[0] = fmaf(v.x, w0, acc[0]);
+                        acc[1] = fmaf(v.y, w1, acc[1]);
+                        acc[2] = fmaf(v.z, w2, acc[2]);
+                        acc[3] = fmaf(v.w, w3, acc[3]);
+                        w0 = w1;
+                        w1 = w2;
+                        w2 = w3;
+                    }
+                }
+            }
+        }
+        if (active) y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
+    }
+}
+
+// BDIA, pass-window form: the x windows of all bands for one 1024-row pass
+// sit side by side in shared memory (band b at b*1023 + bptr[b], length
+// 1023 + width_b), loaded with cp.async while the previous pass computes
+// (double buffer), so a pass needs one barrier instead of two per band.
+// Used when two window sets fit in shared memory; `win_floats` =
+// nband*1023 + ndiag.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void bdia_prefetch(const BdiaArgs& a, long long pass, float* buf)
+{
+    for (int bd = 0; bd < a.nband; bd++) {
+        const int wo = bd * (kBdiaRowsPerPass - 1) + a.bptr[bd];
+        const int wl = kBdiaRowsPerPass - 1 + (a.bptr[bd + 1] - a.bptr[bd]);
+        const long long c0 = pass + a.offsets[bd];
+        for (int t = threadIdx.x; t < wl; t += kBlock) {
+            const long long c = c0 + t;
+            const bool in = c >= 0 && c < a.cols;
+            cp_async4(buf + wo + t, in ? a.x + c : a.x, in);
+        }
+    }
+    cp_async_commit();
+}
+
+template <bool ATOMIC>
+__device__ __forceinline__ void bdia_window_cta(const BdiaArgs& a, int win_floats, int cta, int ncta, char* smem)
+{
+    float* bufs = reinterpret_cast<float*>(smem);
+    const uint64_t pe = policy_evict_first();
+    long long b, e;
+    cta_share(a.rows, 4, cta, ncta, b, e);
+    const int l0 = threadIdx.x * 4;
+    if (b < e) bdia_prefetch(a, b, bufs);
+    int k = 0;
+    for (long long pass = b; pass < e; pass += kBdiaRowsPerPass, k++) {
+        const long long next = pass + kBdiaRowsPerPass;
+        if (next < e) {
+            bdia_prefetch(a, next, bufs + ((k + 1) & 1) * win_floats);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float* buf = bufs + (k & 1) * win_floats;
+        const long long row0 = pass + l0;
+        if (row0 < e) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int bd = 0; bd < a.nband; bd++) {
+                const int dbeg = a.bptr[bd], dend = a.bptr[bd + 1];
+                const float* w = buf + bd * (kBdiaRowsPerPass - 1) + dbeg + l0;
+                const float* dp = a.data + (size_t)dbeg * a.len + row0;
+                float w0 = w[0], w1 = w[1], w2 = w[2];
+#pragma unroll 4
+                for (int j = 0; j < dend - dbeg; j++) {
+                    const float w3 = w[j + 3];
                     const float4 v = ld_stream_f4(dp + (size_t)j * a.len, pe);
-                    acc0 = fmaf(v.x, w0, acc0);
-                    acc1 = fmaf(v.y, w1, acc1);
-                    acc2 = fmaf(v.z, w2, acc2);
-                    acc3 = fmaf(v.w, w3, acc3);
+                    acc[0] = fmaf(v.x, w0, acc[0]);
+                    acc[1] = fmaf(v.y, w1, acc[1]);
+                    acc[2] = fmaf(v.z, w2, acc[2]);
+                    acc[3] = fmaf(v.w, w3, acc[3]);
                     w0 = w1;
                     w1 = w2;
                     w2 = w3;
                 }
             }
+            y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
         }
-    }
-    if (active) {
-        y_update<ATOMIC>(a.y, row0, a.alpha, a.beta, acc0);
-        if (row0 + 1 < a.rows) y_update<ATOMIC>(a.y, row0 + 1, a.alpha, a.beta, acc1);
-        if (row0 + 2 < a.rows) y_update<ATOMIC>(a.y, row0 + 2, a.alpha, a.beta, acc2);
-        if (row0 + 3 < a.rows) y_update<ATOMIC>(a.y, row0 + 3, a.alpha, a.beta, acc3);
+        __syncthreads();
     }
 }
 
@@ -152,88 +264,126 @@ __device__ __forceinline__ void bdia_tile(const BdiaArgs& a, int tile, char* sme
 // ELL (kernels/spmv_ell.cl:4-104, the _v4 form): 4 rows per thread, int4 and
 // float4 loads of each column-major slot.
 // ---------------------------------------------------------------------------
-constexpr int kEllRowsPerTile = kBlock * 4;
+constexpr int kEllRowsPerPass = kBlock * 4;
 
 template <bool ATOMIC>
-__device__ __forceinline__ void ell_tile(const EllArgs& a, int tile, char*)
+__device__ __forceinline__ void ell_cta(const EllArgs& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int row0 = tile * kEllRowsPerTile + threadIdx.x * 4;
-    if (row0 >= a.rows) return;
-    const int* cp = a.col + row0;
-    const float* dp = a.data + row0;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+    long long b, e;
+    cta_share(a.rows, 4, cta, ncta, b, e);
+    for (long long row0 = b + threadIdx.x * 4; row0 < e; row0 += kEllRowsPerPass) {
+        const int* cp = a.col + row0;
+        const float* dp = a.data + row0;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 4
-    for (int k = 0; k < a.ell_num; k++) {
-        const int4 c = ld_stream_i4(cp + (size_t)k * a.len, pe);
-        const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
-        acc0 = fmaf(v.x, ld_x(a.x + c.x, pl), acc0);
-        acc1 = fmaf(v.y, ld_x(a.x + c.y, pl), acc1);
-        acc2 = fmaf(v.z, ld_x(a.x + c.z, pl), acc2);
-        acc3 = fmaf(v.w, ld_x(a.x + c.w, pl), acc3);
+        for (int k = 0; k < a.ell_num; k++) {
+            const int4 c = ld_stream_i4(cp + (size_t)k * a.len, pe);
+            const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
+            acc[0] = fmaf(v.x, ld_x(a.x + c.x, pl), acc[0]);
+            acc[1] = fmaf(v.y, ld_x(a.x + c.y, pl), acc[1]);
+            acc[2] = fmaf(v.z, ld_x(a.x + c.z, pl), acc[2]);
+            acc[3] = fmaf(v.w, ld_x(a.x + c.w, pl), acc[3]);
+        }
+        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
     }
-    y_update<ATOMIC>(a.y, row0, a.alpha, a.beta, acc0);
-    if (row0 + 1 < a.rows) y_update<ATOMIC>(a.y, row0 + 1, a.alpha, a.beta, acc1);
-    if (row0 + 2 < a.rows) y_update<ATOMIC>(a.y, row0 + 2, a.alpha, a.beta, acc2);
-    if (row0 + 3 < a.rows) y_update<ATOMIC>(a.y, row0 + 3, a.alpha, a.beta, acc3);
 }
 
 // ---------------------------------------------------------------------------
-// SELL (kernels/spmv_sell.cl:4-130): each thread owns 4 consecutive rows of a
-// slice (slice height a multiple of 4), so slice height 128 is one warp per
-// slice reading 512 contiguous bytes per slot, and slice height 32 is 8
-// threads per slice. Slice starts are multiples of the slice height, hence
-// 16-byte aligned.
+// SELL (kernels/spmv_sell.cl:4-130), balanced by columns: the slot space of
+// all slices is split into equal runs of slice columns (one column = the
+// slice_height slots of one width step), so a slice 10,000 columns wide is
+// shared by many warps instead of serialising one. Q = slice_height / 4
+// lanes cover one column with 128-bit loads (4 rows per lane) and a warp
+// steps 32 / Q columns at a time; partial row sums are combined with
+// shuffles and added to y (directly when the warp saw the whole slice, with
+// red.global.add when the slice is shared). Requires slice_height in
+// {4, 8, 16, 32, 64, 128} and beta already applied.
 // ---------------------------------------------------------------------------
-template <bool ATOMIC>
-__device__ __forceinline__ void sell_tile(const SellArgs& a, int tile, char*)
+constexpr int kSellWarpCols = 64;
+
+template <int Q, bool ATOMIC_ALL>
+__device__ __forceinline__ void sell_cta(const SellArgs& a, int cta, int ncta, char*)
 {
+    constexpr int G = 32 / Q;             // columns per warp step
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int sh = a.slice_height;
-    const int qps = sh >> 2;
-    const int q = tile * kBlock + threadIdx.x;
-    const int s = q / qps;
-    if (s >= a.nslice) return;
-    const int sub = q - s * qps;
-    const int start = a.slice_ptr[s];
-    const int width = (a.slice_ptr[s + 1] - start) / sh;
-    const int* cp = a.col + start + sub * 4;
-    const float* dp = a.data + start + sub * 4;
-    float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc3 = 0.f;
+    const int sh = Q * 4;
+    const long long total_cols = (long long)a.slice_ptr[a.nslice] / sh;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / Q, q = lane % Q;
+    const long long nwarps_total = (long long)ncta * (kBlock / 32);
+    const long long wid = (long long)cta * (kBlock / 32) + (threadIdx.x >> 5);
+    for (long long c0 = wid * kSellWarpCols; c0 < total_cols; c0 += nwarps_total * kSellWarpCols) {
+        const long long c1 = min(c0 + kSellWarpCols, total_cols);
+        // first slice whose column range ends after c0
+        int lo = 0, hi = a.nslice - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((long long)a.slice_ptr[mid + 1] <= c0 * sh) lo = mid + 1;
+            else hi = mid;
+        }
+        int s = lo;
+        long long c = c0;
+        while (c < c1) {
+            const long long sb = a.slice_ptr[s] / sh, se = a.slice_ptr[s + 1] / sh;
+            if (se <= c) {
+                s++;
+                continue;
+            }
+            const long long ce = min(c1, se);
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 4
-    for (int k = 0; k < width; k++) {
-        const int4 c = ld_stream_i4(cp + (size_t)k * sh, pe);
-        const float4 v = ld_stream_f4(dp + (size_t)k * sh, pe);
-        acc0 = fmaf(v.x, ld_x(a.x + c.x, pl), acc0);
-        acc1 = fmaf(v.y, ld_x(a.x + c.y, pl), acc1);
-        acc2 = fmaf(v.z, ld_x(a.x + c.z, pl), acc2);
-        acc3 = fmaf(v.w, ld_x(a.x + c.w, pl), acc3);
+            for (long long cc = c + g; cc < ce; cc += G) {
+                const size_t base = (size_t)cc * sh + 4 * q;
+                const int4 cv = ld_stream_i4(a.col + base, pe);
+                const float4 v = ld_stream_f4(a.data + base, pe);
+                acc[0] = fmaf(v.x, ld_x(a.x + cv.x, pl), acc[0]);
+                acc[1] = fmaf(v.y, ld_x(a.x + cv.y, pl), acc[1]);
+                acc[2] = fmaf(v.z, ld_x(a.x + cv.z, pl), acc[2]);
+                acc[3] = fmaf(v.w, ld_x(a.x + cv.w, pl), acc[3]);
+            }
+#pragma unroll
+            for (int off = Q; off < 32; off <<= 1) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(kFull, acc[i], off);
+            }
+            if (g == 0) {
+                const bool whole = sb >= c0 && se <= c1;
+                const long long row0 = (long long)s * sh + 4 * q;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (row0 + i < a.rows) {
+                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += a.alpha * acc[i];
+                        else atomicAdd(a.y + row0 + i, a.alpha * acc[i]);
+                    }
+                }
+            }
+            c = ce;
+            s++;
+        }
     }
-    const int row0 = s * sh + sub * 4;
-    if (row0 < a.rows) y_update<ATOMIC>(a.y, row0, a.alpha, a.beta, acc0);
-    if (row0 + 1 < a.rows) y_update<ATOMIC>(a.y, row0 + 1, a.alpha, a.beta, acc1);
-    if (row0 + 2 < a.rows) y_update<ATOMIC>(a.y, row0 + 2, a.alpha, a.beta, acc2);
-    if (row0 + 3 < a.rows) y_update<ATOMIC>(a.y, row0 + 3, a.alpha, a.beta, acc3);
 }
 
-// Slice heights that are not a multiple of 4: one row per thread.
+// Other slice heights: one row per thread, slice by slice.
 template <bool ATOMIC>
-__device__ __forceinline__ void sell_tile_scalar(const SellArgs& a, int tile, char*)
+__device__ __forceinline__ void sell_rows_cta(const SellArgs& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int row = tile * kBlock + threadIdx.x;
-    if (row >= a.rows) return;
+    long long b, e;
+    cta_share(a.rows, 1, cta, ncta, b, e);
     const int sh = a.slice_height;
-    const int s = row / sh, lr = row - s * sh;
-    const int start = a.slice_ptr[s];
-    const int width = (a.slice_ptr[s + 1] - start) / sh;
-    float acc = 0.f;
+    for (long long row = b + threadIdx.x; row < e; row += kBlock) {
+        const int s = (int)(row / sh), lr = (int)(row - (long long)s * sh);
+        const int start = a.slice_ptr[s];
+        const int width = (a.slice_ptr[s + 1] - start) / sh;
+        float acc = 0.f;
 #pragma unroll 4
-    for (int k = 0; k < width; k++) {
-        const size_t i = (size_t)start + (size_t)k * sh + lr;
-        acc = fmaf(ld_stream_f(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
+        for (int k = 0; k < width; k++) {
+            const size_t i = (size_t)start + (size_t)k * sh + lr;
+            acc = fmaf(ld_stream_f(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
+        }
+        y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
     }
-    y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -242,47 +392,16 @@ __device__ __forceinline__ void sell_tile_scalar(const SellArgs& a, int tile, ch
 // _float4_noif input) use 128-bit loads.
 // ---------------------------------------------------------------------------
 template <bool ATOMIC>
-__device__ __forceinline__ void csr_scalar_tile(const CsrArgs& a, int tile, char*)
+__device__ __forceinline__ void csr_scalar_cta(const CsrArgs& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int row = tile * kBlock + threadIdx.x;
-    if (row >= a.rows) return;
-    const int s = a.row_ptr[row], e = a.row_ptr[row + 1];
-    float acc = 0.f;
-    if (((s | e) & 3) == 0) {
-        for (int j = s; j < e; j += 4) {
-            const int4 c = ld_l1_i4(a.col + j, pe);
-            const float4 v = ld_l1_f4(a.val + j, pe);
-            acc = fmaf(v.x, ld_x(a.x + c.x, pl), acc);
-            acc = fmaf(v.y, ld_x(a.x + c.y, pl), acc);
-            acc = fmaf(v.z, ld_x(a.x + c.z, pl), acc);
-            acc = fmaf(v.w, ld_x(a.x + c.w, pl), acc);
-        }
-    } else {
-#pragma unroll 4
-        for (int j = s; j < e; j++) acc = fmaf(ld_l1_f(a.val + j, pe), ld_x(a.x + ld_l1_i(a.col + j, pe), pl), acc);
-    }
-    y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
-}
-
-// ---------------------------------------------------------------------------
-// CSR vector (kernels/spmv_csr_vector.cl:4-191): T lanes per row with a
-// shuffle reduction (the reference uses a volatile __local reduction that
-// assumes lock-step warps). Rows padded to a multiple of 4 use 128-bit
-// loads, 4 consecutive entries per lane.
-// ---------------------------------------------------------------------------
-template <int T, bool ATOMIC>
-__device__ __forceinline__ void csr_vector_tile(const CsrArgs& a, int tile, char*)
-{
-    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int g = (tile * kBlock + threadIdx.x) / T;
-    const int l = threadIdx.x % T;
-    const bool active = g < a.rows;
-    float acc = 0.f;
-    if (active) {
-        const int s = a.row_ptr[g], e = a.row_ptr[g + 1];
-        if (((s | e) & 3) == 0) {
-            for (int j = s + 4 * l; j < e; j += 4 * T) {
+    long long b, e;
+    cta_share(a.rows, 1, cta, ncta, b, e);
+    for (long long row = b + threadIdx.x; row < e; row += kBlock) {
+        const int s = a.row_ptr[row], en = a.row_ptr[row + 1];
+        float acc = 0.f;
+        if (((s | en) & 3) == 0) {
+            for (int j = s; j < en; j += 4) {
                 const int4 c = ld_l1_i4(a.col + j, pe);
                 const float4 v = ld_l1_f4(a.val + j, pe);
                 acc = fmaf(v.x, ld_x(a.x + c.x, pl), acc);
@@ -292,29 +411,67 @@ __device__ __forceinline__ void csr_vector_tile(const CsrArgs& a, int tile, char
             }
         } else {
 #pragma unroll 4
-            for (int j = s + l; j < e; j += T) acc = fmaf(ld_l1_f(a.val + j, pe), ld_x(a.x + ld_l1_i(a.col + j, pe), pl), acc);
+            for (int j = s; j < en; j++) acc = fmaf(ld_l1_f(a.val + j, pe), ld_x(a.x + ld_l1_i(a.col + j, pe), pl), acc);
         }
+        y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
     }
-#pragma unroll
-    for (int off = T / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off, T);
-    if (active && l == 0) y_update<ATOMIC>(a.y, g, a.alpha, a.beta, acc);
 }
 
 // ---------------------------------------------------------------------------
-// CSR merge path: a tile owns kMergeTile consecutive items of the merge of
-// the row-end offsets row_ptr[1..m] with the nonzero indices 0..nnz-1, so
-// every CTA does the same work whatever the row-length distribution. The
-// tile's row pointers and its nonzero products are staged in shared memory;
-// each thread walks kMergeIPT merge items and accumulates finished rows into
-// a shared per-row sum with shared-memory atomics. Rows that cross a tile
-// boundary are added to y with global atomics; rows owned by the tile are
-// written directly.
+// CSR vector (kernels/spmv_csr_vector.cl:4-191): T lanes per row with a
+// shuffle reduction (the reference uses a volatile __local reduction that
+// assumes lock-step warps). Rows padded to a multiple of 4 use 128-bit
+// loads, 4 consecutive entries per lane.
+// ---------------------------------------------------------------------------
+template <int T, bool ATOMIC>
+__device__ __forceinline__ void csr_vector_cta(const CsrArgs& a, int cta, int ncta, char*)
+{
+    constexpr int kRowsPerPass = kBlock / T;
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    long long b, e;
+    cta_share(a.rows, 1, cta, ncta, b, e);
+    const int l = threadIdx.x % T;
+    for (long long pass = b; pass < e; pass += kRowsPerPass) {
+        const long long g = pass + threadIdx.x / T;
+        const bool active = g < e;
+        float acc = 0.f;
+        if (active) {
+            const int s = a.row_ptr[g], en = a.row_ptr[g + 1];
+            if (((s | en) & 3) == 0) {
+                for (int j = s + 4 * l; j < en; j += 4 * T) {
+                    const int4 c = ld_l1_i4(a.col + j, pe);
+                    const float4 v = ld_l1_f4(a.val + j, pe);
+                    acc = fmaf(v.x, ld_x(a.x + c.x, pl), acc);
+                    acc = fmaf(v.y, ld_x(a.x + c.y, pl), acc);
+                    acc = fmaf(v.z, ld_x(a.x + c.z, pl), acc);
+                    acc = fmaf(v.w, ld_x(a.x + c.w, pl), acc);
+                }
+            } else {
+#pragma unroll 4
+                for (int j = s + l; j < en; j += T) acc = fmaf(ld_l1_f(a.val + j, pe), ld_x(a.x + ld_l1_i(a.col + j, pe), pl), acc);
+            }
+        }
+#pragma unroll
+        for (int off = T / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off, T);
+        if (active && l == 0) y_update<ATOMIC>(a.y, g, a.alpha, a.beta, acc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CSR merge path: tile t owns the kMergeTile consecutive items starting at
+// diagonal t * kMergeTile of the merge of the row-end offsets row_ptr[1..m]
+// with the nonzero indices 0..nnz-1, so every tile does the same work
+// whatever the row-length distribution. The tile's row pointers and its
+// nonzero products are staged in shared memory with fully unrolled loads;
+// each thread walks kMergeIPT merge items and adds finished rows into a
+// per-row shared sum with shared-memory atomics; the tile's rows are then
+// added to y with red.global.add (rows that straddle tiles get one
+// contribution per tile). beta must already be applied.
 // ---------------------------------------------------------------------------
 constexpr int kMergeIPT = 8;
 constexpr int kMergeTile = kBlock * kMergeIPT;
 constexpr int kMergeSmemBytes = (kMergeTile + 2) * sizeof(int) + kMergeTile * sizeof(float) + (kMergeTile + 1) * sizeof(float);
 
-template <bool ATOMIC_ALL>
 __device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __restrict__ tc, int tile, char* smem)
 {
     int* s_rp = reinterpret_cast<int*>(smem);
@@ -324,15 +481,34 @@ __device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __re
     const int x0 = tc[2 * tile], y0 = tc[2 * tile + 1];
     const int x1 = tc[2 * tile + 2], y1 = tc[2 * tile + 3];
     const int nfin = x1 - x0, nz = y1 - y0;
-    for (int k = threadIdx.x; k <= nfin + 1; k += kBlock) {
-        const int r = x0 + k;
-        s_rp[k] = r <= a.rows ? a.row_ptr[r] : INT_MAX;
+    {
+        int cidx[kMergeIPT];
+        float vv[kMergeIPT];
+#pragma unroll
+        for (int i = 0; i < kMergeIPT; i++) {
+            const int k = threadIdx.x + i * kBlock;
+            cidx[i] = k < nz ? ld_stream_i(a.col + y0 + k, pe) : 0;
+        }
+#pragma unroll
+        for (int i = 0; i < kMergeIPT; i++) {
+            const int k = threadIdx.x + i * kBlock;
+            vv[i] = k < nz ? ld_stream_f(a.val + y0 + k, pe) : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i <= kMergeIPT; i++) {
+            const int k = threadIdx.x + i * kBlock;
+            if (k <= nfin + 1) {
+                const int r = x0 + k;
+                s_rp[k] = r <= a.rows ? a.row_ptr[r] : INT_MAX;
+            }
+            if (k <= nfin) s_y[k] = 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < kMergeIPT; i++) {
+            const int k = threadIdx.x + i * kBlock;
+            if (k < nz) s_prod[k] = vv[i] * ld_x(a.x + cidx[i], pl);
+        }
     }
-    for (int k = threadIdx.x; k < nz; k += kBlock) {
-        const int j = y0 + k;
-        s_prod[k] = ld_stream_f(a.val + j, pe) * ld_x(a.x + ld_stream_i(a.col + j, pe), pl);
-    }
-    for (int k = threadIdx.x; k <= nfin; k += kBlock) s_y[k] = 0.f;
     __syncthreads();
 
     const int total = nfin + nz;
@@ -359,26 +535,20 @@ __device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __re
     if (acc != 0.f) atomicAdd(s_y + xi, acc);
     __syncthreads();
 
-    for (int k = threadIdx.x; k <= nfin; k += kBlock) {
+#pragma unroll
+    for (int i = 0; i <= kMergeIPT; i++) {
+        const int k = threadIdx.x + i * kBlock;
+        if (k > nfin) break;
         const int r = x0 + k;
-        if (r >= a.rows) continue;
+        if (r >= a.rows) break;
         const int rs = s_rp[k], re = s_rp[k + 1];
-        const float v = s_y[k];
-        const bool ends_here = k < nfin;
-        if (rs >= y0 && ends_here) {
-            if (rs != re) {
-                if (ATOMIC_ALL) atomicAdd(a.y + r, a.alpha * v);
-                else a.y[r] = a.y[r] + a.alpha * v;
-            }
-        } else {
-            const int from = max(rs, y0), to = ends_here ? re : y1;
-            if (to > from) atomicAdd(a.y + r, a.alpha * v);
-        }
+        const int from = max(rs, y0), to = k < nfin ? re : y1;
+        if (to > from) atomicAdd(a.y + r, a.alpha * s_y[k]);
     }
 }
 
 // Tile start coordinates (rows finished, nonzeros consumed) of the merge
-// path at diagonals t * kMergeTile, t = 0..ntiles.
+// path at diagonal `diag`.
 __device__ __forceinline__ void csr_merge_search(int rows, int nnz, const int* row_ptr, long long diag, int* out)
 {
     const long long total = (long long)rows + nnz;
@@ -394,80 +564,135 @@ __device__ __forceinline__ void csr_merge_search(int rows, int nnz, const int* r
 }
 
 // ---------------------------------------------------------------------------
-// COO (kernels/spmv_coo.cl:4-217): single pass. A warp takes 32*kCooK
-// consecutive nonzeros (row-sorted), loads them lane-striped (coalesced),
-// and runs a segmented inclusive scan per 32-wide step with shuffles, the
-// row id acting as the segment key. The running tail is carried across
-// steps; the first and last row of a warp chunk may be shared with the
-// neighbouring chunk and are added with atomics, interior rows directly.
-// The reference instead writes per-group carries to tmp_rowid/tmp_data and
-// reduces them in a second kernel (gpu_coo_s2).
+// COO (kernels/spmv_coo.cl:4-217): single pass. A warp takes kCooWarpNnz
+// consecutive nonzeros (row-sorted) in steps of 128: each lane loads 4
+// consecutive (row, col, value) with 128-bit loads, reduces them in
+// registers (rows that start and end inside the lane are added to y at
+// once), and only each lane's leading and trailing row partials go through
+// a warp segmented scan (segment starts from one ballot, 5 shuffles). The
+// trailing row of a step is carried into the next step. Every finished row
+// segment is added with red.global.add, so rows shared with the neighbouring
+// chunk need no special case. The reference instead writes per-group carries
+// to tmp_rowid/tmp_data and reduces them in a second kernel (gpu_coo_s2).
+// beta must already be applied; arrays must be 16-byte aligned.
 // ---------------------------------------------------------------------------
-constexpr int kCooK = 8;
-constexpr int kCooWarpNnz = 32 * kCooK;
-constexpr int kCooTileNnz = kCooWarpNnz * (kBlock / 32);
+constexpr int kCooSteps = 2;
+constexpr int kCooWarpNnz = 128 * kCooSteps;
+constexpr int kCooCtaNnz = kCooWarpNnz * (kBlock / 32);
+constexpr int kCooNoRow = INT_MAX;
 
-template <bool ATOMIC_ALL>
-__device__ __forceinline__ void coo_put(float* y, int row, float v, int first_row)
+__device__ __forceinline__ void coo_red(float* y, int row, float v)
 {
-    if (ATOMIC_ALL || row == first_row) atomicAdd(y + row, v);
-    else y[row] += v;
+    if (row != kCooNoRow) atomicAdd(y + row, v);
 }
 
-template <bool ATOMIC_ALL>
-__device__ __forceinline__ void coo_tile(const CooArgs& a, int tile, char*)
+__device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base, uint64_t pe, uint64_t pl)
 {
-    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     const int lane = threadIdx.x & 31;
-    const long long base = (long long)tile * kCooTileNnz + (long long)(threadIdx.x >> 5) * kCooWarpNnz;
-    if (base >= a.nnz) return;
-    int r[kCooK], c[kCooK];
-    float p[kCooK];
+    int r[kCooSteps][4];
+    float p[kCooSteps][4];
+    {
+        int c[kCooSteps][4];
 #pragma unroll
-    for (int k = 0; k < kCooK; k++) {
-        const long long idx = base + k * 32 + lane;
-        if (idx < a.nnz) {
-            r[k] = ld_stream_i(a.row + idx, pe);
-            c[k] = ld_stream_i(a.col + idx, pe);
-            p[k] = ld_stream_f(a.val + idx, pe);
-        } else {
-            r[k] = -1;
-            c[k] = 0;
-            p[k] = 0.f;
+        for (int s = 0; s < kCooSteps; s++) {
+            const long long idx = base + s * 128 + lane * 4;
+            if (idx + 3 < a.nnz) {
+                const int4 rv = ld_stream_i4(a.row + idx, pe);
+                const int4 cv = ld_stream_i4(a.col + idx, pe);
+                const float4 vv = ld_stream_f4(a.val + idx, pe);
+                r[s][0] = rv.x; r[s][1] = rv.y; r[s][2] = rv.z; r[s][3] = rv.w;
+                c[s][0] = cv.x; c[s][1] = cv.y; c[s][2] = cv.z; c[s][3] = cv.w;
+                p[s][0] = vv.x; p[s][1] = vv.y; p[s][2] = vv.z; p[s][3] = vv.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const bool in = idx + j < a.nnz;
+                    r[s][j] = in ? ld_stream_i(a.row + idx + j, pe) : kCooNoRow;
+                    c[s][j] = in ? ld_stream_i(a.col + idx + j, pe) : 0;
+                    p[s][j] = in ? ld_stream_f(a.val + idx + j, pe) : 0.f;
+                }
+            }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < kCooK; k++)
-        if (r[k] >= 0) p[k] *= ld_x(a.x + c[k], pl);
-    const int first_row = __shfl_sync(kFull, r[0], 0);
+        for (int s = 0; s < kCooSteps; s++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (r[s][j] != kCooNoRow) p[s][j] *= ld_x(a.x + c[s][j], pl);
+    }
     float carry = 0.f;
     int carry_row = -1;
 #pragma unroll
-    for (int k = 0; k < kCooK; k++) {
-        const int rr = r[k];
-        float v = p[k];
-        const int lead = __shfl_sync(kFull, rr, 0);
-        if (carry_row >= 0 && lead != carry_row) {
-            if (lane == 0) coo_put<ATOMIC_ALL>(a.y, carry_row, a.alpha * carry, first_row);
-            carry = 0.f;
-            carry_row = -1;
+    for (int s = 0; s < kCooSteps; s++) {
+        const int head_row = r[s][0], tail_row = r[s][3];
+        const bool single = head_row == tail_row;
+        float head = 0.f, tail = 0.f;
+        if (single) {
+            tail = p[s][0] + p[s][1] + p[s][2] + p[s][3];
+        } else {
+            head = p[s][0];
+            tail = p[s][3];
+            int run_row = -1;
+            float run = 0.f;
+#pragma unroll
+            for (int j = 1; j < 3; j++) {
+                const int rj = r[s][j];
+                if (rj == head_row) {
+                    head += p[s][j];
+                } else if (rj == tail_row) {
+                    tail += p[s][j];
+                } else if (rj == run_row) {
+                    run += p[s][j];
+                } else {
+                    if (run_row >= 0) coo_red(a.y, run_row, a.alpha * run);
+                    run_row = rj;
+                    run = p[s][j];
+                }
+            }
+            if (run_row >= 0) coo_red(a.y, run_row, a.alpha * run);
         }
+        // the previous step's trailing row
+        const int lead = __shfl_sync(kFull, head_row, 0);
+        if (carry_row >= 0 && lead != carry_row) {
+            if (lane == 0) coo_red(a.y, carry_row, a.alpha * carry);
+            carry_row = -1;
+            carry = 0.f;
+        }
+        if (lane == 0 && carry_row >= 0) {
+            if (single) tail += carry;
+            else head += carry;
+        }
+        // segmented inclusive scan of the lanes' trailing partials
+        const int prev_tail_row = __shfl_up_sync(kFull, tail_row, 1);
+        const bool start = lane == 0 || !single || prev_tail_row != tail_row;
+        const unsigned smask = __ballot_sync(kFull, start);
+        const int seg0 = 31 - __clz(smask & (0xffffffffu >> (31 - lane)));
+        float v = tail;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-            const float vu = __shfl_up_sync(kFull, v, off);
-            const int ru = __shfl_up_sync(kFull, rr, off);
-            if (lane >= off && ru == rr) v += vu;
+            const float t = __shfl_up_sync(kFull, v, off);
+            if (lane - off >= seg0) v += t;
         }
-        if (rr == carry_row) v += carry;
-        const int rn = __shfl_down_sync(kFull, rr, 1);
-        const bool tail = lane == 31 || rn != rr;
-        const float v31 = __shfl_sync(kFull, v, 31);
-        const int r31 = __shfl_sync(kFull, rr, 31);
-        if (tail && lane != 31 && rr >= 0) coo_put<ATOMIC_ALL>(a.y, rr, a.alpha * v, first_row);
-        carry = v31;
-        carry_row = r31;
+        const float prev_v = __shfl_up_sync(kFull, v, 1);
+        if (!single) {
+            const float cin = (lane > 0 && prev_tail_row == head_row) ? prev_v : 0.f;
+            coo_red(a.y, head_row, a.alpha * (head + cin));
+        }
+        const int next_head = __shfl_down_sync(kFull, head_row, 1);
+        if (lane < 31 && next_head != tail_row) coo_red(a.y, tail_row, a.alpha * v);
+        carry = __shfl_sync(kFull, v, 31);
+        carry_row = __shfl_sync(kFull, tail_row, 31);
+        if (carry_row == kCooNoRow) carry_row = -1;
     }
-    if (carry_row >= 0 && lane == 0) atomicAdd(a.y + carry_row, a.alpha * carry);
+    if (carry_row >= 0 && lane == 0) coo_red(a.y, carry_row, a.alpha * carry);
+}
+
+__device__ __forceinline__ void coo_cta(const CooArgs& a, int cta, int ncta, char*)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    const long long nchunks = ((long long)a.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
+    long long b, e;
+    cta_share(nchunks, 1, cta, ncta, b, e);
+    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) coo_warp_chunk(a, ch * kCooWarpNnz, pe, pl);
 }
 
 // ---------------------------------------------------------------------------
@@ -476,33 +701,38 @@ __device__ __forceinline__ void coo_tile(const CooArgs& a, int tile, char*)
 // reads 512 contiguous bytes per load. x blocks are 16-byte aligned float4.
 // ---------------------------------------------------------------------------
 template <int BW4, int BH, bool ATOMIC>
-__device__ __forceinline__ void b4ell_tile(const B4ellArgs& a, int tile, char*)
+__device__ __forceinline__ void b4ell_cta(const B4ellArgs& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int r = tile * kBlock + threadIdx.x;
-    if (r >= a.nbrow) return;
-    float acc[BH];
-#pragma unroll
-    for (int h = 0; h < BH; h++) acc[h] = 0.f;
+    long long b, e;
+    cta_share(a.nbrow, 1, cta, ncta, b, e);
     const size_t colsz = (size_t)a.f4 * BW4 * BH;
-    const float* base = a.data + (size_t)r * 4;
-    for (int j = 0; j < a.ellnum; j++) {
-        const int c4 = ld_stream_i(a.col + (size_t)j * a.len + r, pe);
-        const float* bj = base + (size_t)j * colsz;
+    for (long long r = b + threadIdx.x; r < e; r += kBlock) {
+        float acc[BH];
 #pragma unroll
-        for (int w4 = 0; w4 < BW4; w4++) {
-            const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+        for (int h = 0; h < BH; h++) acc[h] = 0.f;
+        const float* base = a.data + (size_t)r * 4;
+#pragma unroll 2
+        for (int j = 0; j < a.ellnum; j++) {
+            const int c4 = ld_stream_i(a.col + (size_t)j * a.len + r, pe);
+            const float* bj = base + (size_t)j * colsz;
+            float4 v[BW4][BH];
 #pragma unroll
-            for (int h = 0; h < BH; h++) {
-                const float4 v = ld_stream_f4(bj + (size_t)w4 * a.f4 * BH + (size_t)h * a.f4, pe);
-                acc[h] = dot4(v, xv, acc[h]);
+            for (int w4 = 0; w4 < BW4; w4++)
+#pragma unroll
+                for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bj + (size_t)w4 * a.f4 * BH + (size_t)h * a.f4, pe);
+#pragma unroll
+            for (int w4 = 0; w4 < BW4; w4++) {
+                const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+#pragma unroll
+                for (int h = 0; h < BH; h++) acc[h] = dot4(v[w4][h], xv, acc[h]);
             }
         }
-    }
 #pragma unroll
-    for (int h = 0; h < BH; h++) {
-        const int row = r * BH + h;
-        if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+        for (int h = 0; h < BH; h++) {
+            const long long row = r * BH + h;
+            if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+        }
     }
 }
 
@@ -512,38 +742,43 @@ __device__ __forceinline__ void b4ell_tile(const B4ellArgs& a, int tile, char*)
 // is 512 contiguous bytes.
 // ---------------------------------------------------------------------------
 template <int BW4, int BH, bool ATOMIC>
-__device__ __forceinline__ void sbell_tile(const SbellArgs& a, int tile, char*)
+__device__ __forceinline__ void sbell_cta(const SbellArgs& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int r = tile * kBlock + threadIdx.x;
-    if (r >= a.nbrow) return;
+    long long b, e;
+    cta_share(a.nbrow, 32, cta, ncta, b, e);
     const int sh = a.slice_height;
-    const int s = r / sh, lr = r - s * sh;
-    const int cs = a.slice_ptr[s];
-    const int width = (a.slice_ptr[s + 1] - cs) / sh;
-    float acc[BH];
-#pragma unroll
-    for (int h = 0; h < BH; h++) acc[h] = 0.f;
     const size_t bs = (size_t)BW4 * 4 * BH;
     const size_t colsz = (size_t)sh * BW4 * BH * 4, hsz = (size_t)sh * 4, w4sz = (size_t)sh * BH * 4;
-    const float* base = a.data + (size_t)cs * bs + (size_t)lr * 4;
-    for (int j = 0; j < width; j++) {
-        const int c4 = ld_stream_i(a.col + (size_t)cs + lr + (size_t)j * sh, pe);
-        const float* bj = base + (size_t)j * colsz;
+    for (long long r = b + threadIdx.x; r < e; r += kBlock) {
+        const int s = (int)(r / sh), lr = (int)(r - (long long)s * sh);
+        const int cs = a.slice_ptr[s];
+        const int width = (a.slice_ptr[s + 1] - cs) / sh;
+        float acc[BH];
 #pragma unroll
-        for (int w4 = 0; w4 < BW4; w4++) {
-            const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+        for (int h = 0; h < BH; h++) acc[h] = 0.f;
+        const float* base = a.data + (size_t)cs * bs + (size_t)lr * 4;
+#pragma unroll 2
+        for (int j = 0; j < width; j++) {
+            const int c4 = ld_stream_i(a.col + (size_t)cs + lr + (size_t)j * sh, pe);
+            const float* bj = base + (size_t)j * colsz;
+            float4 v[BW4][BH];
 #pragma unroll
-            for (int h = 0; h < BH; h++) {
-                const float4 v = ld_stream_f4(bj + (size_t)w4 * w4sz + (size_t)h * hsz, pe);
-                acc[h] = dot4(v, xv, acc[h]);
+            for (int w4 = 0; w4 < BW4; w4++)
+#pragma unroll
+                for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bj + (size_t)w4 * w4sz + (size_t)h * hsz, pe);
+#pragma unroll
+            for (int w4 = 0; w4 < BW4; w4++) {
+                const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+#pragma unroll
+                for (int h = 0; h < BH; h++) acc[h] = dot4(v[w4][h], xv, acc[h]);
             }
         }
-    }
 #pragma unroll
-    for (int h = 0; h < BH; h++) {
-        const int row = r * BH + h;
-        if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+        for (int h = 0; h < BH; h++) {
+            const long long row = r * BH + h;
+            if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+        }
     }
 }
 
@@ -555,42 +790,49 @@ __device__ __forceinline__ void sbell_tile(const SbellArgs& a, int tile, char*)
 // (the reference reduces in __local memory per 128-thread group).
 // ---------------------------------------------------------------------------
 template <int BW4, int BH, int T, bool ATOMIC>
-__device__ __forceinline__ void b4csr_tile(const B4csrArgs& a, int tile, char*)
+__device__ __forceinline__ void b4csr_cta(const B4csrArgs& a, int cta, int ncta, char*)
 {
+    constexpr int kRowsPerPass = kBlock / T;
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    const int g = (tile * kBlock + threadIdx.x) / T;
+    long long b, e;
+    cta_share(a.nbrow, 1, cta, ncta, b, e);
     const int l = threadIdx.x % T;
-    const bool active = g < a.nbrow;
-    float acc[BH];
+    const size_t plane_w4 = (size_t)a.len * BH;
+    for (long long pass = b; pass < e; pass += kRowsPerPass) {
+        const long long g = pass + threadIdx.x / T;
+        const bool active = g < e;
+        float acc[BH];
 #pragma unroll
-    for (int h = 0; h < BH; h++) acc[h] = 0.f;
-    if (active) {
-        const int s = a.row_ptr[g], e = a.row_ptr[g + 1];
-        const size_t plane_w4 = (size_t)a.len * BH;
-        for (int i = s + l; i < e; i += T) {
-            const int c4 = ld_stream_i(a.col + i, pe);
-            const float* bi = a.data + (size_t)i * 4;
+        for (int h = 0; h < BH; h++) acc[h] = 0.f;
+        if (active) {
+            const int s = a.row_ptr[g], en = a.row_ptr[g + 1];
+            for (int i = s + l; i < en; i += T) {
+                const int c4 = ld_stream_i(a.col + i, pe);
+                const float* bi = a.data + (size_t)i * 4;
+                float4 v[BW4][BH];
 #pragma unroll
-            for (int w4 = 0; w4 < BW4; w4++) {
-                const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+                for (int w4 = 0; w4 < BW4; w4++)
 #pragma unroll
-                for (int h = 0; h < BH; h++) {
-                    const float4 v = ld_stream_f4(bi + w4 * plane_w4 + (size_t)h * a.len, pe);
-                    acc[h] = dot4(v, xv, acc[h]);
+                    for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bi + w4 * plane_w4 + (size_t)h * a.len, pe);
+#pragma unroll
+                for (int w4 = 0; w4 < BW4; w4++) {
+                    const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
+#pragma unroll
+                    for (int h = 0; h < BH; h++) acc[h] = dot4(v[w4][h], xv, acc[h]);
                 }
             }
         }
-    }
-#pragma unroll
-    for (int h = 0; h < BH; h++) {
-#pragma unroll
-        for (int off = T / 2; off > 0; off >>= 1) acc[h] += __shfl_xor_sync(kFull, acc[h], off, T);
-    }
-    if (active && l == 0) {
 #pragma unroll
         for (int h = 0; h < BH; h++) {
-            const int row = g * BH + h;
-            if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+#pragma unroll
+            for (int off = T / 2; off > 0; off >>= 1) acc[h] += __shfl_xor_sync(kFull, acc[h], off, T);
+        }
+        if (active && l == 0) {
+#pragma unroll
+            for (int h = 0; h < BH; h++) {
+                const long long row = g * BH + h;
+                if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+            }
         }
     }
 }

@@ -5,6 +5,9 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
 #include "clspmv_b200.h"
 #include "kernels.cuh"
 #include "api_internal.h"
@@ -50,36 +53,44 @@ template <bool A>
 __global__ void __launch_bounds__(kBlock) k_dia(DiaArgs a)
 {
     __shared__ __align__(16) char smem[kDiaSmemBytes];
-    dia_tile<A>(a, blockIdx.x, smem);
+    dia_cta<A>(a, blockIdx.x, gridDim.x, smem);
 }
 
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgs a)
 {
     __shared__ __align__(16) char smem[kBdiaSmemBytes];
-    bdia_tile<A>(a, blockIdx.x, smem);
+    bdia_cta<A>(a, blockIdx.x, gridDim.x, smem);
 }
 
 template <bool A>
-__global__ void __launch_bounds__(kBlock) k_ell(EllArgs a) { ell_tile<A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_bdia_win(BdiaArgs a, int win_cap)
+{
+    extern __shared__ __align__(16) char dsmem[];
+    const int win = a.nband * (kBdiaRowsPerPass - 1) + a.bptr[a.nband];
+    if (win <= win_cap) bdia_window_cta<A>(a, win, blockIdx.x, gridDim.x, dsmem);
+    else bdia_cta<A>(a, blockIdx.x, gridDim.x, dsmem);
+}
 
 template <bool A>
-__global__ void __launch_bounds__(kBlock) k_sell(SellArgs a) { sell_tile<A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_ell(EllArgs a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+
+template <int Q, bool A>
+__global__ void __launch_bounds__(kBlock) k_sell(SellArgs a) { sell_cta<Q, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <bool A>
-__global__ void __launch_bounds__(kBlock) k_sell_scalar(SellArgs a) { sell_tile_scalar<A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_sell_rows(SellArgs a) { sell_rows_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <bool A>
-__global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_tile<A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <int T, bool A>
-__global__ void __launch_bounds__(kBlock) k_csr_vector(CsrArgs a) { csr_vector_tile<T, A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_csr_vector(CsrArgs a) { csr_vector_cta<T, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_merge(CsrArgs a, const int* __restrict__ tc)
 {
     extern __shared__ __align__(16) char dsmem[];
-    csr_merge_tile<A>(a, tc, blockIdx.x, dsmem);
+    csr_merge_tile(a, tc, blockIdx.x, dsmem);
 }
 
 __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, const int* __restrict__ row_ptr, int* tc, int ntiles)
@@ -89,17 +100,47 @@ __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, co
     csr_merge_search(rows, nnz, row_ptr, (long long)t * kMergeTile, tc + 2 * t);
 }
 
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_coo(CooArgs a) { coo_tile<A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_coo(CooArgs a) { coo_cta(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <int BW4, int BH, bool A>
-__global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgs a) { b4ell_tile<BW4, BH, A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgs a) { b4ell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <int BW4, int BH, bool A>
-__global__ void __launch_bounds__(kBlock) k_sbell(SbellArgs a) { sbell_tile<BW4, BH, A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_sbell(SbellArgs a) { sbell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <int BW4, int BH, int T, bool A>
-__global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgs a) { b4csr_tile<BW4, BH, T, A>(a, blockIdx.x, nullptr); }
+__global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgs a) { b4csr_cta<BW4, BH, T, A>(a, blockIdx.x, gridDim.x, nullptr); }
+
+// CTAs that fit on the device at once for `kernel` (SM count x resident
+// CTAs per SM), cached per kernel.
+int resident_ctas(const void* kernel, int smem_bytes)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(kernel);
+    if (it != cache.end()) return it->second;
+    int dev = 0, nsm = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlock, smem_bytes) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        per = 1;
+    }
+    const int n = nsm * per;
+    cache[kernel] = n;
+    return n;
+}
+
+// Grid for a persistent launch: all resident CTAs, but no more CTAs than
+// passes of work.
+template <class K>
+unsigned persistent_grid(K kernel, long long units, long long units_per_pass, int smem_bytes = 0)
+{
+    const long long passes = (units + units_per_pass - 1) / units_per_pass;
+    const long long res = resident_ctas(reinterpret_cast<const void*>(kernel), smem_bytes);
+    return (unsigned)std::max(1LL, std::min(passes, res));
+}
 
 // ---------------------------------------------------------------------------
 // Shape dispatch helpers.
@@ -195,7 +236,7 @@ int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float
     if (m->dia_num > 0 && (!m->dia_offsets || !m->dia_data)) return CLSPMV_ERR_ARG;
     if ((m->dia_length_aligned & 3) || !aligned16(m->dia_data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
     DiaArgs a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, m->dia_data, x, y, alpha, beta};
-    k_dia<false><<<grid_for(rows, kDiaRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    k_dia<false><<<persistent_grid(k_dia<false>, rows, kDiaRowsPerPass), kBlock, 0, S(stream)>>>(a);
     return after_launch(1);
 }
 
@@ -207,7 +248,27 @@ int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, flo
     if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data)) return CLSPMV_ERR_ARG;
     if ((m->bdia_length_aligned & 3) || !aligned16(m->bdia_data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
     BdiaArgs a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, m->bdia_data, x, y, alpha, beta};
-    k_bdia<false><<<grid_for(rows, kBdiaRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    // Window-set size for the shared-memory kernel. The diagonal count
+    // bptr[nband] lives on the device; the host bounds it with the DIA
+    // acceptance rule (a converted matrix has (D-1)*len < 2*nnz,
+    // include/matrix_storage.h:972) and the kernel re-checks the true count,
+    // taking the per-band path when the window set does not fit.
+    const long long len = std::max(1, m->bdia_length_aligned);
+    const long long dbound = (2LL * std::max(0, m->matinfo.nnz) - 1) / len + 1;
+    const long long win = (long long)m->bdia_band_num * (kBdiaRowsPerPass - 1) + dbound;
+    const long long smem = 2 * win * (long long)sizeof(float);
+    cudaStream_t st = S(stream);
+    if (m->bdia_band_num > 0 && smem <= kBdiaWinMaxSmem) {
+        static std::once_flag once;
+        static int attr_rc = CLSPMV_OK;
+        std::call_once(once, [] {
+            attr_rc = cuda_status(cudaFuncSetAttribute(k_bdia_win<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBdiaWinMaxSmem));
+        });
+        if (attr_rc) return attr_rc;
+        k_bdia_win<false><<<persistent_grid(k_bdia_win<false>, rows, kBdiaRowsPerPass, (int)smem), kBlock, (size_t)smem, st>>>(a, (int)win);
+        return after_launch(1);
+    }
+    k_bdia<false><<<persistent_grid(k_bdia<false>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
@@ -220,7 +281,7 @@ int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float
     if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned16(m->ell_data) || rows > m->ell_height_aligned)
         return CLSPMV_ERR_ALIGN;
     EllArgs a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, m->ell_data, x, y, alpha, beta};
-    k_ell<false><<<grid_for(rows, kEllRowsPerTile), kBlock, 0, S(stream)>>>(a);
+    k_ell<false><<<persistent_grid(k_ell<false>, rows, kEllRowsPerPass), kBlock, 0, S(stream)>>>(a);
     return after_launch(1);
 }
 
@@ -232,12 +293,19 @@ int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, flo
     if (rows <= 0) return CLSPMV_OK;
     if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
     SellArgs a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data, x, y, alpha, beta};
-    if ((sh & 3) == 0 && aligned16(m->sell_col_id) && aligned16(m->sell_data)) {
-        const long long quads = (long long)m->sell_slice_num * (sh / 4);
-        k_sell<false><<<grid_for(quads, kBlock), kBlock, 0, S(stream)>>>(a);
-    } else {
-        k_sell_scalar<false><<<grid_for(rows, kBlock), kBlock, 0, S(stream)>>>(a);
+    cudaStream_t st = S(stream);
+    const bool vec = aligned16(m->sell_col_id) && aligned16(m->sell_data);
+    if (vec && (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
+        int rc = prescale(y, rows, beta, st);
+        if (rc) return rc;
+        a.beta = 1.0f;
+        return dispatch_lanes(sh / 4, [&](auto q) {
+            constexpr int Q = decltype(q)::value;
+            k_sell<Q, false><<<persistent_grid(k_sell<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a);
+            return after_launch(1);
+        });
     }
+    k_sell_rows<false><<<persistent_grid(k_sell_rows<false>, rows, kBlock), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
@@ -248,7 +316,7 @@ int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y
     if (rows <= 0) return CLSPMV_OK;
     if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
     CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
-    k_csr_scalar<false><<<grid_for(rows, kBlock), kBlock, 0, S(stream)>>>(a);
+    k_csr_scalar<false><<<persistent_grid(k_csr_scalar<false>, rows, kBlock), kBlock, 0, S(stream)>>>(a);
     return after_launch(1);
 }
 
@@ -260,10 +328,10 @@ int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y
     if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
     if (tpr == 0) tpr = pow2_lanes((double)m->matinfo.nnz / rows, 2, 32);
     CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
-    const unsigned grid = grid_for((long long)rows * tpr, kBlock);
     cudaStream_t st = S(stream);
     return dispatch_lanes(tpr, [&](auto t) {
-        k_csr_vector<decltype(t)::value, false><<<grid, kBlock, 0, st>>>(a);
+        constexpr int T = decltype(t)::value;
+        k_csr_vector<T, false><<<persistent_grid(k_csr_vector<T, false>, rows, kBlock / T), kBlock, 0, st>>>(a);
         return after_launch(1);
     });
 }
@@ -293,14 +361,8 @@ int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* m, const int* tc, const floa
     int rc = prescale(y, rows, beta, st);
     if (rc) return rc;
     const int ntiles = clspmv_csr_merge_tiles(rows, m->matinfo.nnz);
-    static bool attr_set = false;
-    if (!attr_set) {
-        rc = cuda_status(cudaFuncSetAttribute(k_csr_merge<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMergeSmemBytes));
-        if (rc) return rc;
-        attr_set = true;
-    }
     CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, 1.0f};
-    k_csr_merge<false><<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
+    k_csr_merge<<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
     return after_launch(1);
 }
 
@@ -314,8 +376,9 @@ int clspmv_coo_spmv_f32(const clspmv_coo_f32* m, const float* x, float* y, float
     if (rc) return rc;
     if (m->matinfo.nnz <= 0) return CLSPMV_OK;
     if (!m->coo_row_id || !m->coo_col_id || !m->coo_data) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned16(m->coo_data)) return CLSPMV_ERR_ALIGN;
     CooArgs a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, m->coo_data, x, y, alpha};
-    k_coo<false><<<grid_for(m->matinfo.nnz, kCooTileNnz), kBlock, 0, st>>>(a);
+    k_coo<<<persistent_grid(k_coo, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
@@ -336,7 +399,8 @@ int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* m, const float* x, float* y, f
                       m->b4ell_float4_aligned, m->b4ell_col_id, m->b4ell_data, x, y, alpha, beta};
     cudaStream_t st = S(stream);
     return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
-        k_b4ell<decltype(bw4)::value, decltype(bh)::value, false><<<grid_for(a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+        k_b4ell<BW4, BH, false><<<persistent_grid(k_b4ell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
         return after_launch(1);
     });
 }
@@ -353,7 +417,8 @@ int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* m, const float* x, float* y, f
                       m->sbell_slice_ptr, m->sbell_col_id, m->sbell_data, x, y, alpha, beta};
     cudaStream_t st = S(stream);
     return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
-        k_sbell<decltype(bw4)::value, decltype(bh)::value, false><<<grid_for(a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+        k_sbell<BW4, BH, false><<<persistent_grid(k_sbell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
         return after_launch(1);
     });
 }
@@ -373,8 +438,9 @@ int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, f
     return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
         return dispatch_lanes(lanes, [&](auto t) {
             constexpr int T = decltype(t)::value;
-            k_b4csr<decltype(bw4)::value, decltype(bh)::value, T, false>
-                <<<grid_for((long long)a.nbrow * T, kBlock), kBlock, 0, st>>>(a);
+            constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+            k_b4csr<BW4, BH, T, false>
+                <<<persistent_grid(k_b4csr<BW4, BH, T, false>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
             return after_launch(1);
         });
     });
