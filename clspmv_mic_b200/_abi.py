@@ -83,6 +83,19 @@ class Sbell(C.Structure):
                 ("sbell_slice_ptr", VP), ("sbell_col_id", VP), ("sbell_data", VP)]
 
 
+COCKTAIL_PARTS = [("bdia", "bdia"), ("dia", "dia"), ("sbell", "sbell"), ("bell", "b4ell"), ("bcsr", "b4csr"),
+                  ("sell", "sell"), ("ell", "ell"), ("csr", "csr"), ("coo", "coo")]
+
+
+class Cocktail(C.Structure):
+    """cocktail<int,int,float> (include/analyze.h:105-144 of clSpMV)."""
+    _fields_ = ([(f"ifuse{n}", C.c_bool) for n in ("bdia", "dia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo")] +
+                [(f"{n}_meth_num", I32) for n in ("bdia", "dia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo")] +
+                [("csr_group_num", I32), ("coo_group_num", I32), ("mat_width", I32), ("mat_height", I32), ("mat_nnz", I32),
+                 ("bdia", Bdia), ("dia", Dia), ("sbell", Sbell), ("bell", B4ell), ("bcsr", B4csr), ("sell", Sell),
+                 ("ell", Ell), ("csr", Csr), ("coo", Coo)])
+
+
 def _n_bdia_data(s):
     if s.bdia_band_num <= 0:
         return 0
@@ -186,8 +199,10 @@ def _declare(lib):
         "clspmv_b4ell_spmv_f32": (I32, [S["b4ell"], VP, VP, f32, f32, VP]),
         "clspmv_sbell_spmv_f32": (I32, [S["sbell"], VP, VP, f32, f32, VP]),
         "clspmv_b4csr_spmv_f32": (I32, [S["b4csr"], VP, VP, f32, f32, VP]),
+        "clspmv_analyze_matrix_f32": (I32, [S["coo"], P(Cocktail), C.c_char_p, f32, I32, I32]),
+        "clspmv_free_cocktail_f32": (None, [P(Cocktail)]),
     }
-    for fmt in ("csr", "dia", "bdia", "ell", "bcsr", "bell", "b4csr", "b4ell", "sbell"):
+    for fmt in ("csr", "dia", "bdia", "ell", "sell", "bcsr", "bell", "b4csr", "b4ell", "sbell", "coo"):
         sigs[f"clspmv_{fmt}2coo_f32"] = (I32, [S[fmt], S["coo"]])
     for fmt in FORMATS:
         sigs[f"clspmv_free_{fmt}_f32"] = (None, [S[fmt]])

@@ -1,0 +1,79 @@
+"""Cocktail partitioning (analyze_matrix) and the partitioned matrix.
+
+analyze(coo, table_dir) runs the library's restatement of clSpMV's
+analyze_matrix (src/analyze.cpp) through the C ABI and returns a
+CocktailMatrix: the nine part slots of cocktail<int,int,float> as
+HostMatrix views (None for unused parts) plus the chosen variants.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+from . import _abi
+from ._abi import COCKTAIL_PARTS, check, lib
+from .formats import HostMatrix
+
+
+class CocktailMatrix:
+    def __init__(self, struct: _abi.Cocktail, owner: str = "lib", releaser=None):
+        self.struct = struct
+        self._owner = owner
+        self._releaser = releaser
+
+    def __del__(self):
+        if getattr(self, "_owner", None) == "lib":
+            try:
+                lib().clspmv_free_cocktail_f32(C.byref(self.struct))
+            except Exception:
+                pass
+        elif getattr(self, "_releaser", None) is not None:
+            try:
+                self._releaser(self.struct)
+            except Exception:
+                pass
+        self._owner = None
+        self._releaser = None
+
+    def uses(self, part: str) -> bool:
+        return bool(getattr(self.struct, f"ifuse{part}"))
+
+    def part(self, part: str):
+        """HostMatrix view of one part (no copy), or None when unused."""
+        if not self.uses(part):
+            return None
+        fmt = dict(COCKTAIL_PARTS)[part]
+        return HostMatrix(fmt, getattr(self.struct, part))
+
+    def parts(self) -> dict:
+        return {p: self.part(p) for p, _ in COCKTAIL_PARTS if self.uses(p)}
+
+    def summary(self) -> dict:
+        s = self.struct
+        out = {"shape": (s.mat_height, s.mat_width), "nnz": s.mat_nnz}
+        for p, _ in COCKTAIL_PARTS:
+            if self.uses(p):
+                m = self.part(p)
+                out[p] = {"nnz": m.nnz, "meth": getattr(s, f"{p}_meth_num")}
+        out["csr_group_num"] = s.csr_group_num
+        out["coo_group_num"] = s.coo_group_num
+        return out
+
+
+def analyze(coo: HostMatrix, table_dir: str | os.PathLike | None = None, dia_priority_multiplier: float = 1.0,
+            estimate_flat_partial: bool = True, estimate_flat_full: bool = False) -> CocktailMatrix:
+    """analyze_matrix (src/analyze.cpp:3714-3900): tables from
+    <table_dir>/benchmark/*.ben (default: $CLSPMVPATH, then the package's
+    tables)."""
+    if table_dir is None:
+        table_dir = os.environ.get("CLSPMVPATH")
+    if table_dir is None:
+        from .tables import ensure_default_tables
+        table_dir = ensure_default_tables()
+    out = _abi.Cocktail()
+    rc = lib().clspmv_analyze_matrix_f32(C.byref(coo.struct), C.byref(out), str(table_dir).encode(),
+                                         dia_priority_multiplier, int(estimate_flat_partial), int(estimate_flat_full))
+    m = CocktailMatrix(out, owner="lib" if rc == 0 else None)
+    check(rc, "analyze_matrix")
+    return m

@@ -6,6 +6,8 @@
 // cited in clspmv_b200.h next to each declaration.
 #include <cstddef>
 #include <new>
+#include <cstring>
+#include <cstdlib>
 #include "clspmv_b200.h"
 #include "matrix_storage.h"
 
@@ -236,10 +238,31 @@ INVERSE(clspmv_bdia2coo_f32, clspmv_bdia_f32, bdia_t, bdia2coo)
 INVERSE(clspmv_ell2coo_f32, clspmv_ell_f32, ell_t, ell2coo)
 INVERSE(clspmv_bcsr2coo_f32, clspmv_bcsr_f32, bcsr_t, bcsr2coo)
 INVERSE(clspmv_bell2coo_f32, clspmv_bell_f32, bell_t, bell2coo)
+INVERSE(clspmv_sell2coo_f32, clspmv_sell_f32, sell_t, sell2coo)
 INVERSE(clspmv_b4csr2coo_f32, clspmv_b4csr_f32, b4csr_t, b4csr2coo)
 INVERSE(clspmv_b4ell2coo_f32, clspmv_b4ell_f32, b4ell_t, b4ell2coo)
 INVERSE(clspmv_sbell2coo_f32, clspmv_sbell_f32, sbell_t, sbell2coo)
 #undef INVERSE
+
+int clspmv_coo2coo_f32(const clspmv_coo_f32* src, clspmv_coo_f32* dst)
+{
+    if (!coo_ok(src) || !dst) return CLSPMV_ERR_ARG;
+    const size_t n = (size_t)src->matinfo.nnz;
+    dst->matinfo = src->matinfo;
+    dst->coo_row_id = (int*)malloc(sizeof(int) * (n ? n : 1));
+    dst->coo_col_id = (int*)malloc(sizeof(int) * (n ? n : 1));
+    dst->coo_data = (float*)malloc(sizeof(float) * (n ? n : 1));
+    if (!dst->coo_row_id || !dst->coo_col_id || !dst->coo_data) {
+        clspmv_free_coo_f32(dst);
+        return CLSPMV_ERR_ALLOC;
+    }
+    if (n) {
+        memcpy(dst->coo_row_id, src->coo_row_id, n * sizeof(int));
+        memcpy(dst->coo_col_id, src->coo_col_id, n * sizeof(int));
+        memcpy(dst->coo_data, src->coo_data, n * sizeof(float));
+    }
+    return CLSPMV_OK;
+}
 
 void clspmv_free_coo_f32(clspmv_coo_f32* m) { if (m) free_coo_matrix(*as_tmpl<coo_t>(m)); }
 void clspmv_free_csr_f32(clspmv_csr_f32* m) { if (m) free_csr_matrix(*as_tmpl<csr_t>(m)); }

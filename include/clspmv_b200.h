@@ -27,6 +27,9 @@
 
 #include <stddef.h>
 #include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -142,6 +145,28 @@ typedef struct {
     int* sbell_slice_ptr; int* sbell_col_id; float* sbell_data;
 } clspmv_sbell_f32;
 
+/* cocktail<int,int,float>: include/analyze.h:105-144 of clSpMV. The result
+ * of the Cocktail partitioner: which of the nine formats are used, the
+ * kernel variant / work-group count the tables chose for each, and the
+ * parts themselves (host arrays after analysis, device arrays after
+ * clspmv_cocktail_upload). */
+typedef struct {
+    bool ifusebdia, ifusedia, ifusesbell, ifusebell, ifusebcsr, ifusesell, ifuseell, ifusecsr, ifusecoo;
+    int bdia_meth_num, dia_meth_num, sbell_meth_num, bell_meth_num, bcsr_meth_num, sell_meth_num, ell_meth_num,
+        csr_meth_num, coo_meth_num;
+    int csr_group_num, coo_group_num;
+    int mat_width, mat_height, mat_nnz;
+    clspmv_bdia_f32 bdia;
+    clspmv_dia_f32 dia;
+    clspmv_sbell_f32 sbell;
+    clspmv_b4ell_f32 bell;
+    clspmv_b4csr_f32 bcsr;
+    clspmv_sell_f32 sell;
+    clspmv_ell_f32 ell;
+    clspmv_csr_f32 csr;
+    clspmv_coo_f32 coo;
+} clspmv_cocktail_f32;
+
 /* ------------------------------------------------------------------------ */
 /* Library                                                                   */
 /* ------------------------------------------------------------------------ */
@@ -197,15 +222,18 @@ int clspmv_coo2sbell_f32(const clspmv_coo_f32* src, clspmv_sbell_f32* dst,
 
 /* Inverse converters (allocate dst arrays). csr2coo :1238-1266, dia2coo
  * :825-863, bdia2coo :1136-1181, ell2coo :1309-1337, bcsr2coo :1545-1589,
- * bell2coo :1900-1938. The b4csr/b4ell/sbell inverses have no reference
- * counterpart; they exist for round-trip checks of the block layouts. */
+ * bell2coo :1900-1938. The sell/b4csr/b4ell/sbell inverses have no
+ * reference counterpart; they exist for round-trip checks of the layouts. */
 int clspmv_csr2coo_f32(const clspmv_csr_f32* src, clspmv_coo_f32* dst);
 int clspmv_dia2coo_f32(const clspmv_dia_f32* src, clspmv_coo_f32* dst);
 int clspmv_bdia2coo_f32(const clspmv_bdia_f32* src, clspmv_coo_f32* dst);
 int clspmv_ell2coo_f32(const clspmv_ell_f32* src, clspmv_coo_f32* dst);
 int clspmv_bcsr2coo_f32(const clspmv_bcsr_f32* src, clspmv_coo_f32* dst);
 int clspmv_bell2coo_f32(const clspmv_bell_f32* src, clspmv_coo_f32* dst);
+int clspmv_sell2coo_f32(const clspmv_sell_f32* src, clspmv_coo_f32* dst);
 int clspmv_b4csr2coo_f32(const clspmv_b4csr_f32* src, clspmv_coo_f32* dst);
+/* Deep copy of a COO matrix (malloc'ed arrays). */
+int clspmv_coo2coo_f32(const clspmv_coo_f32* src, clspmv_coo_f32* dst);
 int clspmv_b4ell2coo_f32(const clspmv_b4ell_f32* src, clspmv_coo_f32* dst);
 int clspmv_sbell2coo_f32(const clspmv_sbell_f32* src, clspmv_coo_f32* dst);
 
@@ -320,6 +348,20 @@ int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* dev, const float* x, float* y,
  * kernels/spmv_bcsr.cl, driver src/spmv_bcsr.cpp:224-278. */
 int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* dev, const float* x, float* y,
                           float alpha, float beta, clspmv_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Cocktail partitioning (src/analyze.cpp of clSpMV).                        */
+/* ------------------------------------------------------------------------ */
+
+/* analyze_matrix (src/analyze.cpp:3714-3900) with the benchmark tables read
+ * from <table_dir>/benchmark/<fmt>.ben (NULL: $CLSPMVPATH, as the reference).
+ * `coo` must be sorted by (row, col). `out` is initialised here; release it
+ * with clspmv_free_cocktail_f32. CLSPMV_ERR_ARG when a table is missing or
+ * empty (the reference segfaults there). */
+int clspmv_analyze_matrix_f32(const clspmv_coo_f32* coo, clspmv_cocktail_f32* out, const char* table_dir,
+                              float dia_priority_multiplier, int estimate_flat_partial, int estimate_flat_full);
+/* free_cocktail (include/analyze.h:183-205) */
+void clspmv_free_cocktail_f32(clspmv_cocktail_f32* m);
 
 /* Number of kernels this library launched since load (all entry points). */
 long long clspmv_launch_count(void);

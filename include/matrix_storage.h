@@ -841,6 +841,29 @@ void bell2coo(bell_matrix<dimType, dataType>* source, coo_matrix<dimType, dataTy
     clspmv_detail::coo_from_triplets(dest, source->matinfo, r, c, v, false);
 }
 
+/* sell2coo: no reference counterpart; inverse of coo2sell (padding slots
+ * hold 0 and are dropped). */
+template <class dimType, class dataType>
+void sell2coo(const sell_matrix<dimType, dataType>* s, coo_matrix<dimType, dataType>* dest)
+{
+    std::vector<dimType> r, c;
+    std::vector<dataType> v;
+    const dimType sh = (dimType)s->sell_slice_height;
+    for (dimType sl = 0; sl < s->sell_slice_num; sl++) {
+        const size_t st = (size_t)s->sell_slice_ptr[sl];
+        const dimType wdt = (s->sell_slice_ptr[sl + 1] - s->sell_slice_ptr[sl]) / sh;
+        for (dimType lr = 0; lr < sh; lr++) {
+            const dimType row = sl * sh + lr;
+            if (row >= s->matinfo.height) break;
+            for (dimType k = 0; k < wdt; k++) {
+                const size_t i = st + (size_t)k * sh + lr;
+                if (s->sell_data[i] != (dataType)0) { r.push_back(row); c.push_back(s->sell_col_id[i]); v.push_back(s->sell_data[i]); }
+            }
+        }
+    }
+    clspmv_detail::coo_from_triplets(dest, s->matinfo, r, c, v, false);
+}
+
 /* b4csr2coo / b4ell2coo / sbell2coo: no reference counterpart; inverse of
  * the block layouts above, used for round-trip checks. */
 template <class dimType, class dataType>

@@ -12,6 +12,7 @@
 #include "matrix_storage.h"
 #include "spmv_serial.h"
 #include "util.h"
+#include "analyze.h"
 #include "../include/clspmv_b200.h"
 
 typedef coo_matrix<int, float> coo_t;
@@ -73,6 +74,16 @@ void ref_sell_spmv(clspmv_sell_f32* m, float* x, float* y, int n) { sell_spmv(R<
 void ref_sbell_spmv(clspmv_sbell_f32* m, float* x, float* y, int n) { sbell_spmv(R<sbell_t>(m), x, y, n); }
 void ref_bcsr_spmv(clspmv_bcsr_f32* m, float* x, float* y, int n) { bcsr_spmv(R<bcsr_t>(m), x, y, n); }
 void ref_bell_spmv(clspmv_bell_f32* m, float* x, float* y, int n) { bell_spmv(R<bell_t>(m), x, y, n); }
+// analyze_matrix (src/analyze.cpp:3714-3900) with CLSPMVPATH pointing at
+// `table_root` (it reads <table_root>/benchmark/*.ben).
+void ref_analyze_matrix(clspmv_coo_f32* m, clspmv_cocktail_f32* out, const char* table_root, float mult, int partial, int full)
+{
+    setenv("CLSPMVPATH", table_root, 1);
+    cocktail<int, int, float>* c = reinterpret_cast<cocktail<int, int, float>*>(out);
+    init_cocktail(*c);
+    analyze_matrix(*R<coo_t>(m), *c, mult, partial != 0, full != 0);
+}
+static_assert(sizeof(clspmv_cocktail_f32) == sizeof(cocktail<int, int, float>), "cocktail");
 // spmv_only: src/util.cpp:85-91 (zeroes y, then coo_spmv)
 void ref_spmv_only(clspmv_coo_f32* m, float* x, float* y) { spmv_only(R<coo_t>(m), x, y); }
 

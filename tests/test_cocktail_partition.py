@@ -1,0 +1,140 @@
+"""Cocktail partition parity: the library's analyze_matrix against the
+reference's (src/analyze.cpp, compiled from its sources) on the same COO
+input and the same benchmark tables. Every flag, chosen variant, group
+count, part scalar and part array must be identical (entries the reference
+leaves uninitialised excepted). The table configurations are chosen so the
+partitions cover single-format results for all nine formats and the
+diagonal + block, diagonal + flat and block + flat combinations."""
+import itertools
+
+import numpy as np
+import pytest
+
+from clspmv_mic_b200 import cocktail as CK
+from clspmv_mic_b200 import formats as F
+from clspmv_mic_b200 import synth, tables
+from tests.cocktail_util import compare_cocktails, ref_analyze
+from tests.conftest import ref_or_skip
+
+
+def _union(*ts):
+    h, w = ts[0][0], ts[0][1]
+    r = np.concatenate([t[2] for t in ts]).astype(np.int64)
+    c = np.concatenate([t[3] for t in ts]).astype(np.int64)
+    v = np.concatenate([t[4] for t in ts])
+    key, idx = np.unique(r * w + c, return_index=True)
+    return (h, w, (key // w).astype(np.int32), (key % w).astype(np.int32), v[idx])
+
+
+def _matrices():
+    b = synth.block_rows(2500, 6, seed=2)
+    return {
+        "mixed": synth.cocktail_mixed(12000, 10000, 8000, seed=4),
+        "blocks_noise": _union(b, synth.random_coo(10000, 10000, 0.0006, seed=5)),
+        "band_blocks_noise": _union(synth.banded(10000, 5, seed=3), b, synth.random_coo(10000, 10000, 0.0004, seed=6)),
+        "band_noise": _union(synth.banded(10000, 9, seed=3), synth.random_coo(10000, 10000, 0.0008, seed=7)),
+        "stencil16": synth.stencil_27pt(16),
+        "powerlaw": synth.powerlaw(10000, maxlen=2000, seed=5),
+        "laplace128": synth.laplacian_2d(128),
+        "wide": synth.random_coo(3000, 7000, 0.002, seed=8),
+    }
+
+
+def _table_configs():
+    """(name, model_tables kwargs)"""
+    cfgs = [("plain", {}), ("fast_launch", {"launch_us": 0.2}), ("slow_launch", {"launch_us": 20.0})]
+    rng = np.random.default_rng(1)
+    for i in range(6):
+        sc = {k: float(np.exp(rng.uniform(np.log(0.1), np.log(4)))) for k in tables.IMP}
+        cfgs.append((f"random{i}", {"seed": i + 1, "scale": sc, "launch_us": float(rng.choice([0.5, 4.0]))}))
+    for fl, bl, dia in [(1, 8, 6), (3, 3, 1), (1, 3, 6), (0.3, 2, 8), (1, 1, 0.2)]:
+        cfgs.append((f"fl{fl}_bl{bl}_dia{dia}", {"seed": 1, "launch_us": 0.2, "gather_per_s": 2e12,
+                                                 "scale": {"sell": fl, "ell": fl, "csr": fl, "coo": fl, "sbell": bl, "bell": bl,
+                                                           "bcsr": bl, "dia": dia, "bdia": dia}}))
+    # partial blocks + flat remainder, and diagonals + flat remainder
+    cfgs.append(("block_partial", {"seed": 1, "launch_us": 0.05, "gather_per_s": 1e13,
+                                   "scale": {"dia": 6, "bdia": 6}}))
+    cfgs.append(("dia_flat", {"seed": 1, "launch_us": 0.2, "gather_per_s": 2e12,
+                              "scale": {"sell": 0.5, "ell": 0.5, "csr": 0.5, "coo": 0.5, "dia": 6, "bdia": 6}}))
+    cfgs.append(("sell_ell_fast", {"seed": 3, "scale": {"sell": 4, "ell": 4, "csr": 0.5, "coo": 0.5, "dia": 0.3, "bdia": 0.3,
+                                                         "sbell": 0.3, "bell": 0.3, "bcsr": 0.3}}))
+    cfgs.append(("sbell_bell", {"seed": 5, "scale": {"bcsr": 0.2, "sbell": 2.0, "bell": 1.8}}))
+    return cfgs
+
+
+@pytest.fixture(scope="module")
+def table_dirs(tmp_path_factory):
+    out = {}
+    for name, kw in _table_configs():
+        d = tmp_path_factory.mktemp(f"tables_{name}")
+        tables.model_tables(d, **kw)
+        out[name] = d
+    return out
+
+
+@pytest.fixture(scope="module")
+def matrices():
+    return {k: F.coo_matrix(*v) for k, v in _matrices().items()}
+
+
+COVERED = set()
+# analyze_matrix options per table configuration: (dia_priority_multiplier,
+# estimate_flat_partial, estimate_flat_full); alternated to bound the run time.
+_ALL_MODES = [(1.0, True, False), (1.0, False, False), (0.5, True, True), (3.0, True, False)]
+MODES = {name: [_ALL_MODES[i % 4], _ALL_MODES[(i + 1) % 4]] for i, (name, _) in enumerate(_table_configs())}
+MODES["block_partial"] = [(1.0, False, False), (1.0, True, False)]
+MODES["dia_flat"] = [(1.0, True, False), (3.0, True, False)]
+
+
+@pytest.mark.parametrize("cfg", [c[0] for c in _table_configs()])
+def test_partition_identical(cfg, table_dirs, matrices):
+    ref_or_skip()
+    d = table_dirs[cfg]
+    for (mname, coo), (mult, partial, full) in itertools.product(
+            matrices.items(), MODES[cfg]):
+        mine = CK.analyze(coo, d, mult, partial, full)
+        theirs = ref_analyze(coo, d, mult, partial, full)
+        diffs = compare_cocktails(mine, theirs)
+        assert not diffs, f"{cfg}/{mname} mult={mult} partial={partial} full={full}: {diffs[:5]}"
+        COVERED.add(tuple(p for p, _ in [("bdia", 0), ("dia", 0), ("sbell", 0), ("bell", 0), ("bcsr", 0), ("sell", 0),
+                                          ("ell", 0), ("csr", 0), ("coo", 0)] if mine.uses(p)))
+
+
+def test_partitions_cover_branches():
+    """The cases above must have driven the partitioner through these
+    outcomes (runs after test_partition_identical)."""
+    ref_or_skip()
+    if not COVERED:
+        pytest.skip("partition cases did not run")
+    singles = {u[0] for u in COVERED if len(u) == 1}
+    assert {"dia", "bdia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo"} <= singles, (singles, COVERED)
+    fams = {"bdia": "d", "dia": "d", "sbell": "b", "bell": "b", "bcsr": "b", "sell": "f", "ell": "f", "csr": "f", "coo": "f"}
+    combos = {"".join(sorted({fams[p] for p in u})) for u in COVERED}
+    assert {"bd", "df", "bf"} <= combos, (combos, COVERED)
+
+
+def test_partition_parts_reassemble_matrix(table_dirs, matrices):
+    """Without the reference: the parts of every partition add up to the
+    input matrix (each nonzero in exactly one part)."""
+    for cfg in ("plain", "fl1_bl3_dia6", "sell_ell_fast"):
+        for mname, coo in matrices.items():
+            m = CK.analyze(coo, table_dirs[cfg])
+            assert sum(p.nnz for p in m.parts().values()) == coo.nnz, (cfg, mname)
+            rows, cols, vals = [], [], []
+            for name, part in m.parts().items():
+                back = F.to_coo(part)
+                rows.append(back.array("coo_row_id"))
+                cols.append(back.array("coo_col_id"))
+                vals.append(back.array("coo_data"))
+            r, c, v = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+            order = np.lexsort((c, r))
+            assert np.array_equal(r[order], coo.array("coo_row_id"))
+            assert np.array_equal(c[order], coo.array("coo_col_id"))
+            assert np.array_equal(v[order], coo.array("coo_data"))
+
+
+def test_missing_tables_rejected(tmp_path, matrices):
+    from clspmv_mic_b200 import _abi
+    with pytest.raises(_abi.ClspmvError) as e:
+        CK.analyze(matrices["laplace128"], tmp_path)
+    assert e.value.status == _abi.ERR_ARG
