@@ -201,6 +201,10 @@ def _declare(lib):
         "clspmv_b4csr_spmv_f32": (I32, [S["b4csr"], VP, VP, f32, f32, VP]),
         "clspmv_analyze_matrix_f32": (I32, [S["coo"], P(Cocktail), C.c_char_p, f32, I32, I32]),
         "clspmv_free_cocktail_f32": (None, [P(Cocktail)]),
+        "clspmv_cocktail_upload_f32": (I32, [P(Cocktail), P(VP)]),
+        "clspmv_cocktail_spmv_f32": (I32, [VP, VP, VP, f32, f32, VP]),
+        "clspmv_cocktail_device_view": (I32, [VP, P(Cocktail)]),
+        "clspmv_cocktail_free": (I32, [VP]),
     }
     for fmt in ("csr", "dia", "bdia", "ell", "sell", "bcsr", "bell", "b4csr", "b4ell", "sbell", "coo"):
         sigs[f"clspmv_{fmt}2coo_f32"] = (I32, [S[fmt], S["coo"]])

@@ -49,6 +49,9 @@ class CocktailMatrix:
     def parts(self) -> dict:
         return {p: self.part(p) for p, _ in COCKTAIL_PARTS if self.uses(p)}
 
+    def to_device(self) -> "DeviceCocktail":
+        return DeviceCocktail(self)
+
     def summary(self) -> dict:
         s = self.struct
         out = {"shape": (s.mat_height, s.mat_width), "nnz": s.mat_nnz}
@@ -77,3 +80,32 @@ def analyze(coo: HostMatrix, table_dir: str | os.PathLike | None = None, dia_pri
     m = CocktailMatrix(out, owner="lib" if rc == 0 else None)
     check(rc, "analyze_matrix")
     return m
+
+
+class DeviceCocktail:
+    """Device residency of a CocktailMatrix (clspmv_cocktail_upload_f32)."""
+
+    def __init__(self, host: CocktailMatrix):
+        self.handle = C.c_void_p()
+        check(lib().clspmv_cocktail_upload_f32(C.byref(host.struct), C.byref(self.handle)), "cocktail_upload")
+        self.shape = (host.struct.mat_height, host.struct.mat_width)
+        self.nnz = host.struct.mat_nnz
+        self.parts = [p for p, _ in COCKTAIL_PARTS if host.uses(p)]
+        self.stored_bytes = sum(m.stored_bytes() for m in host.parts().values())
+
+    def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None) -> None:
+        """y <- alpha * A x + beta * y, asynchronous on `stream`."""
+        from .formats import _stream_handle
+        check(lib().clspmv_cocktail_spmv_f32(self.handle, x.data_ptr(), y.data_ptr(), alpha, beta,
+                                             _stream_handle(stream)), "cocktail_spmv")
+
+    def close(self):
+        if self.handle:
+            lib().clspmv_cocktail_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,10 +1,28 @@
 // api_internal.h — helpers shared by the .cu files of libclspmv_b200.so.
 #pragma once
 #include <cuda_runtime.h>
+#include "clspmv_b200.h"
 
 namespace clspmv {
 // Maps a CUDA error to a clspmv_status, remembering its text per thread.
 int cuda_status(cudaError_t e);
 // Counts `n` kernel launches and returns the status of the last launch.
 int after_launch(int n);
+
+// Format launchers (spmv_api.cu). With `atomic`, alpha*A*x is added into y
+// with red.global.add and beta is ignored (apply it first with
+// launch_prescale); several launches may then target one y concurrently.
+int launch_prescale(float* y, int n, float beta, cudaStream_t st);
+int launch_dia(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_bdia(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_ell(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_csr_vector(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, cudaStream_t st, bool atomic);
+int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_csr_merge_plan(const clspmv_csr_f32* m, int* tc, cudaStream_t st);
+int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 }  // namespace clspmv

@@ -1,0 +1,185 @@
+// cocktail_rt.cu — the Cocktail runtime: device residency of a partitioned
+// matrix and y <- alpha * A * x + beta * y over all of its parts.
+//
+// The reference (src/spmv_cocktail.cpp) uploads each part into cl_mem
+// buffers (cpy_<fmt>_mat, :304-1009), binds one kernel per part
+// (set_cocktail_kernels, :1012-1085) and runs them one after another on an
+// in-order queue, each reading and writing y (do_spmv, :1088-1132), then
+// clFinish. Here each part's kernel runs on its own stream, forked from and
+// joined back into the caller's stream with events, so the parts of one
+// SpMV overlap on the GPU; every part adds alpha * A_p * x into y with
+// red.global.add (beta is applied once, first). The fork/join is legal
+// inside CUDA graph capture, so a caller can capture one SpMV and replay it
+// without host round trips (the reference's A^k x loop, src/eval.cpp:19-72,
+// synchronises after every step).
+#include <cstddef>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include "clspmv_b200.h"
+#include "api_internal.h"
+
+using namespace clspmv;
+
+struct clspmv_cocktail_handle {
+    clspmv_cocktail_f32 dev;          // part structs with device pointers
+    int* merge_plan = nullptr;        // tile coordinates of the CSR part
+    int nparts = 0;
+    cudaStream_t streams[9] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[9] = {};
+};
+
+namespace {
+
+enum Part { P_BDIA, P_DIA, P_SBELL, P_BELL, P_BCSR, P_SELL, P_ELL, P_CSR, P_COO, P_COUNT };
+
+bool uses(const clspmv_cocktail_f32& c, int p)
+{
+    switch (p) {
+        case P_BDIA: return c.ifusebdia;
+        case P_DIA: return c.ifusedia;
+        case P_SBELL: return c.ifusesbell;
+        case P_BELL: return c.ifusebell;
+        case P_BCSR: return c.ifusebcsr;
+        case P_SELL: return c.ifusesell;
+        case P_ELL: return c.ifuseell;
+        case P_CSR: return c.ifusecsr;
+        case P_COO: return c.ifusecoo;
+    }
+    return false;
+}
+
+int launch_part(const clspmv_cocktail_handle* h, int p, const float* x, float* y, float alpha, float beta, cudaStream_t st,
+                bool atomic)
+{
+    const clspmv_cocktail_f32& d = h->dev;
+    switch (p) {
+        case P_BDIA: return launch_bdia(&d.bdia, x, y, alpha, beta, st, atomic);
+        case P_DIA: return launch_dia(&d.dia, x, y, alpha, beta, st, atomic);
+        case P_SBELL: return launch_sbell(&d.sbell, x, y, alpha, beta, st, atomic);
+        case P_BELL: return launch_b4ell(&d.bell, x, y, alpha, beta, st, atomic);
+        case P_BCSR: return launch_b4csr(&d.bcsr, x, y, alpha, beta, st, atomic);
+        case P_SELL: return launch_sell(&d.sell, x, y, alpha, beta, st, atomic);
+        case P_ELL: return launch_ell(&d.ell, x, y, alpha, beta, st, atomic);
+        case P_CSR: return launch_csr_merge(&d.csr, h->merge_plan, x, y, alpha, beta, st, atomic);
+        case P_COO: return launch_coo(&d.coo, x, y, alpha, beta, st, atomic);
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+void release(clspmv_cocktail_handle* h)
+{
+    clspmv_cocktail_f32& d = h->dev;
+    if (d.ifusebdia) clspmv_device_free_bdia_f32(&d.bdia);
+    if (d.ifusedia) clspmv_device_free_dia_f32(&d.dia);
+    if (d.ifusesbell) clspmv_device_free_sbell_f32(&d.sbell);
+    if (d.ifusebell) clspmv_device_free_b4ell_f32(&d.bell);
+    if (d.ifusebcsr) clspmv_device_free_b4csr_f32(&d.bcsr);
+    if (d.ifusesell) clspmv_device_free_sell_f32(&d.sell);
+    if (d.ifuseell) clspmv_device_free_ell_f32(&d.ell);
+    if (d.ifusecsr) clspmv_device_free_csr_f32(&d.csr);
+    if (d.ifusecoo) clspmv_device_free_coo_f32(&d.coo);
+    if (h->merge_plan) cudaFree(h->merge_plan);
+    for (int i = 0; i < P_COUNT; i++) {
+        if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
+        if (h->join[i]) cudaEventDestroy(h->join[i]);
+    }
+    if (h->fork) cudaEventDestroy(h->fork);
+}
+
+}  // namespace
+
+extern "C" {
+
+int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_handle** out)
+{
+    if (!host || !out) return CLSPMV_ERR_ARG;
+    *out = nullptr;
+    clspmv_cocktail_handle* h = new (std::nothrow) clspmv_cocktail_handle();
+    if (!h) return CLSPMV_ERR_ALLOC;
+    memset(&h->dev, 0, sizeof(h->dev));
+    const clspmv_cocktail_f32& c = *host;
+    clspmv_cocktail_f32& d = h->dev;
+    // flags, variants and sizes are copied; arrays are uploaded part by part
+    memcpy(&d, &c, offsetof(clspmv_cocktail_f32, bdia));
+    d.ifusebdia = d.ifusedia = d.ifusesbell = d.ifusebell = d.ifusebcsr = false;
+    d.ifusesell = d.ifuseell = d.ifusecsr = d.ifusecoo = false;
+    int rc = CLSPMV_OK;
+#define UP(flag, part, fn)                                  \
+    if (!rc && c.flag) {                                    \
+        rc = fn(&c.part, &d.part);                          \
+        if (!rc) d.flag = true;                             \
+    }
+    UP(ifusebdia, bdia, clspmv_upload_bdia_f32)
+    UP(ifusedia, dia, clspmv_upload_dia_f32)
+    UP(ifusesbell, sbell, clspmv_upload_sbell_f32)
+    UP(ifusebell, bell, clspmv_upload_b4ell_f32)
+    UP(ifusebcsr, bcsr, clspmv_upload_b4csr_f32)
+    UP(ifusesell, sell, clspmv_upload_sell_f32)
+    UP(ifuseell, ell, clspmv_upload_ell_f32)
+    UP(ifusecsr, csr, clspmv_upload_csr_f32)
+    UP(ifusecoo, coo, clspmv_upload_coo_f32)
+#undef UP
+    if (!rc && d.ifusecsr) {
+        const int ntiles = clspmv_csr_merge_tiles(d.csr.matinfo.height, d.csr.matinfo.nnz);
+        rc = cuda_status(cudaMalloc(&h->merge_plan, sizeof(int) * 2 * ((size_t)ntiles + 1)));
+        if (!rc) rc = launch_csr_merge_plan(&d.csr, h->merge_plan, 0);
+        if (!rc) rc = cuda_status(cudaStreamSynchronize(0));
+    }
+    for (int p = 0; !rc && p < P_COUNT; p++) {
+        if (!uses(d, p)) continue;
+        h->nparts++;
+        rc = cuda_status(cudaStreamCreateWithFlags(&h->streams[p], cudaStreamNonBlocking));
+        if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->join[p], cudaEventDisableTiming));
+    }
+    if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+    if (rc) {
+        release(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return CLSPMV_OK;
+}
+
+int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y, float alpha, float beta,
+                             clspmv_stream_t stream)
+{
+    if (!h || !x || !y) return CLSPMV_ERR_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int rows = h->dev.mat_height;
+    if (h->nparts == 0) return launch_prescale(y, rows, beta, st);
+    if (h->nparts == 1) {
+        for (int p = 0; p < P_COUNT; p++)
+            if (uses(h->dev, p)) return launch_part(h, p, x, y, alpha, beta, st, false);
+    }
+    int rc = launch_prescale(y, rows, beta, st);
+    if (rc) return rc;
+    rc = cuda_status(cudaEventRecord(h->fork, st));
+    for (int p = 0; !rc && p < P_COUNT; p++) {
+        if (!uses(h->dev, p)) continue;
+        rc = cuda_status(cudaStreamWaitEvent(h->streams[p], h->fork, 0));
+        if (!rc) rc = launch_part(h, p, x, y, alpha, 1.0f, h->streams[p], true);
+        if (!rc) rc = cuda_status(cudaEventRecord(h->join[p], h->streams[p]));
+        if (!rc) rc = cuda_status(cudaStreamWaitEvent(st, h->join[p], 0));
+    }
+    return rc;
+}
+
+int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail_f32* out)
+{
+    if (!h || !out) return CLSPMV_ERR_ARG;
+    *out = h->dev;
+    return CLSPMV_OK;
+}
+
+int clspmv_cocktail_free(clspmv_cocktail_handle* h)
+{
+    if (!h) return CLSPMV_ERR_ARG;
+    release(h);
+    delete h;
+    return CLSPMV_OK;
+}
+
+}  // extern "C"

@@ -124,139 +124,54 @@ __device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, cha
 }
 
 // ---------------------------------------------------------------------------
-// BDIA (kernels/spmv_bdia.cl:4-283): per band, the x window
-// [pass_row0 + offset, pass_row0 + offset + 1024 + width - 1) is staged in
-// shared memory once and every diagonal of the band reads it with a shifted
-// index, kept in a 4-register sliding window. Bands wider than kBdiaChunk
-// diagonals are processed kBdiaChunk diagonals at a time.
+// BDIA (kernels/spmv_bdia.cl:4-283): the reference stages, per band, an x
+// window in __local memory and lets every diagonal of the band read it with
+// a shifted index. Here the same reuse happens in registers: for each run of
+// up to kBdiaRun diagonals of a band, a thread loads the kBdiaRun + 3 x
+// values its 4 rows touch once (they stay L1-resident across neighbouring
+// threads) and slides over them, so a band of w diagonals costs w + 3 x
+// loads instead of 4 w, with no barrier. dia_data is read with one 128-bit
+// evict-first load per diagonal.
 // ---------------------------------------------------------------------------
 constexpr int kBdiaRowsPerPass = kBlock * 4;
-constexpr int kBdiaChunk = 128;
-constexpr int kBdiaSmemBytes = (kBdiaRowsPerPass + kBdiaChunk) * sizeof(float);
-constexpr int kBdiaWinMaxSmem = 100 * 1024;   // two window sets at most
+constexpr int kBdiaRun = 4;
 
 template <bool ATOMIC>
-__device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, char* smem)
+__device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, char*)
 {
-    float* s_x = reinterpret_cast<float*>(smem);
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
     cta_share(a.rows, 4, cta, ncta, b, e);
-    const int l0 = threadIdx.x * 4;
-    for (long long pass = b; pass < e; pass += kBdiaRowsPerPass) {
-        const long long row0 = pass + l0;
-        const bool active = row0 < e;
+    for (long long row0 = b + threadIdx.x * 4; row0 < e; row0 += kBdiaRowsPerPass) {
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
         for (int bd = 0; bd < a.nband; bd++) {
             const int dbeg = a.bptr[bd], dend = a.bptr[bd + 1];
             const int boff = a.offsets[bd];
-            for (int j0 = 0; j0 < dend - dbeg; j0 += kBdiaChunk) {
-                const int nj = min(kBdiaChunk, dend - dbeg - j0);
-                const long long wbase = pass + boff + j0;
-                const int wlen = kBdiaRowsPerPass + nj - 1;
-                __syncthreads();
-                for (int t = threadIdx.x; t < wlen; t += kBlock) {
-                    const long long c = wbase + t;
-                    s_x[t] = (c >= 0 && c < a.cols) ? ld_x(a.x + c, pl) : 0.f;
+            for (int j0 = dbeg; j0 < dend; j0 += kBdiaRun) {
+                const int n = min(kBdiaRun, dend - j0);
+                const long long c0 = row0 + boff + (j0 - dbeg);
+                float xw[kBdiaRun + 3];
+                float4 v[kBdiaRun];
+#pragma unroll
+                for (int t = 0; t < kBdiaRun; t++)
+                    if (t < n) v[t] = ld_stream_f4(a.data + (size_t)(j0 + t) * a.len + row0, pe);
+#pragma unroll
+                for (int t = 0; t < kBdiaRun + 3; t++) {
+                    const long long c = c0 + t;
+                    xw[t] = (t < n + 3 && c >= 0 && c < a.cols) ? ld_x(a.x + c, pl) : 0.f;
                 }
-                __syncthreads();
-                if (active) {
-                    const float* dp = a.data + (size_t)(dbeg + j0) * a.len + row0;
-                    float w0 = s_x[l0], w1 = s_x[l0 + 1], w2 = s_x[l0 + 2];
-#pragma unroll 4
-                    for (int j = 0; j < nj; j++) {
-                        const float w3 = s_x[l0 + j + 3];
-                        const float4 v = ld_stream_f4(dp + (size_t)j * a.len, pe);
-                        acc[0] = fmaf(v.x, w0, acc[0]);
-                        acc[1] = fmaf(v.y, w1, acc[1]);
-                        acc[2] = fmaf(v.z, w2, acc[2]);
-                        acc[3] = fmaf(v.w, w3, acc[3]);
-                        w0 = w1;
-                        w1 = w2;
-                        w2 = w3;
+#pragma unroll
+                for (int t = 0; t < kBdiaRun; t++) {
+                    if (t < n) {
+                        acc[0] = fmaf(v[t].x, xw[t], acc[0]);
+                        acc[1] = fmaf(v[t].y, xw[t + 1], acc[1]);
+                        acc[2] = fmaf(v[t].z, xw[t + 2], acc[2]);
+                        acc[3] = fmaf(v[t].w, xw[t + 3], acc[3]);
                     }
                 }
             }
         }
-        if (active) y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
-    }
-}
-
-// BDIA, pass-window form: the x windows of all bands for one 1024-row pass
-// sit side by side in shared memory (band b at b*1023 + bptr[b], length
-// 1023 + width_b), loaded with cp.async while the previous pass computes
-// (double buffer), so a pass needs one barrier instead of two per band.
-// Used when two window sets fit in shared memory; `win_floats` =
-// nband*1023 + ndiag.
-__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    const int n = valid ? 4 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ void bdia_prefetch(const BdiaArgs& a, long long pass, float* buf)
-{
-    for (int bd = 0; bd < a.nband; bd++) {
-        const int wo = bd * (kBdiaRowsPerPass - 1) + a.bptr[bd];
-        const int wl = kBdiaRowsPerPass - 1 + (a.bptr[bd + 1] - a.bptr[bd]);
-        const long long c0 = pass + a.offsets[bd];
-        for (int t = threadIdx.x; t < wl; t += kBlock) {
-            const long long c = c0 + t;
-            const bool in = c >= 0 && c < a.cols;
-            cp_async4(buf + wo + t, in ? a.x + c : a.x, in);
-        }
-    }
-    cp_async_commit();
-}
-
-template <bool ATOMIC>
-__device__ __forceinline__ void bdia_window_cta(const BdiaArgs& a, int win_floats, int cta, int ncta, char* smem)
-{
-    float* bufs = reinterpret_cast<float*>(smem);
-    const uint64_t pe = policy_evict_first();
-    long long b, e;
-    cta_share(a.rows, 4, cta, ncta, b, e);
-    const int l0 = threadIdx.x * 4;
-    if (b < e) bdia_prefetch(a, b, bufs);
-    int k = 0;
-    for (long long pass = b; pass < e; pass += kBdiaRowsPerPass, k++) {
-        const long long next = pass + kBdiaRowsPerPass;
-        if (next < e) {
-            bdia_prefetch(a, next, bufs + ((k + 1) & 1) * win_floats);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const float* buf = bufs + (k & 1) * win_floats;
-        const long long row0 = pass + l0;
-        if (row0 < e) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            for (int bd = 0; bd < a.nband; bd++) {
-                const int dbeg = a.bptr[bd], dend = a.bptr[bd + 1];
-                const float* w = buf + bd * (kBdiaRowsPerPass - 1) + dbeg + l0;
-                const float* dp = a.data + (size_t)dbeg * a.len + row0;
-                float w0 = w[0], w1 = w[1], w2 = w[2];
-#pragma unroll 4
-                for (int j = 0; j < dend - dbeg; j++) {
-                    const float w3 = w[j + 3];
-                    const float4 v = ld_stream_f4(dp + (size_t)j * a.len, pe);
-                    acc[0] = fmaf(v.x, w0, acc[0]);
-                    acc[1] = fmaf(v.y, w1, acc[1]);
-                    acc[2] = fmaf(v.z, w2, acc[2]);
-                    acc[3] = fmaf(v.w, w3, acc[3]);
-                    w0 = w1;
-                    w1 = w2;
-                    w2 = w3;
-                }
-            }
-            y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
-        }
-        __syncthreads();
+        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
     }
 }
 

@@ -57,20 +57,7 @@ __global__ void __launch_bounds__(kBlock) k_dia(DiaArgs a)
 }
 
 template <bool A>
-__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgs a)
-{
-    __shared__ __align__(16) char smem[kBdiaSmemBytes];
-    bdia_cta<A>(a, blockIdx.x, gridDim.x, smem);
-}
-
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_bdia_win(BdiaArgs a, int win_cap)
-{
-    extern __shared__ __align__(16) char dsmem[];
-    const int win = a.nband * (kBdiaRowsPerPass - 1) + a.bptr[a.nband];
-    if (win <= win_cap) bdia_window_cta<A>(a, win, blockIdx.x, gridDim.x, dsmem);
-    else bdia_cta<A>(a, blockIdx.x, gridDim.x, dsmem);
-}
+__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgs a) { bdia_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_ell(EllArgs a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
@@ -202,6 +189,215 @@ int prescale(float* y, int n, float beta, cudaStream_t st)
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Internal launchers. `atomic` = add alpha*A*x into y with red.global.add
+// (beta must already be applied); used by the Cocktail runtime, whose parts
+// run concurrently into one y.
+// ---------------------------------------------------------------------------
+namespace clspmv {
+
+int launch_prescale(float* y, int n, float beta, cudaStream_t st) { return prescale(y, n, beta, st); }
+
+int launch_dia(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->dia_num > 0 && (!m->dia_offsets || !m->dia_data)) return CLSPMV_ERR_ARG;
+    if ((m->dia_length_aligned & 3) || !aligned16(m->dia_data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
+    DiaArgs a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, m->dia_data, x, y, alpha, beta};
+    if (atomic) k_dia<true><<<persistent_grid(k_dia<true>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    else k_dia<false><<<persistent_grid(k_dia<false>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_bdia(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data)) return CLSPMV_ERR_ARG;
+    if ((m->bdia_length_aligned & 3) || !aligned16(m->bdia_data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
+    BdiaArgs a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, m->bdia_data, x, y, alpha, beta};
+    if (atomic) k_bdia<true><<<persistent_grid(k_bdia<true>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
+    else k_bdia<false><<<persistent_grid(k_bdia<false>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_ell(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->ell_num > 0 && (!m->ell_col_id || !m->ell_data)) return CLSPMV_ERR_ARG;
+    if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned16(m->ell_data) || rows > m->ell_height_aligned)
+        return CLSPMV_ERR_ALIGN;
+    EllArgs a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, m->ell_data, x, y, alpha, beta};
+    if (atomic) k_ell<true><<<persistent_grid(k_ell<true>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
+    else k_ell<false><<<persistent_grid(k_ell<false>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y || !m->sell_slice_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    const int sh = (int)m->sell_slice_height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
+    SellArgs a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data, x, y, alpha, beta};
+    const bool vec = aligned16(m->sell_col_id) && aligned16(m->sell_data);
+    if (vec && (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
+        if (!atomic) {
+            int rc = prescale(y, rows, beta, st);
+            if (rc) return rc;
+        }
+        a.beta = 1.0f;
+        return dispatch_lanes(sh / 4, [&](auto q) {
+            constexpr int Q = decltype(q)::value;
+            if (atomic) k_sell<Q, true><<<persistent_grid(k_sell<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a);
+            else k_sell<Q, false><<<persistent_grid(k_sell<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a);
+            return after_launch(1);
+        });
+    }
+    if (atomic) k_sell_rows<true><<<persistent_grid(k_sell_rows<true>, rows, kBlock), kBlock, 0, st>>>(a);
+    else k_sell_rows<false><<<persistent_grid(k_sell_rows<false>, rows, kBlock), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
+    // one pass per CTA: thread-per-row work is uneven, so CTAs are scheduled dynamically
+    if (atomic) k_csr_scalar<true><<<grid_for(rows, kBlock), kBlock, 0, st>>>(a);
+    else k_csr_scalar<false><<<grid_for(rows, kBlock), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_csr_vector(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
+    if (tpr == 0) tpr = pow2_lanes((double)m->matinfo.nnz / rows, 2, 32);
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
+    return dispatch_lanes(tpr, [&](auto t) {
+        constexpr int T = decltype(t)::value;
+        const unsigned grid = grid_for(rows, kBlock / T);
+        if (atomic) k_csr_vector<T, true><<<grid, kBlock, 0, st>>>(a);
+        else k_csr_vector<T, false><<<grid, kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !tc || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!atomic) {
+        int rc = prescale(y, rows, beta, st);
+        if (rc) return rc;
+    }
+    const int ntiles = clspmv_csr_merge_tiles(rows, m->matinfo.nnz);
+    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, 1.0f};
+    k_csr_merge<<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
+    return after_launch(1);
+}
+
+int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!atomic) {
+        int rc = prescale(y, rows, beta, st);
+        if (rc) return rc;
+    }
+    if (m->matinfo.nnz <= 0) return CLSPMV_OK;
+    if (!m->coo_row_id || !m->coo_col_id || !m->coo_data) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned16(m->coo_data)) return CLSPMV_ERR_ALIGN;
+    CooArgs a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, m->coo_data, x, y, alpha};
+    k_coo<<<persistent_grid(k_coo, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->b4ell_row_num <= 0) return CLSPMV_OK;
+    if (!m->b4ell_col_id || !m->b4ell_data) return CLSPMV_ERR_ARG;
+    if ((m->b4ell_float4_aligned & 3) || !aligned16(m->b4ell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->b4ell_row_num * m->b4ell_bheight < rows || m->b4ell_float4_aligned < 4 * m->b4ell_row_num) return CLSPMV_ERR_ARG;
+    const B4ellArgs a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
+                      m->b4ell_float4_aligned, m->b4ell_col_id, m->b4ell_data, x, y, alpha, beta};
+    return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
+        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+        if (atomic) k_b4ell<BW4, BH, true><<<persistent_grid(k_b4ell<BW4, BH, true>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        else k_b4ell<BW4, BH, false><<<persistent_grid(k_b4ell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->sbell_row_num <= 0) return CLSPMV_OK;
+    if (!m->sbell_slice_ptr || !m->sbell_col_id || !m->sbell_data || m->sbell_slice_height == 0) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->sbell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
+    const SbellArgs a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
+                      m->sbell_slice_ptr, m->sbell_col_id, m->sbell_data, x, y, alpha, beta};
+    return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
+        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+        if (atomic) k_sbell<BW4, BH, true><<<persistent_grid(k_sbell<BW4, BH, true>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        else k_sbell<BW4, BH, false><<<persistent_grid(k_sbell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->b4csr_row_num <= 0) return CLSPMV_OK;
+    if (!m->b4csr_row_ptr || !m->b4csr_col_id || !m->b4csr_data) return CLSPMV_ERR_ARG;
+    if ((m->b4csr_aligned_size & 3) || !aligned16(m->b4csr_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->b4csr_row_num * m->b4csr_bheight < rows) return CLSPMV_ERR_ARG;
+    const B4csrArgs a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
+                      m->b4csr_row_ptr, m->b4csr_col_id, m->b4csr_data, x, y, alpha, beta};
+    const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num, 1, 32);
+    return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
+        return dispatch_lanes(lanes, [&](auto t) {
+            constexpr int T = decltype(t)::value;
+            constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+            if (atomic)
+                k_b4csr<BW4, BH, T, true><<<persistent_grid(k_b4csr<BW4, BH, T, true>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
+            else
+                k_b4csr<BW4, BH, T, false><<<persistent_grid(k_b4csr<BW4, BH, T, false>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
+            return after_launch(1);
+        });
+    });
+}
+
+int launch_csr_merge_plan(const clspmv_csr_f32* m, int* tc, cudaStream_t st)
+{
+    if (!m || !tc || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int ntiles = clspmv_csr_merge_tiles(m->matinfo.height, m->matinfo.nnz);
+    if (ntiles < 0) return CLSPMV_ERR_ARG;
+    k_csr_merge_plan<<<grid_for((long long)ntiles + 1, kBlock), kBlock, 0, st>>>(m->matinfo.height, m->matinfo.nnz, m->csr_row_ptr, tc, ntiles);
+    return after_launch(1);
+}
+
+}  // namespace clspmv
+
+// ---------------------------------------------------------------------------
 // Compute entry points
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -228,222 +424,35 @@ const char* clspmv_last_cuda_error(void) { return g_last_cuda_error.c_str(); }
 
 long long clspmv_launch_count(void) { return g_launches.load(); }
 
-int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (m->dia_num > 0 && (!m->dia_offsets || !m->dia_data)) return CLSPMV_ERR_ARG;
-    if ((m->dia_length_aligned & 3) || !aligned16(m->dia_data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
-    DiaArgs a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, m->dia_data, x, y, alpha, beta};
-    k_dia<false><<<persistent_grid(k_dia<false>, rows, kDiaRowsPerPass), kBlock, 0, S(stream)>>>(a);
-    return after_launch(1);
-}
-
-int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data)) return CLSPMV_ERR_ARG;
-    if ((m->bdia_length_aligned & 3) || !aligned16(m->bdia_data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
-    BdiaArgs a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, m->bdia_data, x, y, alpha, beta};
-    // Window-set size for the shared-memory kernel. The diagonal count
-    // bptr[nband] lives on the device; the host bounds it with the DIA
-    // acceptance rule (a converted matrix has (D-1)*len < 2*nnz,
-    // include/matrix_storage.h:972) and the kernel re-checks the true count,
-    // taking the per-band path when the window set does not fit.
-    const long long len = std::max(1, m->bdia_length_aligned);
-    const long long dbound = (2LL * std::max(0, m->matinfo.nnz) - 1) / len + 1;
-    const long long win = (long long)m->bdia_band_num * (kBdiaRowsPerPass - 1) + dbound;
-    const long long smem = 2 * win * (long long)sizeof(float);
-    cudaStream_t st = S(stream);
-    if (m->bdia_band_num > 0 && smem <= kBdiaWinMaxSmem) {
-        static std::once_flag once;
-        static int attr_rc = CLSPMV_OK;
-        std::call_once(once, [] {
-            attr_rc = cuda_status(cudaFuncSetAttribute(k_bdia_win<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBdiaWinMaxSmem));
-        });
-        if (attr_rc) return attr_rc;
-        k_bdia_win<false><<<persistent_grid(k_bdia_win<false>, rows, kBdiaRowsPerPass, (int)smem), kBlock, (size_t)smem, st>>>(a, (int)win);
-        return after_launch(1);
-    }
-    k_bdia<false><<<persistent_grid(k_bdia<false>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
-    return after_launch(1);
-}
-
-int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (m->ell_num > 0 && (!m->ell_col_id || !m->ell_data)) return CLSPMV_ERR_ARG;
-    if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned16(m->ell_data) || rows > m->ell_height_aligned)
-        return CLSPMV_ERR_ALIGN;
-    EllArgs a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, m->ell_data, x, y, alpha, beta};
-    k_ell<false><<<persistent_grid(k_ell<false>, rows, kEllRowsPerPass), kBlock, 0, S(stream)>>>(a);
-    return after_launch(1);
-}
-
-int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y || !m->sell_slice_ptr) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    const int sh = (int)m->sell_slice_height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
-    SellArgs a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data, x, y, alpha, beta};
-    cudaStream_t st = S(stream);
-    const bool vec = aligned16(m->sell_col_id) && aligned16(m->sell_data);
-    if (vec && (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
-        int rc = prescale(y, rows, beta, st);
-        if (rc) return rc;
-        a.beta = 1.0f;
-        return dispatch_lanes(sh / 4, [&](auto q) {
-            constexpr int Q = decltype(q)::value;
-            k_sell<Q, false><<<persistent_grid(k_sell<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a);
-            return after_launch(1);
-        });
-    }
-    k_sell_rows<false><<<persistent_grid(k_sell_rows<false>, rows, kBlock), kBlock, 0, st>>>(a);
-    return after_launch(1);
-}
-
-int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
-    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
-    k_csr_scalar<false><<<persistent_grid(k_csr_scalar<false>, rows, kBlock), kBlock, 0, S(stream)>>>(a);
-    return after_launch(1);
-}
-
-int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, clspmv_stream_t stream)
-{
-    if (!m || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (!aligned16(m->csr_col_id) || !aligned16(m->csr_data)) return CLSPMV_ERR_ALIGN;
-    if (tpr == 0) tpr = pow2_lanes((double)m->matinfo.nnz / rows, 2, 32);
-    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, beta};
-    cudaStream_t st = S(stream);
-    return dispatch_lanes(tpr, [&](auto t) {
-        constexpr int T = decltype(t)::value;
-        k_csr_vector<T, false><<<persistent_grid(k_csr_vector<T, false>, rows, kBlock / T), kBlock, 0, st>>>(a);
-        return after_launch(1);
-    });
-}
-
 int clspmv_csr_merge_tiles(int rows, int nnz)
 {
     if (rows < 0 || nnz < 0) return -1;
     return (int)(((long long)rows + nnz + kMergeTile - 1) / kMergeTile);
 }
 
-int clspmv_csr_merge_plan(const clspmv_csr_f32* m, int* tc, clspmv_stream_t stream)
-{
-    if (!m || !tc || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
-    const int ntiles = clspmv_csr_merge_tiles(m->matinfo.height, m->matinfo.nnz);
-    if (ntiles < 0) return CLSPMV_ERR_ARG;
-    k_csr_merge_plan<<<grid_for((long long)ntiles + 1, kBlock), kBlock, 0, S(stream)>>>(
-        m->matinfo.height, m->matinfo.nnz, m->csr_row_ptr, tc, ntiles);
-    return after_launch(1);
-}
-
-int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !tc || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    cudaStream_t st = S(stream);
-    int rc = prescale(y, rows, beta, st);
-    if (rc) return rc;
-    const int ntiles = clspmv_csr_merge_tiles(rows, m->matinfo.nnz);
-    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, 1.0f};
-    k_csr_merge<<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
-    return after_launch(1);
-}
-
-int clspmv_coo_spmv_f32(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    cudaStream_t st = S(stream);
-    int rc = prescale(y, rows, beta, st);
-    if (rc) return rc;
-    if (m->matinfo.nnz <= 0) return CLSPMV_OK;
-    if (!m->coo_row_id || !m->coo_col_id || !m->coo_data) return CLSPMV_ERR_ARG;
-    if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned16(m->coo_data)) return CLSPMV_ERR_ALIGN;
-    CooArgs a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, m->coo_data, x, y, alpha};
-    k_coo<<<persistent_grid(k_coo, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
-    return after_launch(1);
-}
-
-}  // extern "C"
-
-
-extern "C" {
-
-int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0 || m->b4ell_row_num <= 0) return CLSPMV_OK;
-    if (!m->b4ell_col_id || !m->b4ell_data) return CLSPMV_ERR_ARG;
-    if ((m->b4ell_float4_aligned & 3) || !aligned16(m->b4ell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
-    if ((long long)m->b4ell_row_num * m->b4ell_bheight < rows || m->b4ell_float4_aligned < 4 * m->b4ell_row_num) return CLSPMV_ERR_ARG;
-    const B4ellArgs a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
-                      m->b4ell_float4_aligned, m->b4ell_col_id, m->b4ell_data, x, y, alpha, beta};
-    cudaStream_t st = S(stream);
-    return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
-        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
-        k_b4ell<BW4, BH, false><<<persistent_grid(k_b4ell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        return after_launch(1);
-    });
-}
-
-int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0 || m->sbell_row_num <= 0) return CLSPMV_OK;
-    if (!m->sbell_slice_ptr || !m->sbell_col_id || !m->sbell_data || m->sbell_slice_height == 0) return CLSPMV_ERR_ARG;
-    if (!aligned16(m->sbell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
-    if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
-    const SbellArgs a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
-                      m->sbell_slice_ptr, m->sbell_col_id, m->sbell_data, x, y, alpha, beta};
-    cudaStream_t st = S(stream);
-    return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
-        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
-        k_sbell<BW4, BH, false><<<persistent_grid(k_sbell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        return after_launch(1);
-    });
-}
-
-int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t stream)
-{
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0 || m->b4csr_row_num <= 0) return CLSPMV_OK;
-    if (!m->b4csr_row_ptr || !m->b4csr_col_id || !m->b4csr_data) return CLSPMV_ERR_ARG;
-    if ((m->b4csr_aligned_size & 3) || !aligned16(m->b4csr_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
-    if ((long long)m->b4csr_row_num * m->b4csr_bheight < rows) return CLSPMV_ERR_ARG;
-    const B4csrArgs a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
-                      m->b4csr_row_ptr, m->b4csr_col_id, m->b4csr_data, x, y, alpha, beta};
-    cudaStream_t st = S(stream);
-    const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num, 1, 32);
-    return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
-        return dispatch_lanes(lanes, [&](auto t) {
-            constexpr int T = decltype(t)::value;
-            constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
-            k_b4csr<BW4, BH, T, false>
-                <<<persistent_grid(k_b4csr<BW4, BH, T, false>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
-            return after_launch(1);
-        });
-    });
-}
+int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_dia(m, x, y, alpha, beta, S(s), false); }
+int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_bdia(m, x, y, alpha, beta, S(s), false); }
+int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_ell(m, x, y, alpha, beta, S(s), false); }
+int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_sell(m, x, y, alpha, beta, S(s), false); }
+int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_csr_scalar(m, x, y, alpha, beta, S(s), false); }
+int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, clspmv_stream_t s)
+{ return launch_csr_vector(m, x, y, alpha, beta, tpr, S(s), false); }
+int clspmv_csr_merge_plan(const clspmv_csr_f32* m, int* tc, clspmv_stream_t s)
+{ return launch_csr_merge_plan(m, tc, S(s)); }
+int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_csr_merge(m, tc, x, y, alpha, beta, S(s), false); }
+int clspmv_coo_spmv_f32(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_coo(m, x, y, alpha, beta, S(s), false); }
+int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_b4ell(m, x, y, alpha, beta, S(s), false); }
+int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_sbell(m, x, y, alpha, beta, S(s), false); }
+int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_b4csr(m, x, y, alpha, beta, S(s), false); }
 
 }  // extern "C"

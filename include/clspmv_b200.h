@@ -363,6 +363,28 @@ int clspmv_analyze_matrix_f32(const clspmv_coo_f32* coo, clspmv_cocktail_f32* ou
 /* free_cocktail (include/analyze.h:183-205) */
 void clspmv_free_cocktail_f32(clspmv_cocktail_f32* m);
 
+/* ------------------------------------------------------------------------ */
+/* Cocktail runtime (src/spmv_cocktail.cpp of clSpMV).                       */
+/* ------------------------------------------------------------------------ */
+
+/* Opaque device residency of a partitioned matrix. */
+typedef struct clspmv_cocktail_handle clspmv_cocktail_handle;
+
+/* Uploads every used part of `host` (replaces init_mat_kernels / cpy_<fmt>_mat,
+ * src/spmv_cocktail.cpp:304-1009, 1590-1611). Synchronous. */
+int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_handle** out);
+/* y <- alpha*A*x + beta*y over all parts (replaces do_spmv,
+ * src/spmv_cocktail.cpp:1088-1132). Parts run concurrently on internal
+ * streams forked from and joined into `stream`; safe to capture in a CUDA
+ * graph. The parts' additions to y are atomic, so the summation order (and
+ * the last bits of y) may differ from run to run within the 1e-5 bound. */
+int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y, float alpha, float beta,
+                             clspmv_stream_t stream);
+/* The device-side part structs (device pointers), e.g. to launch one part. */
+int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail_f32* out);
+/* Releases the device parts (replaces free_mat_kernels, :1613-1618). */
+int clspmv_cocktail_free(clspmv_cocktail_handle* h);
+
 /* Number of kernels this library launched since load (all entry points). */
 long long clspmv_launch_count(void);
 

@@ -1,0 +1,101 @@
+"""Cocktail runtime on the GPU: a partitioned matrix's SpMV over all its
+parts (running concurrently, accumulating atomically into y) against the
+oracle's csr_spmv on the unpartitioned matrix, within the 1e-5 row bound;
+plus replay under CUDA-graph capture (the A^k x loop of src/eval.cpp:19-72
+without host synchronisation)."""
+import numpy as np
+import pytest
+
+from clspmv_mic_b200 import cocktail as CK
+from clspmv_mic_b200 import formats as F
+from clspmv_mic_b200 import synth, tables
+from tests.gpu_util import assert_close, reference_y
+from tests.test_cocktail_partition import _matrices, _table_configs
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("block_partial", "mixed", (1.0, False, False)), ("block_partial", "blocks_noise", (1.0, False, False)),
+         ("dia_flat", "band_noise", (1.0, True, False)), ("random0", "band_blocks_noise", (1.0, True, False)),
+         ("sbell_bell", "blocks_noise", (1.0, True, False)), ("sell_ell_fast", "powerlaw", (1.0, True, False)),
+         ("plain", "laplace128", (1.0, True, False)), ("fl1_bl8_dia6", "mixed", (1.0, True, False)),
+         ("plain", "wide", (1.0, True, False))]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.fixture(scope="module")
+def setup(tmp_path_factory):
+    cfgs = dict(_table_configs())
+    mats = _matrices()
+    out = {}
+    for cfg, mname, mode in CASES:
+        d = tmp_path_factory.mktemp(f"t_{cfg}")
+        tables.model_tables(d, **cfgs[cfg])
+        coo = F.coo_matrix(*mats[mname])
+        out[(cfg, mname)] = (coo, CK.analyze(coo, d, *mode))
+    return out
+
+
+@pytest.mark.parametrize("cfg,mname,mode", CASES)
+@pytest.mark.parametrize("alpha,beta", [(1.0, 1.0), (2.0, -0.5), (1.0, 0.0)])
+def test_cocktail_spmv(setup, cfg, mname, mode, alpha, beta):
+    import torch
+    coo, ck = setup[(cfg, mname)]
+    dev = ck.to_device()
+    x = synth.x_vector(coo.shape[1])
+    y0 = np.random.default_rng(3).standard_normal(coo.shape[0]).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.from_numpy(y0.copy()).cuda()
+    dev.spmv(xd, yd, alpha, beta)
+    torch.cuda.synchronize()
+    y_ref, _, bound = reference_y(coo, x, y0, alpha, beta)
+    assert_close(yd.cpu().numpy(), y_ref, bound, f"cocktail {cfg}/{mname} parts={dev.parts}")
+
+
+def test_cocktail_graph_replay(setup):
+    """Capture y <- A x + y once, replay it k times: y = y0 + k A x."""
+    import torch
+    coo, ck = setup[("block_partial", "mixed")]
+    dev = ck.to_device()
+    assert len(dev.parts) >= 2, dev.parts
+    x = synth.x_vector(coo.shape[1])
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros(coo.shape[0], dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        dev.spmv(xd, yd, 1.0, 1.0, stream=s)   # warm-up outside capture
+    torch.cuda.synchronize()
+    yd.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        dev.spmv(xd, yd, 1.0, 1.0, stream=s)
+    yd.zero_()
+    k = 5
+    for _ in range(k):
+        g.replay()
+    torch.cuda.synchronize()
+    y_ref, _, bound = reference_y(coo, x)
+    assert_close(yd.cpu().numpy() / k, y_ref, bound * 1.0, "graph replay")
+
+
+def test_cocktail_parts_alone_sum_to_whole(setup):
+    """Each part alone, added up, gives the partitioned result."""
+    import torch
+    coo, ck = setup[("fl1_bl8_dia6", "mixed")]
+    x = synth.x_vector(coo.shape[1])
+    xd = torch.from_numpy(x).cuda()
+    total = np.zeros(coo.shape[0], np.float64)
+    for name, part in ck.parts().items():
+        yd = torch.zeros(coo.shape[0], dtype=torch.float32, device="cuda")
+        kw = {"variant": "merge"} if part.fmt == "csr" else {}
+        F.DeviceMatrix(part).spmv(xd, yd, 1.0, 1.0, **kw)
+        torch.cuda.synchronize()
+        total += yd.cpu().numpy()
+    y_ref, _, bound = reference_y(coo, x)
+    assert_close(total.astype(np.float32), y_ref, bound * 2, "sum of parts")
