@@ -47,7 +47,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--small", action="store_true", help="scaled-down matrices (quick check)")
@@ -164,7 +164,7 @@ class ClockSampler:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -357,13 +357,17 @@ def run_ours(args):
             if i is not None:
                 ev[i][K].record(stream)
 
+    clocks = ClockSampler(local)
+    clocks.start()          # sampling starts before the warm-up so it covers the timed region
+    t_warm = time.perf_counter()
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
+    while time.perf_counter() - t_warm < 0.5:   # keep the GPU busy while nvidia-smi spins up
+        step()
+        torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     launches0 = F.launch_count()
     t_all0 = torch.cuda.Event(enable_timing=True)
     t_all1 = torch.cuda.Event(enable_timing=True)
