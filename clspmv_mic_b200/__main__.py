@@ -1,0 +1,66 @@
+"""Command line equivalents of clSpMV's programs.
+
+    python -m clspmv_mic_b200 all <matrix.mtx> [method] [ntimes]
+        spmv_all (src/spmv_all.cpp:156-256): method 0 measures copy
+        bandwidth and launch overhead; 1 csr scalar, 2 csr vector, 3 bdia,
+        4 dia, 5 ell, 6 coo, 7 bell, 8 bcsr, 9 sell, 10 sbell (as the
+        reference); 11 csr merge-path (this library's CSR kernel).
+    python -m clspmv_mic_b200 cocktail <matrix.mtx> [table_dir]
+        spmv_cocktail (src/eval.cpp:100-131): read, print the matrix info,
+        partition with the benchmark tables of table_dir (default
+        $CLSPMVPATH, else the tables shipped with the package), evaluate.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+from . import _abi
+from .cocktail import analyze
+from .drivers import bandwidth_test, evaluate, read_mmf, run_method
+from .tables import ensure_default_tables
+
+_BY_NUMBER = {v: k for k, v in _abi.METHODS.items()}
+
+
+def _usage() -> int:
+    print(__doc__)
+    return 0
+
+
+def main(argv: list[str]) -> int:
+    if len(argv) < 2:
+        return _usage()
+    cmd, path = argv[0], argv[1]
+    if cmd == "all":
+        method = int(argv[2]) if len(argv) > 2 else 1
+        ntimes = int(argv[3]) if len(argv) > 3 else 20
+        if method == 0:
+            for nbytes in [32 << (10 + k) for k in range(11)]:
+                bandwidth_test(nbytes, 100, verbose=True)
+            return 0
+        if method not in _BY_NUMBER:
+            return _usage()
+        coo = read_mmf(path)
+        run_method(coo, _BY_NUMBER[method], ntimes, verbose=True)
+        return 0
+    if cmd == "cocktail":
+        coo = read_mmf(path)
+        table_dir = argv[2] if len(argv) > 2 else os.environ.get("CLSPMVPATH") or str(ensure_default_tables())
+        h, w = coo.shape
+        print(f"\nMatInfo: Width {w} Height {h} NNZ {coo.nnz}")
+        vec = np.ones(w, dtype=np.float32)
+        res = np.zeros(h, dtype=np.float32)
+        a = coo.arrays()
+        coores = np.zeros(h, dtype=np.float32)
+        np.add.at(coores, a["coo_row_id"], a["coo_data"] * vec[a["coo_col_id"]])
+        mat = analyze(coo, table_dir)
+        evaluate(mat, vec, res, coores, 1000, verbose=True)
+        return 0
+    return _usage()
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

@@ -96,6 +96,23 @@ class Cocktail(C.Structure):
                  ("ell", Ell), ("csr", Csr), ("coo", Coo)])
 
 
+BENCH_MAX_VARIANTS = 16
+METHODS = {"bandwidth": 0, "csr_scalar": 1, "csr_vector": 2, "bdia": 3, "dia": 4, "ell": 5, "coo": 6, "bell": 7,
+           "bcsr": 8, "sell": 9, "sbell": 10, "csr_merge": 11}
+
+
+class BenchVariant(C.Structure):
+    """clspmv_bench_variant: one timed variant of a benchmark driver."""
+    _fields_ = [("status", I32), ("param0", I32), ("param1", I32), ("ms", C.c_double), ("gflops", C.c_double),
+                ("distance", C.c_double), ("max_diff", C.c_double), ("max_diff_ratio", C.c_double)]
+
+
+class BenchResult(C.Structure):
+    """clspmv_bench_result: every variant a driver ran and the fastest."""
+    _fields_ = [("method", I32), ("nvariants", I32), ("best", I32), ("best_ms", C.c_double),
+                ("best_gflops", C.c_double), ("v", BenchVariant * BENCH_MAX_VARIANTS)]
+
+
 def _n_bdia_data(s):
     if s.bdia_band_num <= 0:
         return 0
@@ -205,6 +222,11 @@ def _declare(lib):
         "clspmv_cocktail_spmv_f32": (I32, [VP, VP, VP, f32, f32, VP]),
         "clspmv_cocktail_device_view": (I32, [VP, P(Cocktail)]),
         "clspmv_cocktail_free": (I32, [VP]),
+        "clspmv_run_method_f32": (I32, [S["coo"], I32, I32, I32, P(BenchResult)]),
+        "clspmv_bandwidth_test": (I32, [C.c_size_t, I32, I32, P(C.c_double), P(C.c_double)]),
+        "clspmv_cocktail_evaluate_f32": (I32, [P(Cocktail), VP, VP, VP, I32, I32, P(C.c_double), P(C.c_double),
+                                               P(C.c_double)]),
+        "clspmv_read_mmf_f32": (I32, [C.c_char_p, S["coo"]]),
     }
     for fmt in ("csr", "dia", "bdia", "ell", "sell", "bcsr", "bell", "b4csr", "b4ell", "sbell", "coo"):
         sigs[f"clspmv_{fmt}2coo_f32"] = (I32, [S[fmt], S["coo"]])

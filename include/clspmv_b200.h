@@ -385,6 +385,85 @@ int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail
 /* Releases the device parts (replaces free_mat_kernels, :1613-1618). */
 int clspmv_cocktail_free(clspmv_cocktail_handle* h);
 
+/* ------------------------------------------------------------------------ */
+/* Benchmark drivers (src/spmv_all.cpp, src/spmv_<fmt>.cpp, src/eval.cpp).   */
+/* ------------------------------------------------------------------------ */
+
+/* Method numbers of the reference's spmv_all command line
+ * (src/spmv_all.cpp:156-167); CSR_MERGE is this library's addition. */
+enum {
+    CLSPMV_METHOD_BANDWIDTH = 0,
+    CLSPMV_METHOD_CSR_SCALAR = 1,
+    CLSPMV_METHOD_CSR_VECTOR = 2,
+    CLSPMV_METHOD_BDIA = 3,
+    CLSPMV_METHOD_DIA = 4,
+    CLSPMV_METHOD_ELL = 5,
+    CLSPMV_METHOD_COO = 6,
+    CLSPMV_METHOD_BELL = 7,
+    CLSPMV_METHOD_BCSR = 8,
+    CLSPMV_METHOD_SELL = 9,
+    CLSPMV_METHOD_SBELL = 10,
+    CLSPMV_METHOD_CSR_MERGE = 11
+};
+
+#define CLSPMV_BENCH_MAX_VARIANTS 16
+
+/* One timed variant: a block shape (BELL, SBELL, BCSR), a slice height
+ * (SELL), a lane count (CSR vector) or a row padding (CSR scalar). */
+typedef struct {
+    int status;            /* CLSPMV_OK, or why this variant did not run (converter refusal) */
+    int param0, param1;    /* block height / block width, slice height, lanes, padding */
+    double ms;             /* per SpMV, mean over the timed launches */
+    double gflops;         /* 2 * nnz / time */
+    double distance;       /* ||y_gpu - y_host||_2 after one SpMV from y = 0 */
+    double max_diff;       /* max_i | |y_host[i]| - |y_gpu[i]| | (two_vec_compare, src/util.cpp:93-131) */
+    double max_diff_ratio; /* the same difference over max(|y_host[i]|, |y_gpu[i]|) */
+} clspmv_bench_variant;
+
+typedef struct {
+    int method;
+    int nvariants;
+    int best;              /* index of the fastest variant that ran, -1 if none */
+    double best_ms, best_gflops;
+    clspmv_bench_variant v[CLSPMV_BENCH_MAX_VARIANTS];
+} clspmv_bench_result;
+
+/* The per-format benchmark drivers spmv_<fmt>(oclfilename, mat, dim2Size,
+ * ntimes, deviceType) of the reference (include/spmv_<fmt>.h;
+ * src/spmv_csr_scalar.cpp:670-713, spmv_csr_vector.cpp:619-664,
+ * spmv_bdia.cpp:413-441, spmv_dia.cpp:366-395, spmv_ell.cpp:330-359,
+ * spmv_coo.cpp:17-353, spmv_bell.cpp:345-399, spmv_bcsr.cpp:224-278,
+ * spmv_sell.cpp:331-412, spmv_sbell.cpp:225-305): convert the sorted COO
+ * `coo` to the method's format for every variant the reference sweeps, run
+ * one SpMV from y = 0 and compare it with the host coo_spmv answer, then
+ * time `ntimes` SpMVs (after 3 untimed ones) with CUDA events. x is all
+ * ones (i mod 1024 for SBELL, as the reference). With `verbose` the
+ * reference's report lines are printed to stdout. `out` may be NULL.
+ * Returns CLSPMV_ERR_REFUSED when no variant could be converted.
+ * Allocates and frees its own device buffers; synchronous. */
+int clspmv_run_method_f32(const clspmv_coo_f32* coo, int method, int ntimes, int verbose, clspmv_bench_result* out);
+
+/* Method 0 of spmv_all (src/mem_bandwidth.cpp): device copy bandwidth over
+ * `bytes` bytes and the launch overhead of an empty kernel, each the mean
+ * of `ntimes` runs. */
+int clspmv_bandwidth_test(size_t bytes, int ntimes, int verbose, double* copy_gbs, double* launch_us);
+
+/* evaluate (src/spmv_cocktail.cpp:1431-1455): upload the partitioned
+ * matrix, check one SpMV y = A*vec + res against `coores` (NULL: skip), then
+ * time `ntimes` SpMVs (the reference uses 1000). Prints the reference's
+ * report lines with `verbose`. Any of the out pointers may be NULL. */
+int clspmv_cocktail_evaluate_f32(const clspmv_cocktail_f32* host, const float* vec, const float* res,
+                                 const float* coores, int ntimes, int verbose, double* ms, double* gflops,
+                                 double* max_diff);
+
+/* ReadMMF (src/fileio.cpp:10-109): a Matrix Market coordinate file into a
+ * row-sorted COO (1-based indices made 0-based; pattern entries read as
+ * 1.0; a "symmetric" matrix gets its mirrored off-diagonal entries).
+ * CLSPMV_ERR_ARG when the file cannot be opened or parsed,
+ * CLSPMV_ERR_UNSUPPORTED for complex values. Release with
+ * clspmv_free_coo_f32. */
+int clspmv_read_mmf_f32(const char* filename, clspmv_coo_f32* out);
+
 /* Number of kernels this library launched since load (all entry points). */
 long long clspmv_launch_count(void);
 

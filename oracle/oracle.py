@@ -86,6 +86,7 @@ def ref():
                 "ref_coo2b4ell": (I, [_sp("coo"), _sp("b4ell"), U, U, I, I]),
                 "ref_coo2sbell": (I, [_sp("coo"), _sp("sbell"), U, U, U]),
                 "ref_spmv_only": (None, [_sp("coo"), VP, VP]),
+                "ref_read_mmf": (None, [C.c_char_p, _sp("coo")]),
                 "ref_analyze_matrix": (None, [_sp("coo"), C.POINTER(_abi.Cocktail), C.c_char_p, C.c_float, I, I]),
             }
             for fmt in ("dia", "bdia", "ell", "bcsr", "bell"):

@@ -13,6 +13,7 @@
 #include "spmv_serial.h"
 #include "util.h"
 #include "analyze.h"
+#include "fileio.h"
 #include "../include/clspmv_b200.h"
 
 typedef coo_matrix<int, float> coo_t;
@@ -86,5 +87,7 @@ void ref_analyze_matrix(clspmv_coo_f32* m, clspmv_cocktail_f32* out, const char*
 static_assert(sizeof(clspmv_cocktail_f32) == sizeof(cocktail<int, int, float>), "cocktail");
 // spmv_only: src/util.cpp:85-91 (zeroes y, then coo_spmv)
 void ref_spmv_only(clspmv_coo_f32* m, float* x, float* y) { spmv_only(R<coo_t>(m), x, y); }
+// ReadMMF: src/fileio.cpp:10-109 (arrays malloc'ed; release with ref_free)
+void ref_read_mmf(const char* path, clspmv_coo_f32* out) { ReadMMF(const_cast<char*>(path), R<coo_t>(out)); }
 
 }  // extern "C"
