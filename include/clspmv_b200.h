@@ -307,6 +307,27 @@ int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* dev, const int* tile_coord,
                               const float* x, float* y, float alpha, float beta,
                               clspmv_stream_t stream);
 
+/* The same merge-path SpMV for callers that cannot allocate device memory at
+ * the call (a running loop that must not call cudaMalloc/cudaFree, which can
+ * wait for the whole device; a binding with no device allocator; a service
+ * with a fixed memory budget). No counterpart in the reference. The tile
+ * plan is rebuilt on every call in a fixed array that is part of the
+ * library's device image (512 KiB per device), so the call allocates
+ * nothing. Limits and rules:
+ *  - rows + nnz must be at most clspmv_csr_merge_noalloc_max_tiles() * 2048
+ *    (134,215,680); larger matrices get CLSPMV_ERR_UNSUPPORTED and nothing
+ *    is launched;
+ *  - the first call on each device (with that device current) looks the
+ *    array up; make it before starting any stream capture on that device;
+ *  - nothing needs to start at zero: each call writes the whole plan it
+ *    reads, in `stream`, before its SpMV kernel;
+ *  - there is one array per device, so calls on one device must not
+ *    overlap: two in flight at once (other streams or threads) overwrite
+ *    each other's plan. Issue them on one stream or wait in between. */
+int clspmv_csr_merge_noalloc_max_tiles(void);
+int clspmv_csr_merge_spmv_noalloc_f32(const clspmv_csr_f32* dev, const float* x, float* y,
+                                      float alpha, float beta, clspmv_stream_t stream);
+
 /* COO, single-pass warp segmented reduction (row-sorted input). Replaces the
  * two-pass gpu_coo_s1/gpu_coo_s2 (kernels/spmv_coo.cl:4-217), driver
  * src/spmv_coo.cpp:17-353. */
