@@ -53,6 +53,9 @@ def parse_args():
     p.add_argument("--small", action="store_true", help="scaled-down matrices (quick check)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--only", default="", help="comma list of format keys to run (debugging)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the several-right-hand-side, batched and serving measurements")
+    p.add_argument("--serving-requests", type=int, default=1000)
     return p.parse_args()
 
 
@@ -485,6 +488,8 @@ def run_ours(args):
         "formats": formats,
         "variants": variant_stats,
     }
+    if not args.no_extras and not args.only:
+        line["extras"] = run_extras(args, items, mats, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)
         line["cpu_baseline"] = {"value": round(f_cpu / t_cpu / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
@@ -494,6 +499,57 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def run_extras(args, items, mats, peak):
+    """Several right-hand sides with FP32 / BF16 / FP16 values on the sweep's
+    matrices, 256 uneven matrices as one batched launch, and the serving
+    loop against sequential launches (Poisson arrivals)."""
+    import torch
+    from clspmv_mic_b200 import formats as F
+    from clspmv_mic_b200 import workloads as W
+    out = {}
+    t0 = time.perf_counter()
+    by_key = {it["key"]: it for it in items}
+    csr64 = {}
+    for name, arrs in mats.items():
+        csr_dev = by_key["csr_merge"]["dev"] if name == "powerlaw" else F.DeviceMatrix(F.coo2csr(F.coo_matrix(*arrs)))
+        csr64[name] = W.fp64_of_csr(csr_dev)
+        del csr_dev
+    entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_merge", "bcsr", "sbell")
+               if k in by_key]
+    out["spmm"] = {"note": "Y = A X, beta 0; GB/s over matrix bytes at the stored value width + k (4n + 4m); "
+                           "err_fp64 = max |Y - Y64| / (|A| |X|); CUDA cores (no tensor-core path)",
+                   "results": W.spmm_sweep(entries, hbm_gbs=peak)}
+    del csr64, entries
+    torch.cuda.empty_cache()
+    out["spmm"]["seconds"] = round(time.perf_counter() - t0, 1)
+
+    t0 = time.perf_counter()
+    mats256 = W.uneven_matrices(256)
+    out["batched"] = {"config": "256 CSR matrices, rows log-uniform [1k, 500k], 5-64 nnz/row, banded/blocked/random "
+                                "(generated on the device); one persistent launch replayed from a CUDA graph vs one "
+                                "plain launch per matrix",
+                      "nnz_total": int(sum(m.nnz for _, m in mats256)),
+                      "results": W.batched(mats256)}
+    del mats256
+    torch.cuda.empty_cache()
+    out["batched"]["seconds"] = round(time.perf_counter() - t0, 1)
+
+    t0 = time.perf_counter()
+    smats = W.serving_matrices(64)
+    nnz = int(sum(m.nnz for m in smats))
+    budget = 120 * 10 ** 9
+    out["serving"] = {"config": f"64 resident CSR matrices (rows 10k-4M, 20M-200M nnz, {nnz} nnz in all), "
+                                f"120 GB budget, Poisson arrivals, sequential = one plain launch + sync per request",
+                      "mixed_k": W.serve(smats, budget, args.serving_requests, rate=20_000.0, k_lo=1, k_hi=32),
+                      "k1": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1),
+                      "k1_bf16": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1,
+                                         value_type="bf16")}
+    del smats
+    torch.cuda.empty_cache()
+    out["serving"]["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def main():

@@ -96,6 +96,8 @@ class Cocktail(C.Structure):
                  ("ell", Ell), ("csr", Csr), ("coo", Coo)])
 
 
+FORMAT_IDS = {"csr": 0, "coo": 1, "dia": 2, "bdia": 3, "ell": 4, "sell": 5, "b4csr": 6, "b4ell": 7, "sbell": 8}
+VALUE_TYPES = {"f32": 0, "bf16": 1, "f16": 2}
 BENCH_MAX_VARIANTS = 16
 METHODS = {"bandwidth": 0, "csr_scalar": 1, "csr_vector": 2, "bdia": 3, "dia": 4, "ell": 5, "coo": 6, "bell": 7,
            "bcsr": 8, "sell": 9, "sbell": 10, "csr_merge": 11}
@@ -111,6 +113,12 @@ class BenchResult(C.Structure):
     """clspmv_bench_result: every variant a driver ran and the fastest."""
     _fields_ = [("method", I32), ("nvariants", I32), ("best", I32), ("best_ms", C.c_double),
                 ("best_gflops", C.c_double), ("v", BenchVariant * BENCH_MAX_VARIANTS)]
+
+
+class SpmmJob(C.Structure):
+    """clspmv_spmm_job: one Y <- alpha*A*X + beta*Y of a batch."""
+    _fields_ = [("format", I32), ("dev", VP), ("value_type", I32), ("values", VP), ("row_scale", VP), ("k", I32),
+                ("X", VP), ("ldx", I32), ("Y", VP), ("ldy", I32), ("alpha", C.c_float), ("beta", C.c_float)]
 
 
 def _n_bdia_data(s):
@@ -227,6 +235,13 @@ def _declare(lib):
         "clspmv_cocktail_evaluate_f32": (I32, [P(Cocktail), VP, VP, VP, I32, I32, P(C.c_double), P(C.c_double),
                                                P(C.c_double)]),
         "clspmv_read_mmf_f32": (I32, [C.c_char_p, S["coo"]]),
+        "clspmv_spmm": (I32, [I32, VP, I32, VP, VP, I32, VP, I32, VP, I32, f32, f32, VP]),
+        "clspmv_stored_values": (I32, [I32, VP, P(C.c_size_t)]),
+        "clspmv_pack_values": (I32, [I32, VP, I32, VP, VP, VP]),
+        "clspmv_batch_create": (I32, [I32, P(VP)]),
+        "clspmv_batch_set": (I32, [VP, P(SpmmJob), I32, VP, P(I32)]),
+        "clspmv_batch_run": (I32, [VP, VP]),
+        "clspmv_batch_free": (I32, [VP]),
     }
     for fmt in ("csr", "dia", "bdia", "ell", "sell", "bcsr", "bell", "b4csr", "b4ell", "sbell", "coo"):
         sigs[f"clspmv_{fmt}2coo_f32"] = (I32, [S[fmt], S["coo"]])

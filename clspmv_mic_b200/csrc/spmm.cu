@@ -1,0 +1,877 @@
+// spmm.cu — several right-hand sides at once, Y <- alpha * A * X + beta * Y,
+// for every device format, with FP32 values or values stored as BF16 / FP16
+// (indices untouched, per-row power-of-two scale, FP32 accumulation).
+//
+// The reference multiplies one vector per call (its kernels read `vec` and
+// `result`, e.g. kernels/spmv_ell.cl:4-30). Here X is n x k and Y is m x k,
+// both row major with leading dimensions ldx / ldy, k <= 128. Each row of A
+// is handled by a group of G lanes that split the k columns between them
+// (VEC = 4 columns per lane with 128-bit loads when X / Y rows are 16-byte
+// aligned, else 1), so every stored element of A is read once per group and
+// multiplies one contiguous row of X. The regular formats (DIA, BDIA, ELL,
+// SELL, b4csr, b4ell, SBELL) walk their own layout row by row; CSR and COO
+// split the nonzeros into equal chunks per group (power-law rows cost the
+// same as short ones) and add the partial sums of rows cut by a chunk edge
+// with vector atomics.
+//
+// Reduced-precision storage: clspmv_pack_values converts a device matrix's
+// FP32 values in place of a caller-supplied 16-bit array: every value of row
+// r is divided by s_r = 2^ceil(log2(max_j |a_rj|)) (exact) before rounding,
+// so FP16 keeps its full precision whatever the row's magnitude, and the
+// kernels multiply the row sum by s_r.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include "clspmv_b200.h"
+#include "api_internal.h"
+#include "common.cuh"
+
+using namespace clspmv;
+
+namespace {
+
+constexpr int kSpmmBlock = 256;
+constexpr int kSpmmMaxK = 128;
+
+template <class T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+
+template <class T> __device__ __forceinline__ T from_f(float v);
+template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
+
+template <class T> __device__ __forceinline__ T ld_val(const T* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// Row walks: for_row(m, r, f) calls f(col, idx) for every stored element of
+// row r whose column lies inside the matrix, idx indexing the value array.
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_dia_f32& m, int r, F&& f)
+{
+    const size_t len = (size_t)m.dia_length_aligned;
+    for (int d = 0; d < m.dia_num; d++) {
+        const int col = r + __ldg(m.dia_offsets + d);
+        if (col >= 0 && col < m.matinfo.width) f(col, (size_t)d * len + r);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_bdia_f32& m, int r, F&& f)
+{
+    const size_t len = (size_t)m.bdia_length_aligned;
+    for (int b = 0; b < m.bdia_band_num; b++) {
+        const int i0 = __ldg(m.bdia_bptr + b), i1 = __ldg(m.bdia_bptr + b + 1);
+        int col = r + __ldg(m.bdia_offsets + b);
+        for (int i = i0; i < i1; i++, col++)
+            if (col >= 0 && col < m.matinfo.width) f(col, (size_t)i * len + r);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_ell_f32& m, int r, F&& f)
+{
+    const size_t len = (size_t)m.ell_height_aligned;
+    for (int s = 0; s < m.ell_num; s++) {
+        const size_t idx = (size_t)s * len + r;
+        f(__ldg(m.ell_col_id + idx), idx);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_sell_f32& m, int r, F&& f)
+{
+    const int sh = (int)m.sell_slice_height;
+    const int sl = r / sh;
+    const int start = __ldg(m.sell_slice_ptr + sl);
+    const int width = (__ldg(m.sell_slice_ptr + sl + 1) - start) / sh;
+    for (int s = 0; s < width; s++) {
+        const size_t idx = (size_t)start + (size_t)s * sh + (r - sl * sh);
+        f(__ldg(m.sell_col_id + idx), idx);
+    }
+}
+
+// CSR rows for the batched kernel (one group per row; the single-matrix
+// path splits CSR by nonzeros instead).
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_csr_f32& m, int r, F&& f)
+{
+    const int j1 = __ldg(m.csr_row_ptr + r + 1);
+    for (int j = __ldg(m.csr_row_ptr + r); j < j1; j++) f(__ldg(m.csr_col_id + j), (size_t)j);
+}
+
+// Four consecutive columns of one float4 strip of a block (col0 .. col0+3),
+// stopping at the matrix width like the reference's serial sbell_spmv.
+template <class F>
+__device__ __forceinline__ void strip(int col0, size_t idx0, int width, F&& f)
+{
+#pragma unroll
+    for (int w = 0; w < 4; w++)
+        if (col0 + w < width) f(col0 + w, idx0 + w);
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_b4csr_f32& m, int r, F&& f)
+{
+    const int bh = (int)m.b4csr_bheight, bw4 = (int)m.b4csr_bwidth / 4;
+    const int br = r / bh, h = r - br * bh;
+    const size_t len = (size_t)m.b4csr_aligned_size;
+    const int i0 = __ldg(m.b4csr_row_ptr + br), i1 = __ldg(m.b4csr_row_ptr + br + 1);
+    for (int i = i0; i < i1; i++) {
+        const int c4 = __ldg(m.b4csr_col_id + i);
+        for (int w4 = 0; w4 < bw4; w4++)
+            strip((c4 + w4) * 4, (size_t)w4 * len * bh + (size_t)h * len + (size_t)i * 4, m.matinfo.width, f);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_b4ell_f32& m, int r, F&& f)
+{
+    const int bh = (int)m.b4ell_bheight, bw4 = (int)m.b4ell_bwidth / 4;
+    const int br = r / bh, h = r - br * bh;
+    const size_t len = (size_t)m.b4ell_height_aligned, f4 = (size_t)m.b4ell_float4_aligned;
+    for (int j = 0; j < m.b4ell_block_num; j++) {
+        const int c4 = __ldg(m.b4ell_col_id + (size_t)j * len + br);
+        for (int w4 = 0; w4 < bw4; w4++)
+            strip((c4 + w4) * 4, (size_t)j * f4 * bw4 * bh + (size_t)w4 * f4 * bh + (size_t)h * f4 + (size_t)br * 4,
+                  m.matinfo.width, f);
+    }
+}
+
+template <class F>
+__device__ __forceinline__ void for_row(const clspmv_sbell_f32& m, int r, F&& f)
+{
+    const int bh = (int)m.sbell_bheight, bw4 = (int)m.sbell_bwidth / 4, sh = (int)m.sbell_slice_height;
+    const int br = r / bh, h = r - br * bh;
+    const int sl = br / sh, s = br - sl * sh;
+    const int start = __ldg(m.sbell_slice_ptr + sl);
+    const int width = (__ldg(m.sbell_slice_ptr + sl + 1) - start) / sh;
+    const size_t base = (size_t)start * bw4 * 4 * bh + (size_t)s * 4;
+    for (int j = 0; j < width; j++) {
+        const int c4 = __ldg(m.sbell_col_id + (size_t)start + s + (size_t)j * sh);
+        for (int w4 = 0; w4 < bw4; w4++)
+            strip((c4 + w4) * 4, base + ((size_t)(j * bw4 + w4) * bh + h) * sh * 4, m.matinfo.width, f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Lane helpers: a lane owns VEC consecutive columns c0 .. c0+VEC-1 of X / Y.
+// ---------------------------------------------------------------------------
+template <int VEC> struct Acc;
+template <> struct Acc<1> {
+    float v = 0.0f;
+    __device__ void fma(float a, const float* x) { v = fmaf(a, __ldg(x), v); }
+    __device__ void store(float* y, float alpha, float beta) const
+    {
+        *y = beta == 0.0f ? alpha * v : fmaf(beta, *y, alpha * v);
+    }
+    __device__ void add(float* y, float alpha) const { *y += alpha * v; }
+    __device__ void atomic(float* y, float alpha) const { atomicAdd(y, alpha * v); }
+};
+template <> struct Acc<4> {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    __device__ void fma(float a, const float* x)
+    {
+        const float4 xv = __ldg(reinterpret_cast<const float4*>(x));
+        v.x = fmaf(a, xv.x, v.x);
+        v.y = fmaf(a, xv.y, v.y);
+        v.z = fmaf(a, xv.z, v.z);
+        v.w = fmaf(a, xv.w, v.w);
+    }
+    __device__ void store(float* y, float alpha, float beta) const
+    {
+        float4 o = make_float4(alpha * v.x, alpha * v.y, alpha * v.z, alpha * v.w);
+        if (beta != 0.0f) {
+            const float4 p = *reinterpret_cast<const float4*>(y);
+            o.x = fmaf(beta, p.x, o.x);
+            o.y = fmaf(beta, p.y, o.y);
+            o.z = fmaf(beta, p.z, o.z);
+            o.w = fmaf(beta, p.w, o.w);
+        }
+        *reinterpret_cast<float4*>(y) = o;
+    }
+    __device__ void add(float* y, float alpha) const
+    {
+        float4 p = *reinterpret_cast<float4*>(y);
+        p.x += alpha * v.x;
+        p.y += alpha * v.y;
+        p.z += alpha * v.z;
+        p.w += alpha * v.w;
+        *reinterpret_cast<float4*>(y) = p;
+    }
+    __device__ void atomic(float* y, float alpha) const
+    {
+        atomicAdd(reinterpret_cast<float4*>(y), make_float4(alpha * v.x, alpha * v.y, alpha * v.z, alpha * v.w));
+    }
+};
+
+struct Dense {
+    int k;
+    const float* X;
+    int ldx;
+    float* Y;
+    int ldy;
+    float alpha, beta;
+    const float* scale;   // per-row scale of packed values, or nullptr
+    int lshift;           // log2 of lanes per row group
+};
+
+// Row-walk kernel: one group of 2^lshift lanes per row, grid-stride over rows.
+template <int VEC, class T, class M>
+__global__ void __launch_bounds__(kSpmmBlock) k_spmm_rows(M m, const T* __restrict__ vals, Dense d)
+{
+    const int G = 1 << d.lshift;
+    const long long t = (long long)blockIdx.x * kSpmmBlock + threadIdx.x;
+    const int lane = (int)(t & (G - 1));
+    const int c0 = lane * VEC;
+    if (c0 >= d.k) return;                      // lanes past k have no columns
+    const long long groups = ((long long)gridDim.x * kSpmmBlock) >> d.lshift;
+    for (long long r = t >> d.lshift; r < m.matinfo.height; r += groups) {
+        Acc<VEC> acc;
+        for_row(m, (int)r, [&](int col, size_t idx) { acc.fma(to_f(ld_val(vals + idx)), d.X + (size_t)col * d.ldx + c0); });
+        const float a = d.scale ? d.alpha * d.scale[r] : d.alpha;
+        acc.store(d.Y + (size_t)r * d.ldy + c0, a, d.beta);
+    }
+}
+
+// Nonzero-chunk kernel for CSR (row_ptr) and row-sorted COO (row_id). Y must
+// already hold beta * Y. A row wholly inside a chunk is added with a plain
+// read-modify-write; a row cut by a chunk edge is added atomically.
+template <int VEC, class T, bool IS_CSR>
+__global__ void __launch_bounds__(kSpmmBlock) k_spmm_chunks(int rows, int nnz, const int* __restrict__ row_ptr,
+                                                            const int* __restrict__ row_id, const int* __restrict__ col_id,
+                                                            const T* __restrict__ vals, int chunk, Dense d)
+{
+    const int G = 1 << d.lshift;
+    const long long t = (long long)blockIdx.x * kSpmmBlock + threadIdx.x;
+    const int lane = (int)(t & (G - 1));
+    const int c0 = lane * VEC;
+    if (c0 >= d.k) return;
+    const long long g = t >> d.lshift;
+    const long long e0l = g * chunk;
+    if (e0l >= nnz) return;
+    const int e0 = (int)e0l;
+    const int e1 = (int)min((long long)nnz, e0l + chunk);
+    int row, row_end = 0;
+    if (IS_CSR) {   // last row whose start is <= e0 (skips empty rows)
+        int lo = 0, hi = rows;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(row_ptr + mid) <= e0) lo = mid;
+            else hi = mid - 1;
+        }
+        row = lo;
+        row_end = __ldg(row_ptr + row + 1);
+    } else {
+        row = __ldg(row_id + e0);
+    }
+    bool first = true;   // the current row may have started before e0
+    Acc<VEC> acc;
+    // A row is cut by the chunk if it started before e0 (only the first row
+    // can) or continues past e1 (only the last row can).
+    auto flush = [&](bool last) {
+        const float a = d.scale ? d.alpha * d.scale[row] : d.alpha;
+        float* y = d.Y + (size_t)row * d.ldy + c0;
+        bool cut = false;
+        if (first) cut = IS_CSR ? __ldg(row_ptr + row) < e0 : (e0 > 0 && __ldg(row_id + e0 - 1) == row);
+        if (last) cut = cut || (IS_CSR ? row_end > e1 : (e1 < nnz && __ldg(row_id + e1) == row));
+        if (cut) acc.atomic(y, a);
+        else acc.add(y, a);
+    };
+    for (int e = e0; e < e1; e++) {
+        if (IS_CSR) {
+            if (e >= row_end) {
+                flush(false);
+                first = false;
+                acc = Acc<VEC>();
+                do {
+                    row++;
+                    row_end = __ldg(row_ptr + row + 1);
+                } while (e >= row_end);
+            }
+        } else {
+            const int r = __ldg(row_id + e);
+            if (r != row) {
+                flush(false);
+                first = false;
+                acc = Acc<VEC>();
+                row = r;
+            }
+        }
+        acc.fma(to_f(ld_val(vals + e)), d.X + (size_t)__ldg(col_id + e) * d.ldx + c0);
+    }
+    flush(true);
+}
+
+__global__ void k_scale_rows(float* Y, int rows, int k, int ldy, float beta)
+{
+    const long long n = (long long)rows * k;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / k, c = i - r * k;
+        float* p = Y + r * ldy + c;
+        *p = beta == 0.0f ? 0.0f : beta * *p;
+    }
+}
+
+// Packing: per-row scale (pass 1), then the scaled 16-bit values (pass 2).
+__device__ __forceinline__ float pow2_at_least(float s)
+{
+    if (!(s > 0.0f) || isinf(s)) return 1.0f;
+    int e;
+    const float f = frexpf(s, &e);   // s = f * 2^e, f in [0.5, 1)
+    (void)f;
+    return ldexpf(1.0f, e);
+}
+
+template <class T, class M>
+__global__ void k_pack_rows(M m, const float* __restrict__ src, T* __restrict__ dst, float* __restrict__ scale)
+{
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < m.matinfo.height;
+         r += (long long)gridDim.x * blockDim.x) {
+        float mx = 0.0f;
+        for_row(m, (int)r, [&](int, size_t idx) { mx = fmaxf(mx, fabsf(src[idx])); });
+        const float s = pow2_at_least(mx), inv = 1.0f / s;   // exact: s is a power of two
+        scale[r] = s;
+        for_row(m, (int)r, [&](int, size_t idx) { dst[idx] = from_f<T>(src[idx] * inv); });
+    }
+}
+
+template <class T>
+__global__ void k_pack_csr(int rows, const int* __restrict__ row_ptr, const float* __restrict__ src, T* __restrict__ dst,
+                           float* __restrict__ scale)
+{
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (long long)gridDim.x * blockDim.x) {
+        const int a = row_ptr[r], b = row_ptr[r + 1];
+        float mx = 0.0f;
+        for (int j = a; j < b; j++) mx = fmaxf(mx, fabsf(src[j]));
+        const float s = pow2_at_least(mx), inv = 1.0f / s;
+        scale[r] = s;
+        for (int j = a; j < b; j++) dst[j] = from_f<T>(src[j] * inv);
+    }
+}
+
+// COO rows are runs of equal row ids: the thread at the start of a run packs it.
+template <class T>
+__global__ void k_pack_coo(int nnz, const int* __restrict__ row_id, const float* __restrict__ src, T* __restrict__ dst,
+                           float* __restrict__ scale)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+        const int r = row_id[e];
+        if (e > 0 && row_id[e - 1] == r) continue;
+        long long f = e;
+        float mx = 0.0f;
+        for (; f < nnz && row_id[f] == r; f++) mx = fmaxf(mx, fabsf(src[f]));
+        const float s = pow2_at_least(mx), inv = 1.0f / s;
+        scale[r] = s;
+        for (long long j = e; j < f; j++) dst[j] = from_f<T>(src[j] * inv);
+    }
+}
+
+__global__ void k_fill(float* p, int n, float v)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+int grid_of(long long threads, int block = kSpmmBlock)
+{
+    long long g = (threads + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148LL * 64) g = 148LL * 64;
+    return (int)g;
+}
+
+int log2_ceil(int v)
+{
+    int s = 0;
+    while ((1 << s) < v) s++;
+    return s;
+}
+
+// Lanes per row group and the vector width for k, X and Y.
+int plan_lanes(int k, const float* X, int ldx, const float* Y, int ldy, int* vec, int* lshift)
+{
+    if (k < 1 || k > kSpmmMaxK || ldx < k || ldy < k) return CLSPMV_ERR_ARG;
+    const bool v4 = k % 4 == 0 && ldx % 4 == 0 && ldy % 4 == 0 && ((uintptr_t)X & 15) == 0 && ((uintptr_t)Y & 15) == 0;
+    if (!v4 && k > 32) return CLSPMV_ERR_ALIGN;   // more than 32 lanes per row otherwise
+    *vec = v4 ? 4 : 1;
+    *lshift = log2_ceil(v4 ? k / 4 : k);
+    return CLSPMV_OK;
+}
+
+template <class M> const float* values_of(const M& m);
+template <> const float* values_of(const clspmv_dia_f32& m) { return m.dia_data; }
+template <> const float* values_of(const clspmv_bdia_f32& m) { return m.bdia_data; }
+template <> const float* values_of(const clspmv_ell_f32& m) { return m.ell_data; }
+template <> const float* values_of(const clspmv_sell_f32& m) { return m.sell_data; }
+template <> const float* values_of(const clspmv_b4csr_f32& m) { return m.b4csr_data; }
+template <> const float* values_of(const clspmv_b4ell_f32& m) { return m.b4ell_data; }
+template <> const float* values_of(const clspmv_sbell_f32& m) { return m.sbell_data; }
+
+template <class T, class M>
+int launch_rows(const M& m, const void* vals, Dense d, int vec, cudaStream_t st)
+{
+    const long long threads = (long long)m.matinfo.height << d.lshift;
+    const int grid = grid_of(threads);
+    const T* v = static_cast<const T*>(vals);
+    if (vec == 4) k_spmm_rows<4, T, M><<<grid, kSpmmBlock, 0, st>>>(m, v, d);
+    else k_spmm_rows<1, T, M><<<grid, kSpmmBlock, 0, st>>>(m, v, d);
+    return after_launch(1);
+}
+
+template <class T, bool IS_CSR>
+int launch_chunks(int rows, int nnz, const int* row_ptr, const int* row_id, const int* col_id, const void* vals, Dense d,
+                  int vec, cudaStream_t st)
+{
+    if (d.beta != 1.0f) {
+        k_scale_rows<<<grid_of((long long)rows * d.k), kSpmmBlock, 0, st>>>(d.Y, rows, d.k, d.ldy, d.beta);
+        int rc = after_launch(1);
+        if (rc) return rc;
+    }
+    if (nnz <= 0) return CLSPMV_OK;
+    // about 16 row-sum updates of X per lane: enough work to hide the search
+    const int chunk = d.k <= 4 ? 32 : 16;
+    const long long groups = ((long long)nnz + chunk - 1) / chunk;
+    const long long threads = groups << d.lshift;
+    const int grid = (int)((threads + kSpmmBlock - 1) / kSpmmBlock);
+    const T* v = static_cast<const T*>(vals);
+    if (vec == 4) k_spmm_chunks<4, T, IS_CSR><<<grid, kSpmmBlock, 0, st>>>(rows, nnz, row_ptr, row_id, col_id, v, chunk, d);
+    else k_spmm_chunks<1, T, IS_CSR><<<grid, kSpmmBlock, 0, st>>>(rows, nnz, row_ptr, row_id, col_id, v, chunk, d);
+    return after_launch(1);
+}
+
+template <class T>
+int spmm_typed(int format, const void* dev, const void* vals, Dense d, int vec, cudaStream_t st)
+{
+    switch (format) {
+        case CLSPMV_FORMAT_CSR: {
+            const auto& m = *static_cast<const clspmv_csr_f32*>(dev);
+            if (!m.csr_row_ptr) return CLSPMV_ERR_ARG;
+            return launch_chunks<T, true>(m.matinfo.height, m.matinfo.nnz, m.csr_row_ptr, nullptr, m.csr_col_id,
+                                          vals ? vals : m.csr_data, d, vec, st);
+        }
+        case CLSPMV_FORMAT_COO: {
+            const auto& m = *static_cast<const clspmv_coo_f32*>(dev);
+            return launch_chunks<T, false>(m.matinfo.height, m.matinfo.nnz, nullptr, m.coo_row_id, m.coo_col_id,
+                                           vals ? vals : m.coo_data, d, vec, st);
+        }
+#define ROWS(FMT, TYPE)                                                              \
+    case FMT: {                                                                      \
+        const auto& m = *static_cast<const TYPE*>(dev);                              \
+        return launch_rows<T>(m, vals ? vals : values_of(m), d, vec, st);            \
+    }
+        ROWS(CLSPMV_FORMAT_DIA, clspmv_dia_f32)
+        ROWS(CLSPMV_FORMAT_BDIA, clspmv_bdia_f32)
+        ROWS(CLSPMV_FORMAT_ELL, clspmv_ell_f32)
+        ROWS(CLSPMV_FORMAT_SELL, clspmv_sell_f32)
+        ROWS(CLSPMV_FORMAT_B4CSR, clspmv_b4csr_f32)
+        ROWS(CLSPMV_FORMAT_B4ELL, clspmv_b4ell_f32)
+        ROWS(CLSPMV_FORMAT_SBELL, clspmv_sbell_f32)
+#undef ROWS
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int read_int(const int* dev_ptr, int* out)
+{
+    return cuda_status(cudaMemcpy(out, dev_ptr, sizeof(int), cudaMemcpyDeviceToHost));
+}
+
+bool block_ok(unsigned bw, unsigned bh) { return (bw == 4 || bw == 8) && (bh == 1 || bh == 2 || bh == 4 || bh == 8); }
+
+template <class T>
+int pack_typed(int format, const void* dev, T* dst, float* scale, cudaStream_t st)
+{
+    switch (format) {
+        case CLSPMV_FORMAT_CSR: {
+            const auto& m = *static_cast<const clspmv_csr_f32*>(dev);
+            k_pack_csr<T><<<grid_of(m.matinfo.height), kSpmmBlock, 0, st>>>(m.matinfo.height, m.csr_row_ptr, m.csr_data,
+                                                                           dst, scale);
+            return after_launch(1);
+        }
+        case CLSPMV_FORMAT_COO: {
+            const auto& m = *static_cast<const clspmv_coo_f32*>(dev);
+            k_fill<<<grid_of(m.matinfo.height), kSpmmBlock, 0, st>>>(scale, m.matinfo.height, 1.0f);
+            int rc = after_launch(1);
+            if (rc || m.matinfo.nnz <= 0) return rc;
+            k_pack_coo<T><<<grid_of(m.matinfo.nnz), kSpmmBlock, 0, st>>>(m.matinfo.nnz, m.coo_row_id, m.coo_data, dst, scale);
+            return after_launch(1);
+        }
+#define PACK(FMT, TYPE)                                                                       \
+    case FMT: {                                                                               \
+        const auto& m = *static_cast<const TYPE*>(dev);                                       \
+        k_pack_rows<T, TYPE><<<grid_of(m.matinfo.height), kSpmmBlock, 0, st>>>(m, values_of(m), dst, scale); \
+        return after_launch(1);                                                               \
+    }
+        PACK(CLSPMV_FORMAT_DIA, clspmv_dia_f32)
+        PACK(CLSPMV_FORMAT_BDIA, clspmv_bdia_f32)
+        PACK(CLSPMV_FORMAT_ELL, clspmv_ell_f32)
+        PACK(CLSPMV_FORMAT_SELL, clspmv_sell_f32)
+        PACK(CLSPMV_FORMAT_B4CSR, clspmv_b4csr_f32)
+        PACK(CLSPMV_FORMAT_B4ELL, clspmv_b4ell_f32)
+        PACK(CLSPMV_FORMAT_SBELL, clspmv_sbell_f32)
+#undef PACK
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int check_struct(int format, const void* dev)
+{
+    if (!dev) return CLSPMV_ERR_ARG;
+    switch (format) {
+        case CLSPMV_FORMAT_B4CSR: {
+            const auto& m = *static_cast<const clspmv_b4csr_f32*>(dev);
+            return block_ok(m.b4csr_bwidth, m.b4csr_bheight) ? CLSPMV_OK : CLSPMV_ERR_UNSUPPORTED;
+        }
+        case CLSPMV_FORMAT_B4ELL: {
+            const auto& m = *static_cast<const clspmv_b4ell_f32*>(dev);
+            return block_ok(m.b4ell_bwidth, m.b4ell_bheight) ? CLSPMV_OK : CLSPMV_ERR_UNSUPPORTED;
+        }
+        case CLSPMV_FORMAT_SBELL: {
+            const auto& m = *static_cast<const clspmv_sbell_f32*>(dev);
+            return block_ok(m.sbell_bwidth, m.sbell_bheight) && m.sbell_slice_height > 0 ? CLSPMV_OK : CLSPMV_ERR_UNSUPPORTED;
+        }
+        case CLSPMV_FORMAT_SELL:
+            return static_cast<const clspmv_sell_f32*>(dev)->sell_slice_height > 0 ? CLSPMV_OK : CLSPMV_ERR_UNSUPPORTED;
+        case CLSPMV_FORMAT_CSR:
+        case CLSPMV_FORMAT_COO:
+        case CLSPMV_FORMAT_DIA:
+        case CLSPMV_FORMAT_BDIA:
+        case CLSPMV_FORMAT_ELL:
+            return CLSPMV_OK;
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+// every format struct starts with its matinfo
+int matrix_rows(const void* dev) { return static_cast<const clspmv_matinfo*>(dev)->height; }
+
+
+// ---------------------------------------------------------------------------
+// Batches: many (matrix, X, Y) jobs in one persistent launch. Each job is cut
+// into warp tasks of 32 / G rows (G lanes per row for its k); the tasks of all
+// jobs form one index space that every warp strides through, finding its job
+// by binary search over the jobs' first task numbers.
+// ---------------------------------------------------------------------------
+struct BatchJob {
+    int format, value_type, k, lshift, vec, rows;
+    long long task_begin;
+    int ldx, ldy;
+    float alpha, beta;
+    const void* values;
+    const float* scale;
+    const float* X;
+    float* Y;
+    union {
+        clspmv_csr_f32 csr;
+        clspmv_dia_f32 dia;
+        clspmv_bdia_f32 bdia;
+        clspmv_ell_f32 ell;
+        clspmv_sell_f32 sell;
+        clspmv_b4csr_f32 b4csr;
+        clspmv_b4ell_f32 b4ell;
+        clspmv_sbell_f32 sbell;
+    } m;
+};
+
+template <int VEC, class T, class M>
+__device__ __forceinline__ void batch_row(const M& m, const BatchJob& J, int r, int c0)
+{
+    const T* vals = static_cast<const T*>(J.values);
+    Acc<VEC> acc;
+    for_row(m, r, [&](int col, size_t idx) { acc.fma(to_f(ld_val(vals + idx)), J.X + (size_t)col * J.ldx + c0); });
+    const float a = J.scale ? J.alpha * J.scale[r] : J.alpha;
+    acc.store(J.Y + (size_t)r * J.ldy + c0, a, J.beta);
+}
+
+template <int VEC, class T>
+__device__ __forceinline__ void batch_dispatch(const BatchJob& J, int r, int c0)
+{
+    switch (J.format) {
+        case CLSPMV_FORMAT_CSR: batch_row<VEC, T>(J.m.csr, J, r, c0); break;
+        case CLSPMV_FORMAT_DIA: batch_row<VEC, T>(J.m.dia, J, r, c0); break;
+        case CLSPMV_FORMAT_BDIA: batch_row<VEC, T>(J.m.bdia, J, r, c0); break;
+        case CLSPMV_FORMAT_ELL: batch_row<VEC, T>(J.m.ell, J, r, c0); break;
+        case CLSPMV_FORMAT_SELL: batch_row<VEC, T>(J.m.sell, J, r, c0); break;
+        case CLSPMV_FORMAT_B4CSR: batch_row<VEC, T>(J.m.b4csr, J, r, c0); break;
+        case CLSPMV_FORMAT_B4ELL: batch_row<VEC, T>(J.m.b4ell, J, r, c0); break;
+        case CLSPMV_FORMAT_SBELL: batch_row<VEC, T>(J.m.sbell, J, r, c0); break;
+    }
+}
+
+__global__ void __launch_bounds__(kSpmmBlock) k_batch(const BatchJob* __restrict__ jobs, int njobs, long long tasks)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * kSpmmBlock) >> 5;
+    for (long long t = ((long long)blockIdx.x * kSpmmBlock + threadIdx.x) >> 5; t < tasks; t += nwarps) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].task_begin <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchJob& J = jobs[lo];
+        const long long r = (t - J.task_begin) * (32 >> J.lshift) + (lane >> J.lshift);
+        const int c0 = (lane & ((1 << J.lshift) - 1)) * J.vec;
+        if (r >= J.rows || c0 >= J.k) continue;
+        if (J.vec == 4) {
+            if (J.value_type == CLSPMV_VALUES_F32) batch_dispatch<4, float>(J, (int)r, c0);
+            else if (J.value_type == CLSPMV_VALUES_BF16) batch_dispatch<4, __nv_bfloat16>(J, (int)r, c0);
+            else batch_dispatch<4, __half>(J, (int)r, c0);
+        } else {
+            if (J.value_type == CLSPMV_VALUES_F32) batch_dispatch<1, float>(J, (int)r, c0);
+            else if (J.value_type == CLSPMV_VALUES_BF16) batch_dispatch<1, __nv_bfloat16>(J, (int)r, c0);
+            else batch_dispatch<1, __half>(J, (int)r, c0);
+        }
+    }
+}
+
+int batch_grid()
+{
+    static int grid = 0;
+    if (!grid) {
+        int dev = 0, nsm = 148, per = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch, kSpmmBlock, 0) != cudaSuccess || per < 1) {
+            cudaGetLastError();
+            per = 1;
+        }
+        grid = nsm * per;
+    }
+    return grid;
+}
+
+// Fills one device job from a caller's job description.
+int make_job(const clspmv_spmm_job& in, BatchJob& out)
+{
+    int rc = check_struct(in.format, in.dev);
+    if (rc) return rc;
+    if (in.format == CLSPMV_FORMAT_COO) return CLSPMV_ERR_UNSUPPORTED;   // no row starts to walk
+    if (!in.X || !in.Y) return CLSPMV_ERR_ARG;
+    if (in.value_type != CLSPMV_VALUES_F32 && in.value_type != CLSPMV_VALUES_BF16 && in.value_type != CLSPMV_VALUES_F16)
+        return CLSPMV_ERR_ARG;
+    if (in.value_type != CLSPMV_VALUES_F32 && (!in.values || !in.row_scale)) return CLSPMV_ERR_ARG;
+    memset(&out, 0, sizeof(out));
+    if ((rc = plan_lanes(in.k, in.X, in.ldx, in.Y, in.ldy, &out.vec, &out.lshift))) return rc;
+    out.format = in.format;
+    out.value_type = in.value_type;
+    out.k = in.k;
+    out.rows = matrix_rows(in.dev);
+    out.ldx = in.ldx;
+    out.ldy = in.ldy;
+    out.alpha = in.alpha;
+    out.beta = in.beta;
+    out.scale = in.value_type == CLSPMV_VALUES_F32 ? nullptr : in.row_scale;
+    out.X = in.X;
+    out.Y = in.Y;
+    switch (in.format) {
+        case CLSPMV_FORMAT_CSR: out.m.csr = *static_cast<const clspmv_csr_f32*>(in.dev); out.values = out.m.csr.csr_data; break;
+        case CLSPMV_FORMAT_DIA: out.m.dia = *static_cast<const clspmv_dia_f32*>(in.dev); out.values = out.m.dia.dia_data; break;
+        case CLSPMV_FORMAT_BDIA: out.m.bdia = *static_cast<const clspmv_bdia_f32*>(in.dev); out.values = out.m.bdia.bdia_data; break;
+        case CLSPMV_FORMAT_ELL: out.m.ell = *static_cast<const clspmv_ell_f32*>(in.dev); out.values = out.m.ell.ell_data; break;
+        case CLSPMV_FORMAT_SELL: out.m.sell = *static_cast<const clspmv_sell_f32*>(in.dev); out.values = out.m.sell.sell_data; break;
+        case CLSPMV_FORMAT_B4CSR: out.m.b4csr = *static_cast<const clspmv_b4csr_f32*>(in.dev); out.values = out.m.b4csr.b4csr_data; break;
+        case CLSPMV_FORMAT_B4ELL: out.m.b4ell = *static_cast<const clspmv_b4ell_f32*>(in.dev); out.values = out.m.b4ell.b4ell_data; break;
+        case CLSPMV_FORMAT_SBELL: out.m.sbell = *static_cast<const clspmv_sbell_f32*>(in.dev); out.values = out.m.sbell.sbell_data; break;
+    }
+    if (in.value_type != CLSPMV_VALUES_F32) out.values = in.values;
+    if (out.format == CLSPMV_FORMAT_CSR && !out.m.csr.csr_row_ptr) return CLSPMV_ERR_ARG;
+    return CLSPMV_OK;
+}
+
+}  // namespace
+
+struct clspmv_batch {
+    int capacity = 0;
+    int njobs = 0;
+    long long tasks = 0;
+    BatchJob* host = nullptr;     // pinned staging of the job table
+    BatchJob* dev = nullptr;
+    cudaEvent_t copied = nullptr; // the last table upload has left `host`
+};
+
+namespace {
+}  // namespace
+
+extern "C" {
+
+int clspmv_stored_values(int format, const void* dev, size_t* count)
+{
+    int rc = check_struct(format, dev);
+    if (rc) return rc;
+    if (!count) return CLSPMV_ERR_ARG;
+    int last = 0;
+    switch (format) {
+        case CLSPMV_FORMAT_CSR: *count = (size_t)static_cast<const clspmv_csr_f32*>(dev)->matinfo.nnz; return CLSPMV_OK;
+        case CLSPMV_FORMAT_COO: *count = (size_t)static_cast<const clspmv_coo_f32*>(dev)->matinfo.nnz; return CLSPMV_OK;
+        case CLSPMV_FORMAT_DIA: {
+            const auto& m = *static_cast<const clspmv_dia_f32*>(dev);
+            *count = (size_t)m.dia_num * m.dia_length_aligned;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_BDIA: {
+            const auto& m = *static_cast<const clspmv_bdia_f32*>(dev);
+            if (m.bdia_band_num > 0 && (rc = read_int(m.bdia_bptr + m.bdia_band_num, &last))) return rc;
+            *count = (size_t)last * m.bdia_length_aligned;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_ELL: {
+            const auto& m = *static_cast<const clspmv_ell_f32*>(dev);
+            *count = (size_t)m.ell_num * m.ell_height_aligned;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_SELL: {
+            const auto& m = *static_cast<const clspmv_sell_f32*>(dev);
+            if ((rc = read_int(m.sell_slice_ptr + m.sell_slice_num, &last))) return rc;
+            *count = (size_t)last;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_B4CSR: {
+            const auto& m = *static_cast<const clspmv_b4csr_f32*>(dev);
+            *count = (size_t)m.b4csr_aligned_size * m.b4csr_bwidth * m.b4csr_bheight / 4;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_B4ELL: {
+            const auto& m = *static_cast<const clspmv_b4ell_f32*>(dev);
+            *count = (size_t)m.b4ell_block_num * m.b4ell_float4_aligned * (m.b4ell_bwidth / 4) * m.b4ell_bheight;
+            return CLSPMV_OK;
+        }
+        case CLSPMV_FORMAT_SBELL: {
+            const auto& m = *static_cast<const clspmv_sbell_f32*>(dev);
+            if ((rc = read_int(m.sbell_slice_ptr + m.sbell_slice_num, &last))) return rc;
+            *count = (size_t)last * m.sbell_bwidth * m.sbell_bheight;
+            return CLSPMV_OK;
+        }
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int clspmv_pack_values(int format, const void* dev, int value_type, void* values, float* row_scale,
+                       clspmv_stream_t stream)
+{
+    int rc = check_struct(format, dev);
+    if (rc) return rc;
+    if (!values || !row_scale) return CLSPMV_ERR_ARG;
+    size_t count = 0;
+    if ((rc = clspmv_stored_values(format, dev, &count))) return rc;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // entries no row walk reaches (padding rows, out-of-range diagonals) stay 0
+    if ((rc = cuda_status(cudaMemsetAsync(values, 0, count * 2, st)))) return rc;
+    if (matrix_rows(dev) <= 0) return CLSPMV_OK;
+    if (value_type == CLSPMV_VALUES_BF16) return pack_typed(format, dev, static_cast<__nv_bfloat16*>(values), row_scale, st);
+    if (value_type == CLSPMV_VALUES_F16) return pack_typed(format, dev, static_cast<__half*>(values), row_scale, st);
+    return CLSPMV_ERR_ARG;
+}
+
+int clspmv_spmm(int format, const void* dev, int value_type, const void* values, const float* row_scale, int k,
+                const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream)
+{
+    int rc = check_struct(format, dev);
+    if (rc) return rc;
+    if (!X || !Y) return CLSPMV_ERR_ARG;
+    if (value_type != CLSPMV_VALUES_F32 && (!values || !row_scale)) return CLSPMV_ERR_ARG;
+    int vec = 1, lshift = 0;
+    if ((rc = plan_lanes(k, X, ldx, Y, ldy, &vec, &lshift))) return rc;
+    if (matrix_rows(dev) <= 0) return CLSPMV_OK;
+    Dense d{k, X, ldx, Y, ldy, alpha, beta, value_type == CLSPMV_VALUES_F32 ? nullptr : row_scale, lshift};
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    switch (value_type) {
+        case CLSPMV_VALUES_F32: return spmm_typed<float>(format, dev, nullptr, d, vec, st);
+        case CLSPMV_VALUES_BF16: return spmm_typed<__nv_bfloat16>(format, dev, values, d, vec, st);
+        case CLSPMV_VALUES_F16: return spmm_typed<__half>(format, dev, values, d, vec, st);
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int clspmv_batch_create(int max_jobs, clspmv_batch** out)
+{
+    if (!out || max_jobs < 1) return CLSPMV_ERR_ARG;
+    *out = nullptr;
+    clspmv_batch* b = new (std::nothrow) clspmv_batch();
+    if (!b) return CLSPMV_ERR_ALLOC;
+    b->capacity = max_jobs;
+    int rc = cuda_status(cudaMallocHost(&b->host, sizeof(BatchJob) * max_jobs));
+    if (!rc) rc = cuda_status(cudaMalloc(&b->dev, sizeof(BatchJob) * max_jobs));
+    if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming));
+    if (rc) {
+        clspmv_batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return CLSPMV_OK;
+}
+
+int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, clspmv_stream_t stream, int* bad_job)
+{
+    if (bad_job) *bad_job = -1;
+    if (!b || (!jobs && njobs > 0) || njobs < 0) return CLSPMV_ERR_ARG;
+    if (njobs > b->capacity) return CLSPMV_ERR_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    int rc = cuda_status(cudaEventSynchronize(b->copied));   // staging free again
+    if (rc) return rc;
+    long long tasks = 0;
+    for (int i = 0; i < njobs; i++) {
+        BatchJob& J = b->host[i];
+        if ((rc = make_job(jobs[i], J))) {
+            if (bad_job) *bad_job = i;
+            b->njobs = 0;
+            b->tasks = 0;
+            return rc;
+        }
+        J.task_begin = tasks;
+        tasks += (J.rows + (32 >> J.lshift) - 1) / (32 >> J.lshift);
+    }
+    b->njobs = njobs;
+    b->tasks = tasks;
+    if (njobs == 0) return CLSPMV_OK;
+    rc = cuda_status(cudaMemcpyAsync(b->dev, b->host, sizeof(BatchJob) * njobs, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = cuda_status(cudaEventRecord(b->copied, st));
+    return rc;
+}
+
+int clspmv_batch_run(clspmv_batch* b, clspmv_stream_t stream)
+{
+    if (!b) return CLSPMV_ERR_ARG;
+    if (b->tasks == 0) return CLSPMV_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const long long grid = std::min<long long>(batch_grid(), (b->tasks + 7) / 8);
+    k_batch<<<(int)grid, kSpmmBlock, 0, st>>>(b->dev, b->njobs, b->tasks);
+    return after_launch(1);
+}
+
+int clspmv_batch_free(clspmv_batch* b)
+{
+    if (!b) return CLSPMV_ERR_ARG;
+    if (b->copied) {
+        cudaEventSynchronize(b->copied);
+        cudaEventDestroy(b->copied);
+    }
+    if (b->host) cudaFreeHost(b->host);
+    if (b->dev) cudaFree(b->dev);
+    delete b;
+    return CLSPMV_OK;
+}
+
+#define SPMM_ENTRY(name, FMT, TYPE)                                                                        \
+    int clspmv_##name##_spmm_f32(const TYPE* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, \
+                                 float beta, clspmv_stream_t stream)                                              \
+    {                                                                                                             \
+        return clspmv_spmm(FMT, dev, CLSPMV_VALUES_F32, nullptr, nullptr, k, X, ldx, Y, ldy, alpha, beta, stream); \
+    }
+SPMM_ENTRY(csr, CLSPMV_FORMAT_CSR, clspmv_csr_f32)
+SPMM_ENTRY(coo, CLSPMV_FORMAT_COO, clspmv_coo_f32)
+SPMM_ENTRY(dia, CLSPMV_FORMAT_DIA, clspmv_dia_f32)
+SPMM_ENTRY(bdia, CLSPMV_FORMAT_BDIA, clspmv_bdia_f32)
+SPMM_ENTRY(ell, CLSPMV_FORMAT_ELL, clspmv_ell_f32)
+SPMM_ENTRY(sell, CLSPMV_FORMAT_SELL, clspmv_sell_f32)
+SPMM_ENTRY(b4csr, CLSPMV_FORMAT_B4CSR, clspmv_b4csr_f32)
+SPMM_ENTRY(b4ell, CLSPMV_FORMAT_B4ELL, clspmv_b4ell_f32)
+SPMM_ENTRY(sbell, CLSPMV_FORMAT_SBELL, clspmv_sbell_f32)
+#undef SPMM_ENTRY
+
+}  // extern "C"

@@ -210,6 +210,11 @@ _SPMV = {
 CSR_VARIANTS = ("merge", "vector", "scalar")
 
 
+def _torch_dtype(dt):
+    import torch
+    return torch.float32 if dt == np.float32 else torch.int32
+
+
 def _stream_handle(stream) -> Optional[int]:
     import torch
     if stream is None:
@@ -238,6 +243,34 @@ class DeviceMatrix:
         self.nnz = host.nnz
         self.stored_bytes = host.stored_bytes()
         self._plan = None
+
+    @classmethod
+    def from_device_arrays(cls, fmt: str, scalars: dict, tensors: dict) -> "DeviceMatrix":
+        """A device matrix whose arrays were made on the device (e.g. by a
+        device-side generator): `tensors` maps each array field of the
+        format to a CUDA tensor of the right dtype."""
+        self = cls.__new__(cls)
+        struct_t, spec = FORMATS[fmt]
+        self.fmt = fmt
+        self.struct = struct_t()
+        self.struct.matinfo.width = int(scalars["width"])
+        self.struct.matinfo.height = int(scalars["height"])
+        self.struct.matinfo.nnz = int(scalars["nnz"])
+        for name, _ in struct_t._fields_:
+            if name in scalars and name not in ("width", "height", "nnz"):
+                setattr(self.struct, name, int(scalars[name]))
+        self.tensors = {}
+        for field, dt, _ in spec:
+            t = tensors[field]
+            if t.dtype != (_torch_dtype(dt)):
+                raise TypeError(f"{field} must be {dt}")
+            self.tensors[field] = t
+            setattr(self.struct, field, t.data_ptr())
+        self.shape = (self.struct.matinfo.height, self.struct.matinfo.width)
+        self.nnz = self.struct.matinfo.nnz
+        self.stored_bytes = int(sum(t.numel() * t.element_size() for t in self.tensors.values()))
+        self._plan = None
+        return self
 
     def merge_plan(self, stream=None):
         """Tile coordinates for the merge-path CSR kernel (computed once)."""
@@ -270,6 +303,64 @@ class DeviceMatrix:
             return
         name = _SPMV[self.fmt]
         check(getattr(L, name)(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s), name)
+
+    def pack(self, value_type: str = "bf16", stream=None) -> "PackedValues":
+        """16-bit values ("bf16" or "f16") with per-row scales, for spmm."""
+        return device_pack(self, value_type, stream)
+
+    def spmm(self, X, Y, alpha: float = 1.0, beta: float = 0.0, packed: "PackedValues | None" = None,
+             stream=None) -> None:
+        """Y <- alpha * A X + beta * Y for k = X.shape[1] right-hand sides."""
+        device_spmm(self, X, Y, alpha, beta, packed, stream)
+
+
+class PackedValues:
+    """16-bit copy of a device matrix's values with per-row power-of-two
+    scales (clspmv_pack_values); indices stay those of the FP32 matrix."""
+
+    def __init__(self, values, row_scale, value_type: str):
+        self.values = values
+        self.row_scale = row_scale
+        self.value_type = value_type
+
+    @property
+    def nbytes(self) -> int:
+        return self.values.numel() * 2 + self.row_scale.numel() * 4
+
+
+def _spmm_dev(m: "DeviceMatrix"):
+    if m.fmt not in _abi.FORMAT_IDS:
+        raise ValueError(f"no SpMM for format {m.fmt}")
+    return _abi.FORMAT_IDS[m.fmt]
+
+
+def device_pack(m: "DeviceMatrix", value_type: str = "bf16", stream=None) -> PackedValues:
+    import torch
+    fid = _spmm_dev(m)
+    n = C.c_size_t()
+    check(lib().clspmv_stored_values(fid, C.byref(m.struct), C.byref(n)), "stored_values")
+    dev = next(iter(m.tensors.values())).device
+    vals = torch.zeros(max(int(n.value), 1), dtype=torch.int16, device=dev)
+    scale = torch.ones(max(m.shape[0], 1), dtype=torch.float32, device=dev)
+    check(lib().clspmv_pack_values(fid, C.byref(m.struct), _abi.VALUE_TYPES[value_type], vals.data_ptr(),
+                                   scale.data_ptr(), _stream_handle(stream)), "pack_values")
+    return PackedValues(vals, scale, value_type)
+
+
+def device_spmm(m: "DeviceMatrix", X, Y, alpha: float = 1.0, beta: float = 0.0, packed: PackedValues | None = None,
+                stream=None) -> None:
+    """Y <- alpha * A X + beta * Y; X (width, k) and Y (height, k) float32
+    CUDA tensors with unit column stride."""
+    fid = _spmm_dev(m)
+    if X.dim() != 2 or Y.dim() != 2 or X.stride(1) != 1 or Y.stride(1) != 1:
+        raise ValueError("X and Y must be 2-D with unit column stride")
+    k = X.shape[1]
+    if Y.shape[1] != k or X.shape[0] < m.shape[1] or Y.shape[0] < m.shape[0]:
+        raise ValueError("shape mismatch")
+    vt = 0 if packed is None else _abi.VALUE_TYPES[packed.value_type]
+    check(lib().clspmv_spmm(fid, C.byref(m.struct), vt, None if packed is None else packed.values.data_ptr(),
+                            None if packed is None else packed.row_scale.data_ptr(), k, X.data_ptr(), X.stride(0),
+                            Y.data_ptr(), Y.stride(0), alpha, beta, _stream_handle(stream)), "spmm")
 
 
 def launch_count() -> int:

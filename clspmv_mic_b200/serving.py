@@ -1,0 +1,274 @@
+"""A serving loop for SpMV / SpMM requests against resident matrices.
+
+Matrices are registered once and stay in HBM in their tuned format (FP32 or
+packed 16-bit values) while their bytes fit the memory budget; registration
+past the budget is refused (admission by memory). Requests are
+Y = alpha * A * X with any k; a loop thread forms batches continuously:
+
+* requests waiting when a slot frees up are grouped by matrix, and the X
+  columns of one matrix's requests are placed side by side, so A is read
+  once for all of them (up to 128 columns per job);
+* all jobs of the batch run in ONE persistent launch (clspmv_batch_run);
+* `slots` batches can be in flight at once on separate streams, so requests
+  that arrive while a batch runs are admitted into the next slot and their
+  work overlaps the running batch on the device.
+
+Each request's result is the same whether it runs alone or in a mix: every
+row of Y is one group's sum over that row's stored elements, in storage
+order, whatever the other columns and jobs are (tests/test_serving_gpu.py).
+
+The reference has no serving path; its runtime runs one matrix per call and
+waits for it (src/spmv_cocktail.cpp:1088-1132).
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Optional
+
+from .batch import Batch, Job
+from .formats import DeviceMatrix, PackedValues
+
+MAX_COLUMNS = 128
+
+
+@dataclass
+class Resident:
+    name: str
+    matrix: DeviceMatrix
+    packed: Optional[PackedValues]
+    nbytes: int
+    last_used: float = 0.0
+
+
+@dataclass
+class Request:
+    name: str
+    X: object
+    alpha: float
+    future: Future
+    t_submit: float
+    ready: object = None          # CUDA event recorded after X was produced
+    t_done: float = 0.0
+    nbytes: int = 0               # X and Y bytes the request holds on the device
+    keep: bool = True             # False: the future resolves to None
+
+
+@dataclass
+class _Flight:
+    event: object
+    requests: list
+    outputs: list = field(default_factory=list)
+
+
+class SpmvServer:
+    def __init__(self, budget_bytes: int, slots: int = 2, max_jobs: int = 256, max_requests: int = 1024,
+                 max_batch_bytes: int = 8 << 30, device: str = "cuda"):
+        import torch
+        self.torch = torch
+        self.budget = int(budget_bytes)
+        self.used = 0
+        dev = torch.device(device)
+        self.device = torch.device("cuda", torch.cuda.current_device()) if dev.index is None else dev
+        self.max_requests = max_requests
+        self.max_batch_bytes = int(max_batch_bytes)
+        self.mats: dict[str, Resident] = {}
+        self._pending: deque[Request] = deque()
+        self._cv = threading.Condition()
+        self._streams = [torch.cuda.Stream(device=device) for _ in range(slots)]
+        self._batches = [Batch(max_jobs) for _ in range(slots)]
+        self._flights: list[Optional[_Flight]] = [None] * slots
+        self._stop = False
+        self._thread: Optional[threading.Thread] = None
+        self.batches_run = 0
+        self.jobs_run = 0
+
+    # -- residency ---------------------------------------------------------
+    def register(self, name: str, matrix: DeviceMatrix, packed: Optional[PackedValues] = None) -> bool:
+        """Keeps `matrix` resident for requests; False (nothing kept) when its
+        bytes do not fit the remaining budget."""
+        nbytes = int(matrix.stored_bytes) + (packed.nbytes if packed is not None else 0)
+        with self._cv:
+            if name in self.mats:
+                raise KeyError(f"{name} is already registered")
+            if self.used + nbytes > self.budget:
+                return False
+            self.mats[name] = Resident(name, matrix, packed, nbytes)
+            self.used += nbytes
+        return True
+
+    def unregister(self, name: str) -> None:
+        with self._cv:
+            r = self.mats.pop(name)
+            self.used -= r.nbytes
+
+    # -- requests ----------------------------------------------------------
+    def submit(self, name: str, X, alpha: float = 1.0, keep_result: bool = True) -> Future:
+        """Y = alpha * A_name * X (X: CUDA float32, width x k or width, unit
+        column stride); the future resolves to Y (height x k), or to None
+        with keep_result=False (the request is only timed)."""
+        torch = self.torch
+        if name not in self.mats:
+            raise KeyError(name)
+        if X.dim() == 1:
+            X = X.view(-1, 1)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(X.device))
+        f: Future = Future()
+        m, n = self.mats[name].matrix.shape
+        req = Request(name, X, alpha, f, time.perf_counter(), ev, nbytes=4 * X.shape[1] * (m + n), keep=keep_result)
+        f.request = req     # submission / completion times for latency_stats
+        with self._cv:
+            self._pending.append(req)
+            self._cv.notify()
+        return f
+
+    # -- loop --------------------------------------------------------------
+    def start(self) -> "SpmvServer":
+        self._thread = threading.Thread(target=self._loop, name="clspmv-serving", daemon=True)
+        self._thread.start()
+        return self
+
+    def stop(self) -> None:
+        with self._cv:
+            self._stop = True
+            self._cv.notify()
+        if self._thread:
+            self._thread.join()
+        for b in self._batches:
+            b.close()
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def _reap(self) -> bool:
+        done_any = False
+        for i, fl in enumerate(self._flights):
+            if fl is not None and fl.event.query():
+                now = time.perf_counter()
+                for req, out in zip(fl.requests, fl.outputs):
+                    req.t_done = now
+                    req.future.set_result(out if req.keep else None)
+                self._flights[i] = None
+                done_any = True
+        return done_any
+
+    def _take(self) -> list:
+        """Waiting requests, oldest first, up to max_requests and to
+        max_batch_bytes of X and Y (always at least one)."""
+        out, nbytes = [], 0
+        with self._cv:
+            while self._pending and len(out) < self.max_requests:
+                r = self._pending[0]
+                if out and nbytes + r.nbytes > self.max_batch_bytes:
+                    break
+                out.append(self._pending.popleft())
+                nbytes += r.nbytes
+        return out
+
+    def _launch(self, slot: int, reqs: list) -> None:
+        torch = self.torch
+        st = self._streams[slot]
+        groups: dict[str, list] = {}
+        for r in reqs:
+            groups.setdefault(r.name, []).append(r)
+        jobs, order, outputs = [], [], []
+        with torch.cuda.stream(st):
+            for name, rs in groups.items():
+                res = self.mats[name]
+                res.last_used = time.perf_counter()
+                m, n = res.matrix.shape
+                # pack this matrix's requests into jobs of at most MAX_COLUMNS columns
+                i = 0
+                while i < len(rs):
+                    part, cols = [], 0
+                    while i < len(rs) and (not part or cols + rs[i].X.shape[1] <= MAX_COLUMNS):
+                        part.append(rs[i])
+                        cols += rs[i].X.shape[1]
+                        i += 1
+                    for r in part:
+                        st.wait_event(r.ready)
+                    same_alpha = all(r.alpha == part[0].alpha for r in part)
+                    if len(part) > 1:
+                        Xc = torch.cat([r.X for r in part], dim=1)
+                    else:   # a lone request's X is used in place (any row stride)
+                        Xc = part[0].X if part[0].X.stride(1) == 1 else part[0].X.contiguous()
+                    if not same_alpha:
+                        Xc = torch.cat([r.X * r.alpha for r in part], dim=1)
+                    if Xc.shape[1] % 4 and Xc.shape[1] > 32:
+                        Xc = torch.nn.functional.pad(Xc, (0, 4 - Xc.shape[1] % 4))
+                    Yc = torch.empty((m, Xc.shape[1]), dtype=torch.float32, device=Xc.device)
+                    jobs.append(Job(res.matrix, Xc, Yc, alpha=part[0].alpha if same_alpha else 1.0, beta=0.0,
+                                    packed=res.packed))
+                    off = 0
+                    for r in part:
+                        k = r.X.shape[1]
+                        outputs.append(Yc[:, off:off + k])
+                        order.append(r)
+                        off += k
+            b = self._batches[slot]
+            b.set(jobs, st)
+            b.run(st)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        self._flights[slot] = _Flight(ev, order, outputs)
+        self.batches_run += 1
+        self.jobs_run += len(jobs)
+
+    def _loop(self) -> None:
+        try:
+            self._serve()
+        except BaseException as e:   # the loop died: fail every request it still holds
+            with self._cv:
+                pending = list(self._pending)
+                self._pending.clear()
+            for fl in self._flights:
+                if fl is not None:
+                    pending.extend(fl.requests)
+            for r in pending:
+                if not r.future.done():
+                    r.future.set_exception(e)
+            raise
+
+    def _serve(self) -> None:
+        torch = self.torch
+        torch.cuda.set_device(self.device)
+        while True:
+            self._reap()
+            free = [i for i, f in enumerate(self._flights) if f is None]
+            with self._cv:
+                if self._stop and not self._pending and len(free) == len(self._flights):
+                    return
+                has_work = bool(self._pending)
+                if not has_work and len(free) == len(self._flights):
+                    self._cv.wait(timeout=0.01)
+                    continue
+            if has_work and free:
+                reqs = self._take()
+                if reqs:
+                    try:
+                        self._launch(free[0], reqs)
+                    except Exception as e:   # report the failure on every request of the batch
+                        for r in reqs:
+                            if not r.future.done():
+                                r.future.set_exception(e)
+                continue
+            time.sleep(20e-6)
+
+
+def latency_stats(requests: list) -> dict:
+    """p50 / p99 / mean latency in ms and the request rate between the first
+    submission and the last completion (Requests or the futures submit
+    returned)."""
+    import numpy as np
+    requests = [getattr(r, "request", r) for r in requests]
+    lat = np.array([r.t_done - r.t_submit for r in requests]) * 1e3
+    span = max(r.t_done for r in requests) - min(r.t_submit for r in requests)
+    return dict(requests=len(requests), p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                mean_ms=float(lat.mean()), req_per_s=len(requests) / span if span > 0 else float("inf"))

@@ -161,3 +161,44 @@ def random_coo(m: int, n: int, density: float, seed: int = SEED, empty_row_frac:
         vals = rng.standard_normal(rows.size, dtype=np.float32)
         vals[vals == 0] = 1.0
     return _finish(m, n, rows, cols, vals)
+
+
+def device_csr(rows: int, cols: int, lo: int, hi: int, structure: str = "random", seed: int = SEED,
+               device="cuda"):
+    """A CSR matrix generated on the device (for workloads too large to
+    build on the host): row lengths uniform in [lo, hi]; columns
+    "random" (uniform), "banded" (a contiguous run centred on the diagonal)
+    or "blocked" (runs of 4 at 4-aligned block columns, the same block
+    columns for each group of 4 rows); values N(0, 1). Columns within a row
+    are not sorted and may repeat (both allowed by every CSR kernel)."""
+    import torch
+    from .formats import DeviceMatrix
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    lens = torch.randint(lo, hi + 1, (rows,), generator=g, device=device, dtype=torch.int64)
+    if structure == "blocked":
+        lens = (lens + 3) // 4 * 4
+    row_ptr = torch.zeros(rows + 1, dtype=torch.int64, device=device)
+    torch.cumsum(lens, 0, out=row_ptr[1:])
+    nnz = int(row_ptr[-1].item())
+    if nnz >= 2 ** 31:
+        raise ValueError("more than 2^31 - 1 nonzeros")
+    row_of = torch.repeat_interleave(torch.arange(rows, device=device), lens)
+    pos = torch.arange(nnz, device=device) - row_ptr[:-1][row_of]
+    if structure == "random":
+        col = torch.randint(0, cols, (nnz,), generator=g, device=device, dtype=torch.int64)
+    elif structure == "banded":
+        centre = row_of * cols // rows
+        col = (centre - lens[row_of] // 2 + pos).clamp_(0, cols - 1)
+    elif structure == "blocked":
+        nbc = max(1, cols // 4)
+        key = (row_of // 4) * 1000003 + pos // 4 + int(seed) * 7919
+        bc = (key * 2654435761) % nbc
+        col = (bc * 4 + pos % 4).clamp_(0, cols - 1)
+    else:
+        raise ValueError(structure)
+    vals = torch.randn(nnz, generator=g, device=device, dtype=torch.float32)
+    del row_of, pos
+    return DeviceMatrix.from_device_arrays("csr", dict(width=cols, height=rows, nnz=nnz),
+                                           dict(csr_row_ptr=row_ptr.to(torch.int32), csr_col_id=col.to(torch.int32),
+                                                csr_data=vals))

@@ -1,0 +1,271 @@
+"""Measured workloads beyond the single-vector sweep: several right-hand
+sides with FP32 / BF16 / FP16 values, batches of uneven matrices in one
+persistent launch, and the serving loop against sequential launches.
+
+Accuracy is measured against FP64 on the device: the products and the
+per-entry scale sum_j |a_ij x_jc| are formed from the FP64 copy of the
+matrix (torch sparse CSR, used here only as the checker), and the reported
+error is max |Y - Y64| / scale.
+"""
+from __future__ import annotations
+
+import math
+import threading
+import time
+
+import numpy as np
+
+from .batch import Batch, Job
+from .formats import DeviceMatrix
+from . import synth
+
+VALUE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+class Fp64Rows:
+    """The first `rows` rows of a device CSR matrix kept for the FP64
+    accuracy check (row of each entry, column, FP64 value)."""
+
+    def __init__(self, dev_csr: DeviceMatrix, rows: int = 1 << 16):
+        import torch
+        t = dev_csr.tensors
+        self.rows = min(rows, dev_csr.shape[0])
+        rp = t["csr_row_ptr"][: self.rows + 1].long()
+        end = int(rp[-1].item())
+        self.row_of = torch.repeat_interleave(torch.arange(self.rows, device=rp.device), rp[1:] - rp[:-1])
+        self.col = t["csr_col_id"][:end].long()
+        self.val = t["csr_data"][:end].double()
+
+    def error(self, X, Y) -> float:
+        """max over the kept rows of |Y - A X| / (|A| |X|), in FP64."""
+        import torch
+        Xd = X.double()
+        k = Xd.shape[1]
+        ref = torch.zeros((self.rows, k), dtype=torch.float64, device=Xd.device)
+        scale = torch.zeros_like(ref)
+        xr = Xd[self.col]
+        ref.index_add_(0, self.row_of, self.val[:, None] * xr)
+        scale.index_add_(0, self.row_of, (self.val[:, None] * xr).abs())
+        err = (Y[: self.rows].double() - ref).abs() / scale.clamp_min(1e-300)
+        return float(err.max().item()) if err.numel() else 0.0
+
+
+def fp64_of_csr(dev_csr: DeviceMatrix, rows: int = 1 << 16) -> Fp64Rows:
+    return Fp64Rows(dev_csr, rows)
+
+
+def fp64_error(ref: Fp64Rows, X, Y, rows: int | None = None) -> float:
+    return ref.error(X, Y)
+
+
+def matrix_bytes(m: DeviceMatrix, value_type: str) -> int:
+    """Stored bytes of the matrix as the kernel reads it: indices and
+    pointers, values at their stored width, plus the row scales of 16-bit
+    values."""
+    import torch
+    vals = {"csr": "csr_data", "dia": "dia_data", "bdia": "bdia_data", "ell": "ell_data", "sell": "sell_data",
+            "b4csr": "b4csr_data", "b4ell": "b4ell_data", "sbell": "sbell_data", "coo": "coo_data"}[m.fmt]
+    v = m.tensors[vals]
+    rest = m.stored_bytes - v.numel() * 4
+    extra = 4 * m.shape[0] if value_type != "f32" else 0
+    return int(rest + v.numel() * VALUE_BYTES[value_type] + extra)
+
+
+def spmm_sweep(entries, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: int = 10, hbm_gbs=None):
+    """entries: (key, DeviceMatrix, FP64 sparse copy). Y = A X (beta 0) per
+    k and value type; GFLOP/s = 2 nnz k / t, GB/s over matrix bytes + k (4n + 4m)."""
+    import torch
+    out = {}
+    rng = torch.Generator(device="cuda")
+    rng.manual_seed(5)
+    for key, m, A64 in entries:
+        rows, cols = m.shape
+        nnz = int(m.nnz)
+        packs = {vt: (None if vt == "f32" else m.pack(vt)) for vt in value_types}
+        for k in ks:
+            X = torch.rand((cols, k), generator=rng, device="cuda") * 2 - 1
+            Y = torch.empty((rows, k), device="cuda")
+            for vt in value_types:
+                p = packs[vt]
+                for _ in range(3):
+                    m.spmm(X, Y, 1.0, 0.0, packed=p)
+                e0, e1 = _events(torch)
+                e0.record()
+                for _ in range(reps):
+                    m.spmm(X, Y, 1.0, 0.0, packed=p)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                ab = matrix_bytes(m, vt) + k * (4 * cols + 4 * rows)
+                r = dict(ms=round(ms, 4), gflops=round(2.0 * nnz * k / (ms * 1e-3) / 1e9, 1),
+                         gbs=round(ab / (ms * 1e-3) / 1e9, 1), err_fp64=fp64_error(A64, X, Y, rows=min(rows, 1 << 18)))
+                if hbm_gbs:
+                    r["frac"] = round(r["gbs"] / hbm_gbs, 3)
+                out[f"{key}/k{k}/{vt}"] = r
+            del X, Y
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Batches of uneven matrices (one persistent launch, captured in a graph)
+# ---------------------------------------------------------------------------
+def uneven_matrices(count: int = 256, rows_lo: int = 1000, rows_hi: int = 500_000, npr_lo: int = 5, npr_hi: int = 64,
+                    seed: int = 1234):
+    """Device CSR matrices: rows log-uniform in [rows_lo, rows_hi], mean
+    nonzeros per row uniform in [npr_lo, npr_hi], structure banded /
+    blocked / random drawn per matrix."""
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(count):
+        rows = int(math.exp(rng.uniform(math.log(rows_lo), math.log(rows_hi))))
+        npr = int(rng.integers(npr_lo, npr_hi + 1))
+        structure = ["banded", "blocked", "random"][int(rng.integers(3))]
+        lo, hi = max(1, npr - npr // 4), npr + npr // 4
+        mats.append((structure, synth.device_csr(rows, rows, lo, hi, structure, seed=seed + i)))
+    return mats
+
+
+def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: int = 10, check: int = 8):
+    """Per (value type, k): all matrices as ONE batch launch replayed from a
+    CUDA graph, against the same jobs as one plain launch per matrix."""
+    import torch
+    out = {}
+    nnz_total = sum(m.nnz for _, m in mats)
+    packs = {vt: [None if vt == "f32" else m.pack(vt) for _, m in mats] for vt in value_types}
+    A64 = [fp64_of_csr(m) for _, m in mats[:check]]
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    s = torch.cuda.Stream()
+    for k in ks:
+        Xs = [torch.rand((m.shape[1], k), generator=gen, device="cuda") * 2 - 1 for _, m in mats]
+        Ys = [torch.empty((m.shape[0], k), device="cuda") for _, m in mats]
+        for vt in value_types:
+            jobs = [Job(m, X, Y, 1.0, 0.0, packed=p) for (_, m), X, Y, p in zip(mats, Xs, Ys, packs[vt])]
+            b = Batch(len(jobs))
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                b.set(jobs, s)
+                for _ in range(3):
+                    b.run(s)
+            torch.cuda.current_stream().wait_stream(s)
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                b.run()
+            g.replay()
+            e0, e1 = _events(torch)
+            e0.record()
+            for _ in range(reps):
+                g.replay()
+            e1.record()
+            torch.cuda.synchronize()
+            t_batch = e0.elapsed_time(e1) / reps
+            err = max(fp64_error(a, X, Y) for a, X, Y in zip(A64, Xs, Ys))
+            # the same jobs, one plain clspmv_spmm launch each
+            for j in jobs:
+                j.matrix.spmm(j.X, j.Y, 1.0, 0.0, packed=j.packed)
+            e0.record()
+            for _ in range(reps):
+                for j in jobs:
+                    j.matrix.spmm(j.X, j.Y, 1.0, 0.0, packed=j.packed)
+            e1.record()
+            torch.cuda.synchronize()
+            t_seq = e0.elapsed_time(e1) / reps
+            del g
+            b.close()
+            out[f"k{k}/{vt}"] = dict(ms=round(t_batch, 4), gflops=round(2.0 * nnz_total * k / (t_batch * 1e-3) / 1e9, 1),
+                                     plain_ms=round(t_seq, 4), speedup=round(t_seq / t_batch, 2), err_fp64=err,
+                                     launches=1)
+        del Xs, Ys
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Serving: Poisson arrivals against resident matrices
+# ---------------------------------------------------------------------------
+def serving_matrices(count: int = 64, rows_lo: int = 10_000, rows_hi: int = 4_000_000, nnz_lo: float = 20e6,
+                     nnz_hi: float = 200e6, seed: int = 99):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        rows = int(math.exp(rng.uniform(math.log(rows_lo), math.log(rows_hi))))
+        nnz = math.exp(rng.uniform(math.log(nnz_lo), math.log(nnz_hi)))
+        npr = max(1, int(round(nnz / rows)))
+        npr = min(npr, rows)
+        structure = ["banded", "blocked", "random"][int(rng.integers(3))]
+        out.append(synth.device_csr(rows, rows, max(1, npr - npr // 8), npr + npr // 8, structure, seed=seed + i))
+    return out
+
+
+def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.0, k_lo: int = 1, k_hi: int = 32,
+          value_type: str = "f32", seed: int = 3, slots: int = 2):
+    """Open-loop Poisson stream of `n_requests` at `rate` req/s, k uniform in
+    [k_lo, k_hi], matrix uniform among the admitted ones. Returns the serving
+    loop's and the sequential baseline's req/s and p50 / p99 latency."""
+    import torch
+    from .serving import SpmvServer, latency_stats
+    rng = np.random.default_rng(seed)
+    srv = SpmvServer(budget_bytes, slots=slots)
+    names = []
+    for i, m in enumerate(mats):
+        p = None if value_type == "f32" else m.pack(value_type)
+        if srv.register(f"m{i}", m, p):
+            names.append(f"m{i}")
+    admitted_bytes = srv.used
+    pick = rng.integers(len(names), size=n_requests)
+    ks = rng.integers(k_lo, k_hi + 1, size=n_requests)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    # one (width x k_hi) block of right-hand sides per matrix; a request uses its first k columns
+    pools = {nm: torch.rand((srv.mats[nm].matrix.shape[1], k_hi), generator=gen, device="cuda") for nm in names}
+    Xs = [pools[names[p]][:, :int(k)] for p, k in zip(pick, ks)]
+    torch.cuda.synchronize()
+
+    # sequential plain launches: one clspmv_spmm + synchronize per request, same arrival times
+    lat_seq = []
+    t0 = time.perf_counter()
+    for i in range(n_requests):
+        while time.perf_counter() - t0 < arrivals[i]:
+            pass
+        res = srv.mats[names[pick[i]]]
+        Y = torch.empty((res.matrix.shape[0], int(ks[i])), device="cuda")
+        res.matrix.spmm(Xs[i], Y, 1.0, 0.0, packed=res.packed)
+        torch.cuda.synchronize()
+        lat_seq.append(time.perf_counter() - t0 - arrivals[i])
+        del Y
+    span_seq = time.perf_counter() - t0
+    lat_seq = np.array(lat_seq) * 1e3
+
+    # the serving loop, fed by a client thread on the same schedule
+    futures = [None] * n_requests
+    srv.start()
+    # warm the loop's batches once
+    srv.submit(names[pick[0]], Xs[0], keep_result=False).result(timeout=600)
+
+    def client():
+        t_start = time.perf_counter()
+        for i in range(n_requests):
+            while time.perf_counter() - t_start < arrivals[i]:
+                pass
+            futures[i] = srv.submit(names[pick[i]], Xs[i], keep_result=False)
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    for f in futures:
+        f.result(timeout=600)
+    stats = latency_stats(futures)
+    batches = srv.batches_run
+    srv.stop()
+    return dict(requests=n_requests, offered_req_per_s=rate, k=[k_lo, k_hi], value_type=value_type,
+                matrices=len(names), resident_gb=round(admitted_bytes / 1e9, 2),
+                served=dict(req_per_s=round(stats["req_per_s"], 1), p50_ms=round(stats["p50_ms"], 3),
+                            p99_ms=round(stats["p99_ms"], 3), batches=batches - 1),
+                sequential=dict(req_per_s=round(n_requests / span_seq, 1), p50_ms=round(float(np.percentile(lat_seq, 50)), 3),
+                                p99_ms=round(float(np.percentile(lat_seq, 99)), 3)),
+                speedup=round(stats["req_per_s"] / (n_requests / span_seq), 2))

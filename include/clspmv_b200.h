@@ -371,6 +371,91 @@ int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* dev, const float* x, float* y,
                           float alpha, float beta, clspmv_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Several right-hand sides and 16-bit value storage (no counterpart in the  */
+/* reference, whose kernels multiply one vector per call).                   */
+/* ------------------------------------------------------------------------ */
+
+typedef enum {
+    CLSPMV_FORMAT_CSR = 0, CLSPMV_FORMAT_COO = 1, CLSPMV_FORMAT_DIA = 2, CLSPMV_FORMAT_BDIA = 3,
+    CLSPMV_FORMAT_ELL = 4, CLSPMV_FORMAT_SELL = 5, CLSPMV_FORMAT_B4CSR = 6, CLSPMV_FORMAT_B4ELL = 7,
+    CLSPMV_FORMAT_SBELL = 8
+} clspmv_format;
+
+typedef enum { CLSPMV_VALUES_F32 = 0, CLSPMV_VALUES_BF16 = 1, CLSPMV_VALUES_F16 = 2 } clspmv_values;
+
+/* Y <- alpha * A * X + beta * Y for the device matrix `dev` (a pointer to the
+ * format's struct, e.g. clspmv_csr_f32*, with device arrays). X is width x k,
+ * Y is height x k, both row major with leading dimensions ldx, ldy >= k,
+ * 1 <= k <= 128 (k > 32 needs k, ldx, ldy multiples of 4 and 16-byte aligned
+ * X, Y: CLSPMV_ERR_ALIGN otherwise). FP32 accumulation.
+ * value_type CLSPMV_VALUES_F32 uses the struct's own values (`values`,
+ * `row_scale` ignored); BF16 / F16 use the 16-bit array and per-row scales
+ * made by clspmv_pack_values. CSR and COO must be row sorted; their rows
+ * cut between work chunks are added atomically, so the last bits of Y may
+ * differ between runs (within the FP32 bound). */
+int clspmv_spmm(int format, const void* dev, int value_type, const void* values, const float* row_scale, int k,
+                const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+
+/* Per-format FP32 forms of clspmv_spmm. */
+int clspmv_csr_spmm_f32(const clspmv_csr_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_coo_spmm_f32(const clspmv_coo_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_dia_spmm_f32(const clspmv_dia_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_bdia_spmm_f32(const clspmv_bdia_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_ell_spmm_f32(const clspmv_ell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_sell_spmm_f32(const clspmv_sell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_b4csr_spmm_f32(const clspmv_b4csr_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_b4ell_spmm_f32(const clspmv_b4ell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+int clspmv_sbell_spmm_f32(const clspmv_sbell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
+
+/* Number of stored values (padding included) of the device matrix, i.e. the
+ * length of its value array; reads one int from the device for BDIA, SELL
+ * and SBELL. */
+int clspmv_stored_values(int format, const void* dev, size_t* count);
+
+/* Makes the 16-bit copy of a device matrix's values: row_scale[r] =
+ * 2^ceil(log2(max_j |a_rj|)) (1 for empty rows) and values[i] = a_i /
+ * row_scale[row of i], rounded to nearest (value_type BF16 or F16).
+ * `values` holds clspmv_stored_values entries of 2 bytes, `row_scale` height
+ * floats; stored positions outside the matrix get 0. Asynchronous. */
+int clspmv_pack_values(int format, const void* dev, int value_type, void* values, float* row_scale,
+                       clspmv_stream_t stream);
+
+/* One Y <- alpha * A * X + beta * Y of a batch (fields as in clspmv_spmm). */
+typedef struct {
+    int format;              /* clspmv_format; every format but COO */
+    const void* dev;         /* device matrix struct (read when the batch is set) */
+    int value_type;          /* clspmv_values */
+    const void* values;      /* 16-bit values (BF16 / F16 only) */
+    const float* row_scale;  /* their row scales (BF16 / F16 only) */
+    int k;
+    const float* X;
+    int ldx;
+    float* Y;
+    int ldy;
+    float alpha, beta;
+} clspmv_spmm_job;
+
+/* A batch runs many jobs (different matrices, formats, value types and k)
+ * in ONE persistent kernel launch: the rows of all jobs are cut into warp
+ * tasks that every warp of a device-filling grid strides through. */
+typedef struct clspmv_batch clspmv_batch;
+
+/* Allocates the device job table for up to max_jobs jobs (and a pinned
+ * staging copy). */
+int clspmv_batch_create(int max_jobs, clspmv_batch** out);
+/* Validates the jobs and uploads the table on `stream` (asynchronous; the
+ * structs pointed to by jobs[i].dev are copied, so they may be released
+ * after the call). On an invalid job returns its status and, if bad_job is
+ * not NULL, its index; the batch is then empty. Waits only for this batch's
+ * previous upload to leave the staging buffer. */
+int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, clspmv_stream_t stream, int* bad_job);
+/* Runs the jobs last set: one kernel launch on `stream`, no allocation and no
+ * host synchronisation, so it can be captured in a CUDA graph. Jobs must
+ * not write overlapping Y. */
+int clspmv_batch_run(clspmv_batch* b, clspmv_stream_t stream);
+int clspmv_batch_free(clspmv_batch* b);
+
+/* ------------------------------------------------------------------------ */
 /* Cocktail partitioning (src/analyze.cpp of clSpMV).                        */
 /* ------------------------------------------------------------------------ */
 

@@ -1,0 +1,144 @@
+"""Several right-hand sides (Y = alpha*A*X + beta*Y) and 16-bit value storage.
+
+Oracle: the FP64 restatement of the reference's csr_spmv (oracle/) applied
+column by column. FP32 values must be within 1e-5 * (|alpha| sum_j |a_ij x_jc|
++ |beta y_ic|) per entry, the bound of the single-vector kernels. BF16 / FP16
+values are checked against their own rounding bound (2^-8 and 2^-10 of the
+same row scale, one rounding per stored value) and their error against FP64
+is what the bench reports.
+"""
+import numpy as np
+import pytest
+
+from clspmv_mic_b200 import formats as F
+from clspmv_mic_b200 import synth
+from oracle import oracle as O
+
+from matrices import coo_of
+
+pytestmark = pytest.mark.gpu
+
+RTOL = {"f32": 1e-5, "bf16": 2.0 ** -8, "f16": 2.0 ** -10}
+
+
+def spmm_reference(coo, X, Y0, alpha, beta):
+    csr = F.coo2csr(coo)
+    m, k = coo.shape[0], X.shape[1]
+    ref = np.zeros((m, k))
+    bound = np.zeros((m, k))
+    for c in range(k):
+        y64, sc = O.csr_f64(csr, np.ascontiguousarray(X[:, c]))
+        ref[:, c] = alpha * y64 + beta * Y0[:, c].astype(np.float64)
+        bound[:, c] = abs(alpha) * sc + abs(beta) * np.abs(Y0[:, c].astype(np.float64))
+    return ref, bound
+
+
+def device_of(coo, fmt, *args):
+    host = coo if fmt == "coo" else getattr(F, f"coo2{fmt}")(coo, *args)
+    return F.DeviceMatrix(host)
+
+
+CASES = [
+    ("laplace33", "csr", ()), ("laplace33", "coo", ()), ("laplace33", "dia", ()), ("laplace33", "bdia", ()),
+    ("laplace33", "ell", ()), ("laplace33", "sell", (32,)), ("stencil6", "dia", ()), ("stencil6", "bdia", ()),
+    ("powerlaw3k", "csr", ()), ("powerlaw3k", "coo", ()), ("powerlaw3k", "sell", (128,)), ("powerlaw3k", "ell", ()),
+    ("random_empty_rows", "csr", ()), ("random_empty_rows", "coo", ()), ("blocks_odd", "b4csr", (4, 4)),
+    ("blocks_odd", "b4ell", (8, 2)), ("blocks_odd", "sbell", (4, 4)), ("blocks300", "b4csr", (8, 8)),
+    ("blocks300", "sbell", (4, 1)), ("blocks300", "b4ell", (4, 4)), ("wide", "csr", ()), ("tall", "sell", (32,)),
+]
+
+
+def _run(name, fmt, args, k, alpha, beta, value_type="f32", ld_pad=0):
+    import torch
+    coo = coo_of(name)
+    m, n = coo.shape
+    rng = np.random.default_rng(k * 31 + len(name))
+    X = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    Y0 = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+    dev = device_of(coo, fmt, *args)
+    Xd = torch.zeros((n, k + ld_pad), dtype=torch.float32, device="cuda")
+    Xd[:, :k] = torch.from_numpy(X)
+    Yd = torch.zeros((m, k + ld_pad), dtype=torch.float32, device="cuda")
+    Yd[:, :k] = torch.from_numpy(Y0)
+    packed = None if value_type == "f32" else dev.pack(value_type)
+    dev.spmm(Xd[:, :k], Yd[:, :k], alpha, beta, packed=packed)
+    torch.cuda.synchronize()
+    got = Yd[:, :k].cpu().numpy().astype(np.float64)
+    ref, bound = spmm_reference(coo, X, Y0, alpha, beta)
+    err = np.abs(got - ref)
+    lim = RTOL[value_type] * bound + 1e-30
+    bad = np.argwhere(err > lim)
+    assert bad.size == 0, f"{name}/{fmt}{args} k={k} {value_type}: {len(bad)} entries off, first {bad[:3].tolist()}"
+    return float(np.max(err / np.where(bound > 0, bound, 1.0))) if err.size else 0.0
+
+
+@pytest.mark.parametrize("name,fmt,args", CASES)
+@pytest.mark.parametrize("k", [1, 4, 16, 32])
+def test_spmm_f32(name, fmt, args, k):
+    _run(name, fmt, args, k, 1.0, 0.0)
+
+
+@pytest.mark.parametrize("name,fmt,args", [c for c in CASES if c[0] in ("laplace33", "blocks_odd", "powerlaw3k")])
+@pytest.mark.parametrize("k,ld_pad,alpha,beta", [(3, 1, 0.5, 2.0), (5, 0, -1.0, 1.0), (64, 0, 1.0, -0.5),
+                                                 (128, 4, 2.0, 0.0), (7, 2, 1.0, 1.0)])
+def test_spmm_shapes_and_scalars(name, fmt, args, k, ld_pad, alpha, beta):
+    _run(name, fmt, args, k, alpha, beta, ld_pad=ld_pad)
+
+
+@pytest.mark.parametrize("value_type", ["bf16", "f16"])
+@pytest.mark.parametrize("name,fmt,args", CASES[::2])
+@pytest.mark.parametrize("k", [1, 16])
+def test_spmm_reduced_precision(name, fmt, args, k, value_type):
+    _run(name, fmt, args, k, 1.0, 0.0, value_type=value_type)
+
+
+@pytest.mark.parametrize("value_type", ["bf16", "f16"])
+def test_pack_values_scaled_rounding(value_type):
+    import torch
+    coo = coo_of("powerlaw3k")
+    a = coo.arrays()
+    rows, vals = a["coo_row_id"], a["coo_data"].astype(np.float64) * np.exp(np.linspace(-20, 20, coo.nnz))
+    big = F.coo_matrix(coo.shape[0], coo.shape[1], rows, a["coo_col_id"], vals.astype(np.float32))
+    csr = F.coo2csr(big)          # kept alive: its arrays are viewed below
+    dev = F.DeviceMatrix(csr)
+    p = dev.pack(value_type)
+    torch.cuda.synchronize()
+    dt = torch.bfloat16 if value_type == "bf16" else torch.float16
+    packed = p.values.view(dt).float().cpu().numpy().astype(np.float64)[:big.nnz]
+    scale = p.row_scale.cpu().numpy().astype(np.float64)
+    ref = csr.array("csr_data").astype(np.float64)
+    row_of = np.repeat(np.arange(big.shape[0]), np.diff(csr.array("csr_row_ptr")))
+    mx = np.zeros(big.shape[0])
+    np.maximum.at(mx, row_of, np.abs(ref))
+    assert np.all(np.log2(scale) == np.round(np.log2(scale)))            # powers of two
+    assert np.all((scale >= mx) & ((mx == 0) | (scale < 2 * mx)))
+    rel = np.abs(packed * scale[row_of] - ref) / np.maximum(scale[row_of], 1e-300)
+    assert rel.max() <= RTOL[value_type] / 2 + 1e-12
+
+
+def test_spmm_k1_matches_spmv():
+    import torch
+    coo = coo_of("powerlaw3k")
+    m, n = coo.shape
+    dev = F.DeviceMatrix(F.coo2csr(coo))
+    x = torch.from_numpy(synth.x_vector(n)).cuda()
+    y1 = torch.zeros(m, device="cuda")
+    dev.spmv(x, y1, 1.0, 0.0)
+    y2 = torch.zeros((m, 1), device="cuda")
+    dev.spmm(x.view(n, 1), y2, 1.0, 0.0)
+    torch.cuda.synchronize()
+    _, _, bound = __import__("gpu_util").reference_y(coo, x.cpu().numpy(), None, 1.0, 0.0)
+    assert np.all(np.abs(y1.cpu().numpy() - y2[:, 0].cpu().numpy()) <= 2e-5 * bound + 1e-30)
+
+
+def test_spmm_rejects():
+    import torch
+    from clspmv_mic_b200 import _abi
+    dev = F.DeviceMatrix(F.coo2csr(coo_of("laplace16")))
+    n = dev.shape[1]
+    with pytest.raises(_abi.ClspmvError):
+        dev.spmm(torch.zeros((n, 129), device="cuda"), torch.zeros((dev.shape[0], 129), device="cuda"))
+    X = torch.zeros((n, 40), device="cuda")[:, 1:]      # k = 39 > 32 without 16-byte rows
+    with pytest.raises(_abi.ClspmvError) as e:
+        dev.spmm(X, torch.zeros((dev.shape[0], 39), device="cuda"))
+    assert e.value.status == _abi.ERR_ALIGN
