@@ -263,6 +263,8 @@ def cpu_csr_seconds(mats, budget_s: float = 15.0):
 # Arms
 # ---------------------------------------------------------------------------
 def dist_init(args):
+    """One process per GPU under torchrun (NCCL); gloo when CUDA is absent
+    (the multi-process logic is tested that way on the CPU)."""
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -270,9 +272,31 @@ def dist_init(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return world, rank, local
+
+
+def max_over_ranks(value: float, device) -> float:
+    """The slowest rank's time (replicas are timed on their own devices; the
+    job's time is the maximum)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(flops_per_replica_step: float, world: int, ms_per_step: float) -> float:
+    """Whole-job GFLOP/s: every replica does the same step, the job takes the
+    slowest replica's time."""
+    return flops_per_replica_step * world / (ms_per_step * 1e-3) / 1e9
 
 
 def run_reference(args):
@@ -385,9 +409,7 @@ def run_ours(args):
     per_kernel_ms = np.array([[ev[i][j].elapsed_time(ev[i][j + 1]) for j in range(K)] for i in range(args.steps)])
     clk = clocks.stop()
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dev)
         torch.distributed.barrier()
 
     # e2e through the public API with host buffers: per kernel, pinned x
@@ -419,16 +441,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, dev)
 
     # the ELL part and its COO tail together carry the matrix's flops once
     flops_step = sum(format_flops(it) for it in items if it["part_of"] is None) + \
         sum(format_flops(it) for it in items if it["part_of"] == "ell")
     ms_per_step = total_ms / args.steps
-    value = flops_step * world / (ms_per_step * 1e-3) / 1e9
-    e2e_value = flops_step * world / (e2e_ms * 1e-3) / 1e9
+    value = job_value(flops_step, world, ms_per_step)
+    e2e_value = job_value(flops_step, world, e2e_ms)
 
     peak, peak_kind = hbm_peak()
     med = np.median(per_kernel_ms, axis=0)
@@ -488,7 +508,7 @@ def run_ours(args):
         "formats": formats,
         "variants": variant_stats,
     }
-    if not args.no_extras and not args.only:
+    if not args.no_extras and not args.only and world == 1:
         line["extras"] = run_extras(args, items, mats, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)
