@@ -451,6 +451,12 @@ def run_ours(args):
     e2e_value = job_value(flops_step, world, e2e_ms)
 
     peak, peak_kind = hbm_peak()
+    # the scattered-column formats are bound by random x gathers, not bytes:
+    # measure that ceiling on the power-law matrix's x length
+    gather_peak = None
+    if "powerlaw" in mats:
+        from clspmv_mic_b200.drivers import gather_test
+        gather_peak = gather_test(int(mats["powerlaw"][1]), 1 << 24, 20)
     med = np.median(per_kernel_ms, axis=0)
     mean = per_kernel_ms.mean(axis=0)
     formats = {}
@@ -462,6 +468,9 @@ def run_ours(args):
             "gbs": round(ab / (med[j] * 1e-3) / 1e9, 1), "frac": round(ab / (med[j] * 1e-3) / 1e9 / peak, 3),
             "alg_bytes": ab, "useful_bytes": useful, "nnz": it["nnz"], "rows": it["rows"],
         }
+        if gather_peak and it["matrix"] == "powerlaw":
+            g = it["nnz"] / (med[j] * 1e-3)
+            formats[it["key"]].update(gathers_per_s=round(g / 1e9, 1), gather_frac=round(g / gather_peak, 3))
     # the CSR-vector / CSR-scalar variants, outside the timed step
     variant_stats = {}
     for it in variants:
@@ -478,7 +487,12 @@ def run_ours(args):
         torch.cuda.synchronize()
         ms = v0.elapsed_time(v1) / reps
         ab = algorithmic_bytes(it)
-        variant_stats[it["key"]] = {"matrix": it["matrix"], "ms": round(ms, 5),
+        if gather_peak and it["matrix"] == "powerlaw":
+            g = it["nnz"] / (ms * 1e-3)
+            gextra = {"gathers_per_s": round(g / 1e9, 1), "gather_frac": round(g / gather_peak, 3)}
+        else:
+            gextra = {}
+        variant_stats[it["key"]] = {**gextra, "matrix": it["matrix"], "ms": round(ms, 5),
                                     "gflops": round(format_flops(it) / (ms * 1e-3) / 1e9, 2),
                                     "gbs": round(ab / (ms * 1e-3) / 1e9, 1), "frac": round(ab / (ms * 1e-3) / 1e9 / peak, 3)}
     dom = int(np.argmax(mean))
@@ -503,6 +517,7 @@ def run_ours(args):
                      "traffic": traffic, "alg_bytes_per_launch": ab},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": round(e2e_ms, 4)},
+        "gather_peak_per_s": None if gather_peak is None else round(gather_peak / 1e9, 1),
         "gpu_launches": int(launches),
         "clocks": clk,
         "formats": formats,

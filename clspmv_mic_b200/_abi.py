@@ -232,6 +232,7 @@ def _declare(lib):
         "clspmv_cocktail_free": (I32, [VP]),
         "clspmv_run_method_f32": (I32, [S["coo"], I32, I32, I32, P(BenchResult)]),
         "clspmv_bandwidth_test": (I32, [C.c_size_t, I32, I32, P(C.c_double), P(C.c_double)]),
+        "clspmv_gather_test": (I32, [I32, C.c_longlong, I32, I32, P(C.c_double)]),
         "clspmv_cocktail_evaluate_f32": (I32, [P(Cocktail), VP, VP, VP, I32, I32, P(C.c_double), P(C.c_double),
                                                P(C.c_double)]),
         "clspmv_read_mmf_f32": (I32, [C.c_char_p, S["coo"]]),

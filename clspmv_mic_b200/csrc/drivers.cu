@@ -15,6 +15,7 @@
 #include "api_internal.h"
 #include "matrix_storage.h"
 #include "spmv_serial.h"
+#include "common.cuh"
 
 using namespace clspmv;
 
@@ -27,6 +28,33 @@ __global__ void k_copy4(const float4* __restrict__ a, float4* __restrict__ b, si
 }
 
 __global__ void k_nothing() {}
+
+// Random gathers x[idx[i]] with the SpMV kernels' load forms: indices
+// streamed with 128-bit loads, x read through L1 with an L2 keep policy.
+__global__ void __launch_bounds__(kBlock) k_gather(const int* __restrict__ idx, const float* __restrict__ x,
+                                                   float* __restrict__ out, long long n4)
+{
+    const uint64_t pol_s = policy_evict_first(), pol_x = policy_evict_last();
+    float acc = 0.0f;
+    for (long long i = blockIdx.x * (long long)kBlock + threadIdx.x; i < n4; i += (long long)gridDim.x * kBlock) {
+        const int4 c = ld_stream_i4(idx + 4 * i, pol_s);
+        acc += ld_x(x + c.x, pol_x) + ld_x(x + c.y, pol_x) + ld_x(x + c.z, pol_x) + ld_x(x + c.w, pol_x);
+    }
+    out[blockIdx.x * (long long)kBlock + threadIdx.x] = acc;
+}
+
+__global__ void k_fill_random(int* idx, long long n, int range, unsigned seed)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ull + seed;   // splitmix64 step
+        h ^= h >> 30;
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 27;
+        h *= 0x94D049BB133111EBull;
+        h ^= h >> 31;
+        idx[i] = (int)(h % (unsigned long long)range);
+    }
+}
 
 coo_matrix<int, float>* as_tmpl(const clspmv_coo_f32* c)
 {
@@ -402,6 +430,56 @@ int clspmv_bandwidth_test(size_t bytes, int ntimes, int verbose, double* copy_gb
     }
     if (a) cudaFree(a);
     if (b) cudaFree(b);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    return rc;
+}
+
+int clspmv_gather_test(int x_len, long long count, int ntimes, int verbose, double* gathers_per_s)
+{
+    if (x_len < 1 || count < 4 || ntimes < 1) return CLSPMV_ERR_ARG;
+    const long long n4 = count / 4;
+    int* idx = nullptr;
+    float *x = nullptr, *out = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = sms * 8;
+    int rc = cuda_status(cudaMalloc(&idx, sizeof(int) * 4 * n4));
+    if (!rc) rc = cuda_status(cudaMalloc(&x, sizeof(float) * x_len));
+    if (!rc) rc = cuda_status(cudaMalloc(&out, sizeof(float) * grid * kBlock));
+    if (!rc) rc = cuda_status(cudaMemset(x, 0, sizeof(float) * x_len));
+    if (!rc) rc = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (!rc) rc = cuda_status(cudaEventCreate(&e0));
+    if (!rc) rc = cuda_status(cudaEventCreate(&e1));
+    if (!rc) {
+        k_fill_random<<<grid, kBlock, 0, st>>>(idx, 4 * n4, x_len, 12345u);
+        rc = after_launch(1);
+    }
+    for (int i = 0; !rc && i < 3; i++) {
+        k_gather<<<grid, kBlock, 0, st>>>(idx, x, out, n4);
+        rc = after_launch(1);
+    }
+    if (!rc) rc = cuda_status(cudaEventRecord(e0, st));
+    for (int i = 0; !rc && i < ntimes; i++) {
+        k_gather<<<grid, kBlock, 0, st>>>(idx, x, out, n4);
+        rc = after_launch(1);
+    }
+    if (!rc) rc = cuda_status(cudaEventRecord(e1, st));
+    if (!rc) rc = cuda_status(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    if (!rc) rc = cuda_status(cudaEventElapsedTime(&ms, e0, e1));
+    if (!rc) {
+        const double g = (double)(4 * n4) / ((double)ms / ntimes * 1e-3);
+        if (gathers_per_s) *gathers_per_s = g;
+        if (verbose) printf("\nRandom gathers from %d floats: %.1f G/s (%lld per launch)\n", x_len, g / 1e9, 4 * n4);
+    }
+    if (idx) cudaFree(idx);
+    if (x) cudaFree(x);
+    if (out) cudaFree(out);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);

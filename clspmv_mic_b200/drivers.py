@@ -57,6 +57,14 @@ def bandwidth_test(nbytes: int = 256 << 20, ntimes: int = 20, verbose: bool = Fa
     return dict(copy_gbs=gbs.value, launch_us=us.value, bytes=int(nbytes))
 
 
+def gather_test(x_len: int = 1 << 20, count: int = 1 << 24, ntimes: int = 20, verbose: bool = False) -> float:
+    """Random gathers per second from an x of x_len floats (the bound of the
+    scattered-column formats)."""
+    g = C.c_double()
+    check(lib().clspmv_gather_test(int(x_len), int(count), int(ntimes), int(verbose), C.byref(g)), "gather_test")
+    return g.value
+
+
 def read_mmf(path: str | os.PathLike) -> HostMatrix:
     """ReadMMF: a coordinate Matrix Market file as a row-sorted COO matrix."""
     out = _abi.Coo()

@@ -554,6 +554,14 @@ int clspmv_run_method_f32(const clspmv_coo_f32* coo, int method, int ntimes, int
  * of `ntimes` runs. */
 int clspmv_bandwidth_test(size_t bytes, int ntimes, int verbose, double* copy_gbs, double* launch_us);
 
+/* Random-gather throughput: `count` loads x[idx[i]] with uniformly random
+ * idx over an x of x_len floats, in the load forms the SpMV kernels use
+ * (indices streamed, x through L1 with an L2 keep policy); mean of ntimes
+ * launches. This is the ceiling of the irregular formats (CSR, COO, ELL on
+ * scattered columns), whose time is set by x gathers rather than bytes. No
+ * counterpart in the reference. */
+int clspmv_gather_test(int x_len, long long count, int ntimes, int verbose, double* gathers_per_s);
+
 /* evaluate (src/spmv_cocktail.cpp:1431-1455): upload the partitioned
  * matrix, check one SpMV y = A*vec + res against `coores` (NULL: skip), then
  * time `ntimes` SpMVs (the reference uses 1000). Prints the reference's
