@@ -551,6 +551,38 @@ def run_extras(args, items, mats, peak):
         csr_dev = by_key["csr_merge"]["dev"] if name == "powerlaw" else F.DeviceMatrix(F.coo2csr(F.coo_matrix(*arrs)))
         csr64[name] = W.fp64_of_csr(csr_dev)
         del csr_dev
+    # single-vector SpMV with 16-bit values in each format's own kernel
+    spmv16 = {}
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(11)
+    for key in ("dia", "bdia", "csr_merge", "coo", "sell32", "bell", "sbell", "bcsr"):
+        if key not in by_key:
+            continue
+        it = by_key[key]
+        m = it["dev"]
+        x = torch.rand(it["cols"], generator=gen, device="cuda") * 2 - 1
+        y = torch.zeros(it["rows"], device="cuda")
+        for vt in ("bf16", "f16"):
+            p = m.pack(vt)
+            m.spmv(x, y, 1.0, 0.0, packed=p)
+            err = csr64[it["matrix"]].error(x[:, None], y[:, None])
+            for _ in range(3):
+                m.spmv(x, y, 1.0, 0.0, packed=p)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                m.spmv(x, y, 1.0, 0.0, packed=p)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 20
+            ab = W.matrix_bytes(m, vt) + 4 * it["cols"] + 8 * it["rows"]
+            spmv16[f"{key}/{vt}"] = {"ms": round(ms, 5), "gflops": round(2 * it["nnz"] / (ms * 1e-3) / 1e9, 1),
+                                     "gbs": round(ab / (ms * 1e-3) / 1e9, 1), "frac": round(ab / (ms * 1e-3) / 1e9 / peak, 3),
+                                     "alg_bytes": ab, "err_fp64": err}
+            del p
+    out["spmv16"] = {"note": "y = A x with values stored as BF16 / FP16 (per-row power-of-two scale, FP32 "
+                             "accumulation) in each format's own kernel; GB/s over the bytes at 2-byte values",
+                     "results": spmv16}
     entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_merge", "bcsr", "sbell")
                if k in by_key]
     out["spmm"] = {"note": "Y = A X, beta 0; GB/s over matrix bytes at the stored value width + k (4n + 4m); "

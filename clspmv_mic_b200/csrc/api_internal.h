@@ -24,5 +24,7 @@ int launch_csr_merge_plan(const clspmv_csr_f32* m, int* tc, cudaStream_t st);
 int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_packed(int format, const void* dev, int value_type, const void* values, const float* scale, const int* tc,
+                  const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 }  // namespace clspmv

@@ -56,11 +56,12 @@ __device__ __forceinline__ void cta_share(long long units, int quantum, int cta,
 }
 
 template <bool ATOMIC>
-__device__ __forceinline__ void y_put4(const float* acc, long long row0, long long e, float* y, float alpha, float beta)
+__device__ __forceinline__ void y_put4(const float* acc, long long row0, long long e, float* y, float alpha, float beta,
+                                       const float* scale = nullptr)
 {
 #pragma unroll
     for (int i = 0; i < 4; i++)
-        if (row0 + i < e) y_update<ATOMIC>(y, row0 + i, alpha, beta, acc[i]);
+        if (row0 + i < e) y_update<ATOMIC>(y, row0 + i, row_alpha(alpha, scale, row0 + i), beta, acc[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -71,8 +72,8 @@ __device__ __forceinline__ void y_put4(const float* acc, long long row0, long lo
 constexpr int kDiaRowsPerPass = kBlock * 4;
 constexpr int kDiaSmemBytes = kBlock * sizeof(int);
 
-template <bool ATOMIC>
-__device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, char* smem)
+template <bool ATOMIC, class V>
+__device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta, char* smem)
 {
     int* s_off = reinterpret_cast<int*>(smem);
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
@@ -95,11 +96,11 @@ __device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, cha
                 __syncthreads();
             }
             if (active) {
-                const float* dp = a.data + (size_t)d0 * a.len + row0;
+                const V* dp = a.data + (size_t)d0 * a.len + row0;
 #pragma unroll 4
                 for (int k = 0; k < nd; k++) {
                     const int c = (int)row0 + s_off[k];
-                    const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
+                    const float4 v = ldv4(dp + (size_t)k * a.len, pe);
                     float x0, x1, x2, x3;
                     if (c >= 0 && c + 3 < a.cols) {
                         x0 = ld_x(a.x + c, pl);
@@ -119,7 +120,7 @@ __device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, cha
                 }
             }
         }
-        if (active) y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
+        if (active) y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta, scl(a));
     }
 }
 
@@ -136,8 +137,8 @@ __device__ __forceinline__ void dia_cta(const DiaArgs& a, int cta, int ncta, cha
 constexpr int kBdiaRowsPerPass = kBlock * 4;
 constexpr int kBdiaRun = 4;
 
-template <bool ATOMIC>
-__device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, char*)
+template <bool ATOMIC, class V>
+__device__ __forceinline__ void bdia_cta(const BdiaArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
@@ -154,7 +155,7 @@ __device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, c
                 float4 v[kBdiaRun];
 #pragma unroll
                 for (int t = 0; t < kBdiaRun; t++)
-                    if (t < n) v[t] = ld_stream_f4(a.data + (size_t)(j0 + t) * a.len + row0, pe);
+                    if (t < n) v[t] = ldv4(a.data + (size_t)(j0 + t) * a.len + row0, pe);
 #pragma unroll
                 for (int t = 0; t < kBdiaRun + 3; t++) {
                     const long long c = c0 + t;
@@ -171,7 +172,7 @@ __device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, c
                 }
             }
         }
-        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
+        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta, scl(a));
     }
 }
 
@@ -181,26 +182,26 @@ __device__ __forceinline__ void bdia_cta(const BdiaArgs& a, int cta, int ncta, c
 // ---------------------------------------------------------------------------
 constexpr int kEllRowsPerPass = kBlock * 4;
 
-template <bool ATOMIC>
-__device__ __forceinline__ void ell_cta(const EllArgs& a, int cta, int ncta, char*)
+template <bool ATOMIC, class V>
+__device__ __forceinline__ void ell_cta(const EllArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
     cta_share(a.rows, 4, cta, ncta, b, e);
     for (long long row0 = b + threadIdx.x * 4; row0 < e; row0 += kEllRowsPerPass) {
         const int* cp = a.col + row0;
-        const float* dp = a.data + row0;
+        const V* dp = a.data + row0;
         float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 4
         for (int k = 0; k < a.ell_num; k++) {
             const int4 c = ld_stream_i4(cp + (size_t)k * a.len, pe);
-            const float4 v = ld_stream_f4(dp + (size_t)k * a.len, pe);
+            const float4 v = ldv4(dp + (size_t)k * a.len, pe);
             acc[0] = fmaf(v.x, ld_x(a.x + c.x, pl), acc[0]);
             acc[1] = fmaf(v.y, ld_x(a.x + c.y, pl), acc[1]);
             acc[2] = fmaf(v.z, ld_x(a.x + c.z, pl), acc[2]);
             acc[3] = fmaf(v.w, ld_x(a.x + c.w, pl), acc[3]);
         }
-        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta);
+        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta, scl(a));
     }
 }
 
@@ -217,8 +218,8 @@ __device__ __forceinline__ void ell_cta(const EllArgs& a, int cta, int ncta, cha
 // ---------------------------------------------------------------------------
 constexpr int kSellWarpCols = 64;
 
-template <int Q, bool ATOMIC_ALL>
-__device__ __forceinline__ void sell_cta(const SellArgs& a, int cta, int ncta, char*)
+template <int Q, bool ATOMIC_ALL, class V>
+__device__ __forceinline__ void sell_cta(const SellArgsT<V>& a, int cta, int ncta, char*)
 {
     constexpr int G = 32 / Q;             // columns per warp step
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
@@ -251,7 +252,7 @@ __device__ __forceinline__ void sell_cta(const SellArgs& a, int cta, int ncta, c
             for (long long cc = c + g; cc < ce; cc += G) {
                 const size_t base = (size_t)cc * sh + 4 * q;
                 const int4 cv = ld_stream_i4(a.col + base, pe);
-                const float4 v = ld_stream_f4(a.data + base, pe);
+                const float4 v = ldv4(a.data + base, pe);
                 acc[0] = fmaf(v.x, ld_x(a.x + cv.x, pl), acc[0]);
                 acc[1] = fmaf(v.y, ld_x(a.x + cv.y, pl), acc[1]);
                 acc[2] = fmaf(v.z, ld_x(a.x + cv.z, pl), acc[2]);
@@ -268,8 +269,9 @@ __device__ __forceinline__ void sell_cta(const SellArgs& a, int cta, int ncta, c
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     if (row0 + i < a.rows) {
-                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += a.alpha * acc[i];
-                        else atomicAdd(a.y + row0 + i, a.alpha * acc[i]);
+                        const float al = row_alpha(a.alpha, scl(a), row0 + i);
+                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += al * acc[i];
+                        else atomicAdd(a.y + row0 + i, al * acc[i]);
                     }
                 }
             }
@@ -280,8 +282,8 @@ __device__ __forceinline__ void sell_cta(const SellArgs& a, int cta, int ncta, c
 }
 
 // Other slice heights: one row per thread, slice by slice.
-template <bool ATOMIC>
-__device__ __forceinline__ void sell_rows_cta(const SellArgs& a, int cta, int ncta, char*)
+template <bool ATOMIC, class V>
+__device__ __forceinline__ void sell_rows_cta(const SellArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
@@ -295,9 +297,9 @@ __device__ __forceinline__ void sell_rows_cta(const SellArgs& a, int cta, int nc
 #pragma unroll 4
         for (int k = 0; k < width; k++) {
             const size_t i = (size_t)start + (size_t)k * sh + lr;
-            acc = fmaf(ld_stream_f(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
+            acc = fmaf(ldv(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
         }
-        y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
+        y_update<ATOMIC>(a.y, row, row_alpha(a.alpha, scl(a), row), a.beta, acc);
     }
 }
 
@@ -387,7 +389,8 @@ constexpr int kMergeIPT = 8;
 constexpr int kMergeTile = kBlock * kMergeIPT;
 constexpr int kMergeSmemBytes = (kMergeTile + 2) * sizeof(int) + kMergeTile * sizeof(float) + (kMergeTile + 1) * sizeof(float);
 
-__device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __restrict__ tc, int tile, char* smem)
+template <class V>
+__device__ __forceinline__ void csr_merge_tile(const CsrArgsT<V>& a, const int* __restrict__ tc, int tile, char* smem)
 {
     int* s_rp = reinterpret_cast<int*>(smem);
     float* s_prod = reinterpret_cast<float*>(s_rp + kMergeTile + 2);
@@ -407,7 +410,7 @@ __device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __re
 #pragma unroll
         for (int i = 0; i < kMergeIPT; i++) {
             const int k = threadIdx.x + i * kBlock;
-            vv[i] = k < nz ? ld_stream_f(a.val + y0 + k, pe) : 0.f;
+            vv[i] = k < nz ? ldv(a.val + y0 + k, pe) : 0.f;
         }
 #pragma unroll
         for (int i = 0; i <= kMergeIPT; i++) {
@@ -458,7 +461,7 @@ __device__ __forceinline__ void csr_merge_tile(const CsrArgs& a, const int* __re
         if (r >= a.rows) break;
         const int rs = s_rp[k], re = s_rp[k + 1];
         const int from = max(rs, y0), to = k < nfin ? re : y1;
-        if (to > from) atomicAdd(a.y + r, a.alpha * s_y[k]);
+        if (to > from) atomicAdd(a.y + r, row_alpha(a.alpha, scl(a), r) * s_y[k]);
     }
 }
 
@@ -496,12 +499,15 @@ constexpr int kCooWarpNnz = 128 * kCooSteps;
 constexpr int kCooCtaNnz = kCooWarpNnz * (kBlock / 32);
 constexpr int kCooNoRow = INT_MAX;
 
-__device__ __forceinline__ void coo_red(float* y, int row, float v)
+// adds alpha * v (times the row's scale for 16-bit values) to y[row]
+template <class V>
+__device__ __forceinline__ void coo_red(const CooArgsT<V>& a, int row, float v)
 {
-    if (row != kCooNoRow) atomicAdd(y + row, v);
+    if (row != kCooNoRow) atomicAdd(a.y + row, row_alpha(a.alpha, scl(a), row) * v);
 }
 
-__device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base, uint64_t pe, uint64_t pl)
+template <class V>
+__device__ __forceinline__ void coo_warp_chunk(const CooArgsT<V>& a, long long base, uint64_t pe, uint64_t pl)
 {
     const int lane = threadIdx.x & 31;
     int r[kCooSteps][4];
@@ -514,7 +520,7 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base,
             if (idx + 3 < a.nnz) {
                 const int4 rv = ld_stream_i4(a.row + idx, pe);
                 const int4 cv = ld_stream_i4(a.col + idx, pe);
-                const float4 vv = ld_stream_f4(a.val + idx, pe);
+                const float4 vv = ldv4(a.val + idx, pe);
                 r[s][0] = rv.x; r[s][1] = rv.y; r[s][2] = rv.z; r[s][3] = rv.w;
                 c[s][0] = cv.x; c[s][1] = cv.y; c[s][2] = cv.z; c[s][3] = cv.w;
                 p[s][0] = vv.x; p[s][1] = vv.y; p[s][2] = vv.z; p[s][3] = vv.w;
@@ -524,7 +530,7 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base,
                     const bool in = idx + j < a.nnz;
                     r[s][j] = in ? ld_stream_i(a.row + idx + j, pe) : kCooNoRow;
                     c[s][j] = in ? ld_stream_i(a.col + idx + j, pe) : 0;
-                    p[s][j] = in ? ld_stream_f(a.val + idx + j, pe) : 0.f;
+                    p[s][j] = in ? ldv(a.val + idx + j, pe) : 0.f;
                 }
             }
         }
@@ -558,17 +564,17 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base,
                 } else if (rj == run_row) {
                     run += p[s][j];
                 } else {
-                    if (run_row >= 0) coo_red(a.y, run_row, a.alpha * run);
+                    if (run_row >= 0) coo_red(a, run_row, run);
                     run_row = rj;
                     run = p[s][j];
                 }
             }
-            if (run_row >= 0) coo_red(a.y, run_row, a.alpha * run);
+            if (run_row >= 0) coo_red(a, run_row, run);
         }
         // the previous step's trailing row
         const int lead = __shfl_sync(kFull, head_row, 0);
         if (carry_row >= 0 && lead != carry_row) {
-            if (lane == 0) coo_red(a.y, carry_row, a.alpha * carry);
+            if (lane == 0) coo_red(a, carry_row, carry);
             carry_row = -1;
             carry = 0.f;
         }
@@ -590,18 +596,19 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgs& a, long long base,
         const float prev_v = __shfl_up_sync(kFull, v, 1);
         if (!single) {
             const float cin = (lane > 0 && prev_tail_row == head_row) ? prev_v : 0.f;
-            coo_red(a.y, head_row, a.alpha * (head + cin));
+            coo_red(a, head_row, head + cin);
         }
         const int next_head = __shfl_down_sync(kFull, head_row, 1);
-        if (lane < 31 && next_head != tail_row) coo_red(a.y, tail_row, a.alpha * v);
+        if (lane < 31 && next_head != tail_row) coo_red(a, tail_row, v);
         carry = __shfl_sync(kFull, v, 31);
         carry_row = __shfl_sync(kFull, tail_row, 31);
         if (carry_row == kCooNoRow) carry_row = -1;
     }
-    if (carry_row >= 0 && lane == 0) coo_red(a.y, carry_row, a.alpha * carry);
+    if (carry_row >= 0 && lane == 0) coo_red(a, carry_row, carry);
 }
 
-__device__ __forceinline__ void coo_cta(const CooArgs& a, int cta, int ncta, char*)
+template <class V>
+__device__ __forceinline__ void coo_cta(const CooArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     const long long nchunks = ((long long)a.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
@@ -615,8 +622,8 @@ __device__ __forceinline__ void coo_cta(const CooArgs& a, int cta, int ncta, cha
 // (slot, w4, h) plane is a contiguous float4 array over block rows, so a warp
 // reads 512 contiguous bytes per load. x blocks are 16-byte aligned float4.
 // ---------------------------------------------------------------------------
-template <int BW4, int BH, bool ATOMIC>
-__device__ __forceinline__ void b4ell_cta(const B4ellArgs& a, int cta, int ncta, char*)
+template <int BW4, int BH, bool ATOMIC, class V>
+__device__ __forceinline__ void b4ell_cta(const B4ellArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
@@ -626,16 +633,16 @@ __device__ __forceinline__ void b4ell_cta(const B4ellArgs& a, int cta, int ncta,
         float acc[BH];
 #pragma unroll
         for (int h = 0; h < BH; h++) acc[h] = 0.f;
-        const float* base = a.data + (size_t)r * 4;
+        const V* base = a.data + (size_t)r * 4;
 #pragma unroll 2
         for (int j = 0; j < a.ellnum; j++) {
             const int c4 = ld_stream_i(a.col + (size_t)j * a.len + r, pe);
-            const float* bj = base + (size_t)j * colsz;
+            const V* bj = base + (size_t)j * colsz;
             float4 v[BW4][BH];
 #pragma unroll
             for (int w4 = 0; w4 < BW4; w4++)
 #pragma unroll
-                for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bj + (size_t)w4 * a.f4 * BH + (size_t)h * a.f4, pe);
+                for (int h = 0; h < BH; h++) v[w4][h] = ldv4(bj + (size_t)w4 * a.f4 * BH + (size_t)h * a.f4, pe);
 #pragma unroll
             for (int w4 = 0; w4 < BW4; w4++) {
                 const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
@@ -646,7 +653,7 @@ __device__ __forceinline__ void b4ell_cta(const B4ellArgs& a, int cta, int ncta,
 #pragma unroll
         for (int h = 0; h < BH; h++) {
             const long long row = r * BH + h;
-            if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+            if (row < a.rows) y_update<ATOMIC>(a.y, row, row_alpha(a.alpha, scl(a), row), a.beta, acc[h]);
         }
     }
 }
@@ -656,8 +663,8 @@ __device__ __forceinline__ void b4ell_cta(const B4ellArgs& a, int cta, int ncta,
 // thread per block row, so a 32-high slice is one warp and every plane load
 // is 512 contiguous bytes.
 // ---------------------------------------------------------------------------
-template <int BW4, int BH, bool ATOMIC>
-__device__ __forceinline__ void sbell_cta(const SbellArgs& a, int cta, int ncta, char*)
+template <int BW4, int BH, bool ATOMIC, class V>
+__device__ __forceinline__ void sbell_cta(const SbellArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     long long b, e;
@@ -672,16 +679,16 @@ __device__ __forceinline__ void sbell_cta(const SbellArgs& a, int cta, int ncta,
         float acc[BH];
 #pragma unroll
         for (int h = 0; h < BH; h++) acc[h] = 0.f;
-        const float* base = a.data + (size_t)cs * bs + (size_t)lr * 4;
+        const V* base = a.data + (size_t)cs * bs + (size_t)lr * 4;
 #pragma unroll 2
         for (int j = 0; j < width; j++) {
             const int c4 = ld_stream_i(a.col + (size_t)cs + lr + (size_t)j * sh, pe);
-            const float* bj = base + (size_t)j * colsz;
+            const V* bj = base + (size_t)j * colsz;
             float4 v[BW4][BH];
 #pragma unroll
             for (int w4 = 0; w4 < BW4; w4++)
 #pragma unroll
-                for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bj + (size_t)w4 * w4sz + (size_t)h * hsz, pe);
+                for (int h = 0; h < BH; h++) v[w4][h] = ldv4(bj + (size_t)w4 * w4sz + (size_t)h * hsz, pe);
 #pragma unroll
             for (int w4 = 0; w4 < BW4; w4++) {
                 const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
@@ -692,7 +699,7 @@ __device__ __forceinline__ void sbell_cta(const SbellArgs& a, int cta, int ncta,
 #pragma unroll
         for (int h = 0; h < BH; h++) {
             const long long row = r * BH + h;
-            if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+            if (row < a.rows) y_update<ATOMIC>(a.y, row, row_alpha(a.alpha, scl(a), row), a.beta, acc[h]);
         }
     }
 }
@@ -704,8 +711,8 @@ __device__ __forceinline__ void sbell_cta(const SbellArgs& a, int cta, int ncta,
 // a warp read contiguous memory. Partial sums are combined with shuffles
 // (the reference reduces in __local memory per 128-thread group).
 // ---------------------------------------------------------------------------
-template <int BW4, int BH, int T, bool ATOMIC>
-__device__ __forceinline__ void b4csr_cta(const B4csrArgs& a, int cta, int ncta, char*)
+template <int BW4, int BH, int T, bool ATOMIC, class V>
+__device__ __forceinline__ void b4csr_cta(const B4csrArgsT<V>& a, int cta, int ncta, char*)
 {
     constexpr int kRowsPerPass = kBlock / T;
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
@@ -723,12 +730,12 @@ __device__ __forceinline__ void b4csr_cta(const B4csrArgs& a, int cta, int ncta,
             const int s = a.row_ptr[g], en = a.row_ptr[g + 1];
             for (int i = s + l; i < en; i += T) {
                 const int c4 = ld_stream_i(a.col + i, pe);
-                const float* bi = a.data + (size_t)i * 4;
+                const V* bi = a.data + (size_t)i * 4;
                 float4 v[BW4][BH];
 #pragma unroll
                 for (int w4 = 0; w4 < BW4; w4++)
 #pragma unroll
-                    for (int h = 0; h < BH; h++) v[w4][h] = ld_stream_f4(bi + w4 * plane_w4 + (size_t)h * a.len, pe);
+                    for (int h = 0; h < BH; h++) v[w4][h] = ldv4(bi + w4 * plane_w4 + (size_t)h * a.len, pe);
 #pragma unroll
                 for (int w4 = 0; w4 < BW4; w4++) {
                     const float4 xv = load_x4_guarded(a.x, (c4 + w4) * 4, a.cols, pl);
@@ -746,7 +753,7 @@ __device__ __forceinline__ void b4csr_cta(const B4csrArgs& a, int cta, int ncta,
 #pragma unroll
             for (int h = 0; h < BH; h++) {
                 const long long row = g * BH + h;
-                if (row < a.rows) y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc[h]);
+                if (row < a.rows) y_update<ATOMIC>(a.y, row, row_alpha(a.alpha, scl(a), row), a.beta, acc[h]);
             }
         }
     }

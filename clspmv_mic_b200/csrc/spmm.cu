@@ -780,6 +780,11 @@ int clspmv_spmm(int format, const void* dev, int value_type, const void* values,
     if (matrix_rows(dev) <= 0) return CLSPMV_OK;
     Dense d{k, X, ldx, Y, ldy, alpha, beta, value_type == CLSPMV_VALUES_F32 ? nullptr : row_scale, lshift};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // one contiguous vector: the format's own single-vector kernel (CSR's needs a merge plan)
+    if (k == 1 && ldx == 1 && ldy == 1 && format != CLSPMV_FORMAT_CSR) {
+        rc = launch_packed(format, dev, value_type, values, row_scale, nullptr, X, Y, alpha, beta, st, false);
+        if (rc != CLSPMV_ERR_ALIGN) return rc;
+    }
     switch (value_type) {
         case CLSPMV_VALUES_F32: return spmm_typed<float>(format, dev, nullptr, d, vec, st);
         case CLSPMV_VALUES_BF16: return spmm_typed<__nv_bfloat16>(format, dev, values, d, vec, st);

@@ -37,6 +37,8 @@ int after_launch(int n)
 namespace {
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+// value arrays are read 4 values at a time
+template <class V> inline bool aligned_v4(const V* p) { return (reinterpret_cast<uintptr_t>(p) & (4 * sizeof(V) - 1)) == 0; }
 inline cudaStream_t S(clspmv_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 inline unsigned grid_for(long long units, long long per_cta) { return (unsigned)((units + per_cta - 1) / per_cta); }
 
@@ -49,24 +51,24 @@ __global__ void __launch_bounds__(kBlock) k_scale(float* y, int n, float beta)
     if (i < n) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
 }
 
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_dia(DiaArgs a)
+template <bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_dia(DiaArgsT<V> a)
 {
     __shared__ __align__(16) char smem[kDiaSmemBytes];
     dia_cta<A>(a, blockIdx.x, gridDim.x, smem);
 }
 
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgs a) { bdia_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgsT<V> a) { bdia_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_ell(EllArgs a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_ell(EllArgsT<V> a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <int Q, bool A>
-__global__ void __launch_bounds__(kBlock) k_sell(SellArgs a) { sell_cta<Q, A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int Q, bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_sell(SellArgsT<V> a) { sell_cta<Q, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <bool A>
-__global__ void __launch_bounds__(kBlock) k_sell_rows(SellArgs a) { sell_rows_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_sell_rows(SellArgsT<V> a) { sell_rows_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
@@ -74,7 +76,8 @@ __global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_c
 template <int T, bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_vector(CsrArgs a) { csr_vector_cta<T, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-__global__ void __launch_bounds__(kBlock) k_csr_merge(CsrArgs a, const int* __restrict__ tc)
+template <class V>
+__global__ void __launch_bounds__(kBlock) k_csr_merge(CsrArgsT<V> a, const int* __restrict__ tc)
 {
     extern __shared__ __align__(16) char dsmem[];
     csr_merge_tile(a, tc, blockIdx.x, dsmem);
@@ -87,16 +90,17 @@ __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, co
     csr_merge_search(rows, nnz, row_ptr, (long long)t * kMergeTile, tc + 2 * t);
 }
 
-__global__ void __launch_bounds__(kBlock) k_coo(CooArgs a) { coo_cta(a, blockIdx.x, gridDim.x, nullptr); }
+template <class V>
+__global__ void __launch_bounds__(kBlock) k_coo(CooArgsT<V> a) { coo_cta(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <int BW4, int BH, bool A>
-__global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgs a) { b4ell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int BW4, int BH, bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgsT<V> a) { b4ell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <int BW4, int BH, bool A>
-__global__ void __launch_bounds__(kBlock) k_sbell(SbellArgs a) { sbell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int BW4, int BH, bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_sbell(SbellArgsT<V> a) { sbell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <int BW4, int BH, int T, bool A>
-__global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgs a) { b4csr_cta<BW4, BH, T, A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int BW4, int BH, int T, bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgsT<V> a) { b4csr_cta<BW4, BH, T, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
 // CTAs that fit on the device at once for `kernel` (SM count x resident
 // CTAs per SM), cached per kernel.
@@ -197,55 +201,78 @@ namespace clspmv {
 
 int launch_prescale(float* y, int n, float beta, cudaStream_t st) { return prescale(y, n, beta, st); }
 
-int launch_dia(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+template <class V>
+int launch_dia_v(const clspmv_dia_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                 cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
     if (rows <= 0) return CLSPMV_OK;
-    if (m->dia_num > 0 && (!m->dia_offsets || !m->dia_data)) return CLSPMV_ERR_ARG;
-    if ((m->dia_length_aligned & 3) || !aligned16(m->dia_data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
-    DiaArgs a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, m->dia_data, x, y, alpha, beta};
-    if (atomic) k_dia<true><<<persistent_grid(k_dia<true>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
-    else k_dia<false><<<persistent_grid(k_dia<false>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    if (m->dia_num > 0 && (!m->dia_offsets || !data)) return CLSPMV_ERR_ARG;
+    if ((m->dia_length_aligned & 3) || !aligned_v4(data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
+    DiaArgsT<V> a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, data, x, y, alpha, beta, scale};
+    if (atomic) k_dia<true, V><<<persistent_grid(k_dia<true, V>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    else k_dia<false, V><<<persistent_grid(k_dia<false, V>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    return after_launch(1);
+}
+
+int launch_dia(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_dia_v<float>(m, m ? m->dia_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+template <class V>
+int launch_bdia_v(const clspmv_bdia_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                  cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !data)) return CLSPMV_ERR_ARG;
+    if ((m->bdia_length_aligned & 3) || !aligned_v4(data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
+    BdiaArgsT<V> a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, data, x, y, alpha, beta, scale};
+    if (atomic) k_bdia<true, V><<<persistent_grid(k_bdia<true, V>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
+    else k_bdia<false, V><<<persistent_grid(k_bdia<false, V>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
 int launch_bdia(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
 {
+    return launch_bdia_v<float>(m, m ? m->bdia_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+template <class V>
+int launch_ell_v(const clspmv_ell_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                 cudaStream_t st, bool atomic)
+{
     if (!m || !x || !y) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
     if (rows <= 0) return CLSPMV_OK;
-    if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data)) return CLSPMV_ERR_ARG;
-    if ((m->bdia_length_aligned & 3) || !aligned16(m->bdia_data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
-    BdiaArgs a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, m->bdia_data, x, y, alpha, beta};
-    if (atomic) k_bdia<true><<<persistent_grid(k_bdia<true>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
-    else k_bdia<false><<<persistent_grid(k_bdia<false>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
+    if (m->ell_num > 0 && (!m->ell_col_id || !data)) return CLSPMV_ERR_ARG;
+    if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned_v4(data) || rows > m->ell_height_aligned)
+        return CLSPMV_ERR_ALIGN;
+    EllArgsT<V> a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, data, x, y, alpha, beta, scale};
+    if (atomic) k_ell<true, V><<<persistent_grid(k_ell<true, V>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
+    else k_ell<false, V><<<persistent_grid(k_ell<false, V>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
 int launch_ell(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
 {
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0) return CLSPMV_OK;
-    if (m->ell_num > 0 && (!m->ell_col_id || !m->ell_data)) return CLSPMV_ERR_ARG;
-    if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned16(m->ell_data) || rows > m->ell_height_aligned)
-        return CLSPMV_ERR_ALIGN;
-    EllArgs a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, m->ell_data, x, y, alpha, beta};
-    if (atomic) k_ell<true><<<persistent_grid(k_ell<true>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
-    else k_ell<false><<<persistent_grid(k_ell<false>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
-    return after_launch(1);
+    return launch_ell_v<float>(m, m ? m->ell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
 }
 
-int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+template <class V>
+int launch_sell_v(const clspmv_sell_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                  cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y || !m->sell_slice_ptr) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
     const int sh = (int)m->sell_slice_height;
     if (rows <= 0) return CLSPMV_OK;
     if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
-    SellArgs a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data, x, y, alpha, beta};
-    const bool vec = aligned16(m->sell_col_id) && aligned16(m->sell_data);
+    SellArgsT<V> a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, data, x, y, alpha, beta, scale};
+    const bool vec = aligned16(m->sell_col_id) && aligned_v4(data);
     if (vec && (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
         if (!atomic) {
             int rc = prescale(y, rows, beta, st);
@@ -254,14 +281,19 @@ int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha,
         a.beta = 1.0f;
         return dispatch_lanes(sh / 4, [&](auto q) {
             constexpr int Q = decltype(q)::value;
-            if (atomic) k_sell<Q, true><<<persistent_grid(k_sell<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a);
-            else k_sell<Q, false><<<persistent_grid(k_sell<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a);
+            if (atomic) k_sell<Q, true, V><<<persistent_grid(k_sell<Q, true, V>, 1LL << 40, 1), kBlock, 0, st>>>(a);
+            else k_sell<Q, false, V><<<persistent_grid(k_sell<Q, false, V>, 1LL << 40, 1), kBlock, 0, st>>>(a);
             return after_launch(1);
         });
     }
-    if (atomic) k_sell_rows<true><<<persistent_grid(k_sell_rows<true>, rows, kBlock), kBlock, 0, st>>>(a);
-    else k_sell_rows<false><<<persistent_grid(k_sell_rows<false>, rows, kBlock), kBlock, 0, st>>>(a);
+    if (atomic) k_sell_rows<true, V><<<persistent_grid(k_sell_rows<true, V>, rows, kBlock), kBlock, 0, st>>>(a);
+    else k_sell_rows<false, V><<<persistent_grid(k_sell_rows<false, V>, rows, kBlock), kBlock, 0, st>>>(a);
     return after_launch(1);
+}
+
+int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_sell_v<float>(m, m ? m->sell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
 }
 
 int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
@@ -294,7 +326,9 @@ int launch_csr_vector(const clspmv_csr_f32* m, const float* x, float* y, float a
     });
 }
 
-int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+template <class V>
+int launch_csr_merge_v(const clspmv_csr_f32* m, const V* data, const float* scale, const int* tc, const float* x, float* y,
+                       float alpha, float beta, cudaStream_t st, bool atomic)
 {
     if (!m || !tc || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
@@ -304,12 +338,19 @@ int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, flo
         if (rc) return rc;
     }
     const int ntiles = clspmv_csr_merge_tiles(rows, m->matinfo.nnz);
-    CsrArgs a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, m->csr_data, x, y, alpha, 1.0f};
-    k_csr_merge<<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
+    CsrArgsT<V> a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, data, x, y, alpha, 1.0f, scale};
+    k_csr_merge<V><<<ntiles, kBlock, kMergeSmemBytes, st>>>(a, tc);
     return after_launch(1);
 }
 
-int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_csr_merge_v<float>(m, m ? m->csr_data : nullptr, nullptr, tc, x, y, alpha, beta, st, atomic);
+}
+
+template <class V>
+int launch_coo_v(const clspmv_coo_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                 cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
@@ -319,71 +360,144 @@ int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, f
         if (rc) return rc;
     }
     if (m->matinfo.nnz <= 0) return CLSPMV_OK;
-    if (!m->coo_row_id || !m->coo_col_id || !m->coo_data) return CLSPMV_ERR_ARG;
-    if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned16(m->coo_data)) return CLSPMV_ERR_ALIGN;
-    CooArgs a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, m->coo_data, x, y, alpha};
-    k_coo<<<persistent_grid(k_coo, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
+    if (!m->coo_row_id || !m->coo_col_id || !data) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
+    CooArgsT<V> a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, data, x, y, alpha, scale};
+    k_coo<V><<<persistent_grid(k_coo<V>, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
-int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_coo_v<float>(m, m ? m->coo_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+template <class V>
+int launch_b4ell_v(const clspmv_b4ell_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                   cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
     if (rows <= 0 || m->b4ell_row_num <= 0) return CLSPMV_OK;
-    if (!m->b4ell_col_id || !m->b4ell_data) return CLSPMV_ERR_ARG;
-    if ((m->b4ell_float4_aligned & 3) || !aligned16(m->b4ell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if (!m->b4ell_col_id || !data) return CLSPMV_ERR_ARG;
+    if ((m->b4ell_float4_aligned & 3) || !aligned_v4(data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
     if ((long long)m->b4ell_row_num * m->b4ell_bheight < rows || m->b4ell_float4_aligned < 4 * m->b4ell_row_num) return CLSPMV_ERR_ARG;
-    const B4ellArgs a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
-                      m->b4ell_float4_aligned, m->b4ell_col_id, m->b4ell_data, x, y, alpha, beta};
+    const B4ellArgsT<V> a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
+                          m->b4ell_float4_aligned, m->b4ell_col_id, data, x, y, alpha, beta, scale};
     return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
         constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
-        if (atomic) k_b4ell<BW4, BH, true><<<persistent_grid(k_b4ell<BW4, BH, true>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        else k_b4ell<BW4, BH, false><<<persistent_grid(k_b4ell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        if (atomic) k_b4ell<BW4, BH, true, V><<<persistent_grid(k_b4ell<BW4, BH, true, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        else k_b4ell<BW4, BH, false, V><<<persistent_grid(k_b4ell<BW4, BH, false, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    });
+}
+
+int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_b4ell_v<float>(m, m ? m->b4ell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+template <class V>
+int launch_sbell_v(const clspmv_sbell_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                   cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0 || m->sbell_row_num <= 0) return CLSPMV_OK;
+    if (!m->sbell_slice_ptr || !m->sbell_col_id || !data || m->sbell_slice_height == 0) return CLSPMV_ERR_ARG;
+    if (!aligned_v4(data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
+    const SbellArgsT<V> a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
+                          m->sbell_slice_ptr, m->sbell_col_id, data, x, y, alpha, beta, scale};
+    return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
+        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
+        if (atomic) k_sbell<BW4, BH, true, V><<<persistent_grid(k_sbell<BW4, BH, true, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        else k_sbell<BW4, BH, false, V><<<persistent_grid(k_sbell<BW4, BH, false, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
         return after_launch(1);
     });
 }
 
 int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
 {
-    if (!m || !x || !y) return CLSPMV_ERR_ARG;
-    const int rows = m->matinfo.height;
-    if (rows <= 0 || m->sbell_row_num <= 0) return CLSPMV_OK;
-    if (!m->sbell_slice_ptr || !m->sbell_col_id || !m->sbell_data || m->sbell_slice_height == 0) return CLSPMV_ERR_ARG;
-    if (!aligned16(m->sbell_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
-    if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
-    const SbellArgs a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
-                      m->sbell_slice_ptr, m->sbell_col_id, m->sbell_data, x, y, alpha, beta};
-    return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
-        constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
-        if (atomic) k_sbell<BW4, BH, true><<<persistent_grid(k_sbell<BW4, BH, true>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        else k_sbell<BW4, BH, false><<<persistent_grid(k_sbell<BW4, BH, false>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        return after_launch(1);
-    });
+    return launch_sbell_v<float>(m, m ? m->sbell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
 }
 
-int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+template <class V>
+int launch_b4csr_v(const clspmv_b4csr_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
+                   cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
     if (rows <= 0 || m->b4csr_row_num <= 0) return CLSPMV_OK;
-    if (!m->b4csr_row_ptr || !m->b4csr_col_id || !m->b4csr_data) return CLSPMV_ERR_ARG;
-    if ((m->b4csr_aligned_size & 3) || !aligned16(m->b4csr_data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
+    if (!m->b4csr_row_ptr || !m->b4csr_col_id || !data) return CLSPMV_ERR_ARG;
+    if ((m->b4csr_aligned_size & 3) || !aligned_v4(data) || !aligned16(x)) return CLSPMV_ERR_ALIGN;
     if ((long long)m->b4csr_row_num * m->b4csr_bheight < rows) return CLSPMV_ERR_ARG;
-    const B4csrArgs a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
-                      m->b4csr_row_ptr, m->b4csr_col_id, m->b4csr_data, x, y, alpha, beta};
+    const B4csrArgsT<V> a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
+                          m->b4csr_row_ptr, m->b4csr_col_id, data, x, y, alpha, beta, scale};
     const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num, 1, 32);
     return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
         return dispatch_lanes(lanes, [&](auto t) {
             constexpr int T = decltype(t)::value;
             constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
             if (atomic)
-                k_b4csr<BW4, BH, T, true><<<persistent_grid(k_b4csr<BW4, BH, T, true>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
+                k_b4csr<BW4, BH, T, true, V><<<persistent_grid(k_b4csr<BW4, BH, T, true, V>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
             else
-                k_b4csr<BW4, BH, T, false><<<persistent_grid(k_b4csr<BW4, BH, T, false>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
+                k_b4csr<BW4, BH, T, false, V><<<persistent_grid(k_b4csr<BW4, BH, T, false, V>, a.nbrow, kBlock / T), kBlock, 0, st>>>(a);
             return after_launch(1);
         });
     });
+}
+
+int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    return launch_b4csr_v<float>(m, m ? m->b4csr_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+// Single-vector SpMV with 16-bit values (clspmv_pack_values) in the format's
+// dedicated kernel.
+template <class V>
+int launch_packed_t(int format, const void* dev, const V* vals, const float* scale, const int* tc, const float* x, float* y,
+                    float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    switch (format) {
+        case CLSPMV_FORMAT_CSR: return launch_csr_merge_v(static_cast<const clspmv_csr_f32*>(dev), vals, scale, tc, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_COO: return launch_coo_v(static_cast<const clspmv_coo_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_DIA: return launch_dia_v(static_cast<const clspmv_dia_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_BDIA: return launch_bdia_v(static_cast<const clspmv_bdia_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_ELL: return launch_ell_v(static_cast<const clspmv_ell_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_SELL: return launch_sell_v(static_cast<const clspmv_sell_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_B4CSR: return launch_b4csr_v(static_cast<const clspmv_b4csr_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_B4ELL: return launch_b4ell_v(static_cast<const clspmv_b4ell_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+        case CLSPMV_FORMAT_SBELL: return launch_sbell_v(static_cast<const clspmv_sbell_f32*>(dev), vals, scale, x, y, alpha, beta, st, atomic);
+    }
+    return CLSPMV_ERR_ARG;
+}
+
+int launch_packed(int format, const void* dev, int value_type, const void* values, const float* scale, const int* tc,
+                  const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!dev) return CLSPMV_ERR_ARG;
+    if (format == CLSPMV_FORMAT_CSR && !tc) return CLSPMV_ERR_ARG;
+    if (value_type == CLSPMV_VALUES_F32) {   // the struct's own FP32 values
+        switch (format) {
+            case CLSPMV_FORMAT_CSR: return launch_csr_merge(static_cast<const clspmv_csr_f32*>(dev), tc, x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_COO: return launch_coo(static_cast<const clspmv_coo_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_DIA: return launch_dia(static_cast<const clspmv_dia_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_BDIA: return launch_bdia(static_cast<const clspmv_bdia_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_ELL: return launch_ell(static_cast<const clspmv_ell_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_SELL: return launch_sell(static_cast<const clspmv_sell_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_B4CSR: return launch_b4csr(static_cast<const clspmv_b4csr_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_B4ELL: return launch_b4ell(static_cast<const clspmv_b4ell_f32*>(dev), x, y, alpha, beta, st, atomic);
+            case CLSPMV_FORMAT_SBELL: return launch_sbell(static_cast<const clspmv_sbell_f32*>(dev), x, y, alpha, beta, st, atomic);
+        }
+        return CLSPMV_ERR_ARG;
+    }
+    if (!values || !scale) return CLSPMV_ERR_ARG;
+    if (value_type == CLSPMV_VALUES_BF16)
+        return launch_packed_t(format, dev, static_cast<const __nv_bfloat16*>(values), scale, tc, x, y, alpha, beta, st, atomic);
+    if (value_type == CLSPMV_VALUES_F16)
+        return launch_packed_t(format, dev, static_cast<const __half*>(values), scale, tc, x, y, alpha, beta, st, atomic);
+    return CLSPMV_ERR_ARG;
 }
 
 int launch_csr_merge_plan(const clspmv_csr_f32* m, int* tc, cudaStream_t st)
@@ -454,5 +568,8 @@ int clspmv_sbell_spmv_f32(const clspmv_sbell_f32* m, const float* x, float* y, f
 { return launch_sbell(m, x, y, alpha, beta, S(s), false); }
 int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_b4csr(m, x, y, alpha, beta, S(s), false); }
+int clspmv_spmv_packed(int format, const void* dev, int value_type, const void* values, const float* row_scale,
+                       const int* tile_coord, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{ return launch_packed(format, dev, value_type, values, row_scale, tile_coord, x, y, alpha, beta, S(s), false); }
 
 }  // extern "C"

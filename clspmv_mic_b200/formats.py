@@ -283,10 +283,17 @@ class DeviceMatrix:
         return self._plan
 
     def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None, variant: str = "merge",
-             threads_per_row: int = 0) -> None:
-        """y <- alpha * A x + beta * y on the device (asynchronous on `stream`)."""
+             threads_per_row: int = 0, packed: "PackedValues | None" = None) -> None:
+        """y <- alpha * A x + beta * y on the device (asynchronous on `stream`);
+        with `packed`, from the 16-bit values of self.pack()."""
         L = lib()
         s = _stream_handle(stream)
+        if packed is not None:
+            plan = self.merge_plan(stream).data_ptr() if self.fmt == "csr" else None
+            check(L.clspmv_spmv_packed(_abi.FORMAT_IDS[self.fmt], C.byref(self.struct), _abi.VALUE_TYPES[packed.value_type],
+                                       packed.values.data_ptr(), packed.row_scale.data_ptr(), plan, x.data_ptr(),
+                                       y.data_ptr(), alpha, beta, s), "spmv_packed")
+            return
         if self.fmt == "csr":
             if variant == "merge":
                 plan = self.merge_plan(stream)

@@ -13,9 +13,12 @@ Y = alpha * A * X with any k; a loop thread forms batches continuously:
   that arrive while a batch runs are admitted into the next slot and their
   work overlaps the running batch on the device.
 
-Each request's result is the same whether it runs alone or in a mix: every
-row of Y is one group's sum over that row's stored elements, in storage
-order, whatever the other columns and jobs are (tests/test_serving_gpu.py).
+Each request's result is the same whether it runs alone or in a mix, within
+the FP32 bound: in a batch every row of Y is one group's sum over that row's
+stored elements in storage order, whatever the other columns and jobs are;
+alone, the same values may be summed in another order (CSR splits rows by
+nonzeros, k = 1 uses the format's single-vector kernel)
+(tests/test_serving_gpu.py).
 
 The reference has no serving path; its runtime runs one matrix per call and
 waits for it (src/spmv_cocktail.cpp:1088-1132).

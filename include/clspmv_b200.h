@@ -420,6 +420,14 @@ int clspmv_stored_values(int format, const void* dev, size_t* count);
 int clspmv_pack_values(int format, const void* dev, int value_type, void* values, float* row_scale,
                        clspmv_stream_t stream);
 
+/* y <- alpha * A * x + beta * y with the 16-bit values and row scales of
+ * clspmv_pack_values, in the format's own single-vector kernel (half the
+ * value bytes of the FP32 call). `tile_coord` is the merge-path plan of the
+ * matrix (clspmv_csr_merge_plan), used and required for CSR only. */
+int clspmv_spmv_packed(int format, const void* dev, int value_type, const void* values, const float* row_scale,
+                       const int* tile_coord, const float* x, float* y, float alpha, float beta,
+                       clspmv_stream_t stream);
+
 /* One Y <- alpha * A * X + beta * Y of a batch (fields as in clspmv_spmm). */
 typedef struct {
     int format;              /* clspmv_format; every format but COO */

@@ -5,7 +5,9 @@
   gives alone (clspmv_spmm), within the FP32 bound;
 * the batch launch replays correctly from a captured CUDA graph;
 * the server admits matrices by memory budget, fuses requests, and every
-  result equals the result of the same request run alone.
+  result equals the result of the same request run alone within the FP32
+  bound (the stored values are the same; only the summation order may
+  differ).
 """
 import random
 import threading
@@ -79,8 +81,9 @@ def test_batch_matches_alone(graph):
     for j, a, (name, fmt, _) in zip(jobs, alone, MATS * 2):
         got, ref = j.Y.cpu().numpy(), a.cpu().numpy()
         assert np.all(np.isfinite(got)), (name, fmt)
-        # rows are summed in storage order in both; CSR alone splits rows by nonzeros
-        tol = 1e-5 * np.abs(ref).max() + 1e-6 if fmt == "csr" else 0.0
+        # the same stored values; alone, CSR splits rows by nonzeros and k = 1 runs the format's own
+        # single-vector kernel, so the summation order (not the values) may differ
+        tol = 1e-5 * np.abs(ref).max() + 1e-6
         assert np.max(np.abs(got - ref)) <= tol, (name, fmt, np.max(np.abs(got - ref)))
     b.close()
 
@@ -137,7 +140,6 @@ def test_server_mixed_requests_match_alone():
         dev, packed = devs[key]
         ref = _alone(dev, X, 1.0, packed).cpu().numpy()
         got = Y.cpu().numpy()
-        fmt = dev.fmt
-        tol = 1e-5 * np.abs(ref).max() + 1e-6 if fmt == "csr" else 0.0
-        assert np.max(np.abs(got - ref)) <= tol, (key, fmt)
+        tol = 1e-5 * np.abs(ref).max() + 1e-6
+        assert np.max(np.abs(got - ref)) <= tol, (key, dev.fmt)
     assert stats["p99_ms"] >= stats["p50_ms"] > 0

@@ -142,3 +142,33 @@ def test_spmm_rejects():
     with pytest.raises(_abi.ClspmvError) as e:
         dev.spmm(X, torch.zeros((dev.shape[0], 39), device="cuda"))
     assert e.value.status == _abi.ERR_ALIGN
+
+
+PACKED_CASES = [("laplace33", "csr", ()), ("powerlaw3k", "coo", ()), ("laplace33", "dia", ()), ("stencil6", "bdia", ()),
+                ("powerlaw3k", "ell", ()), ("powerlaw3k", "sell", (32,)), ("random_empty_rows", "sell", (20,)),
+                ("blocks_odd", "b4csr", (8, 4)), ("blocks300", "b4ell", (4, 2)), ("blocks300", "sbell", (4, 8)),
+                ("random_empty_rows", "csr", ()), ("random_empty_rows", "coo", ())]
+
+
+@pytest.mark.parametrize("value_type", ["bf16", "f16"])
+@pytest.mark.parametrize("name,fmt,args", PACKED_CASES)
+def test_spmv_packed_dedicated(name, fmt, args, value_type):
+    """Single-vector SpMV with 16-bit values in each format's own kernel."""
+    import torch
+    coo = coo_of(name)
+    m, n = coo.shape
+    dev = device_of(coo, fmt, *args)
+    p = dev.pack(value_type)
+    x = synth.x_vector(n, seed=3)
+    y0 = np.random.default_rng(2).uniform(-1, 1, m).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (-0.5, 1.5)]:
+        xd = torch.from_numpy(x).cuda()
+        yd = torch.from_numpy(y0.copy()).cuda()
+        n0 = F.launch_count()
+        dev.spmv(xd, yd, alpha, beta, packed=p)
+        torch.cuda.synchronize()
+        assert F.launch_count() > n0
+        ref, bound = spmm_reference(coo, x[:, None], y0[:, None], alpha, beta)
+        err = np.abs(yd.cpu().numpy().astype(np.float64) - ref[:, 0])
+        lim = RTOL[value_type] * bound[:, 0] + 1e-6 * abs(beta) * np.abs(y0) + 1e-30
+        assert np.all(err <= lim), (name, fmt, args, value_type, alpha, beta, float((err / (bound[:, 0] + 1e-30)).max()))
