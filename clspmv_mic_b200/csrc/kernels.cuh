@@ -72,7 +72,8 @@ __device__ __forceinline__ void y_put4(const float* acc, long long row0, long lo
 constexpr int kDiaRowsPerPass = kBlock * 4;
 constexpr int kDiaSmemBytes = kBlock * sizeof(int);
 
-template <bool ATOMIC, class V>
+// XA: x is 16-byte aligned, so x windows are read with 128-bit loads.
+template <bool ATOMIC, class V, bool XA = false>
 __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta, char* smem)
 {
     int* s_off = reinterpret_cast<int*>(smem);
@@ -102,7 +103,17 @@ __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta,
                     const int c = (int)row0 + s_off[k];
                     const float4 v = ldv4(dp + (size_t)k * a.len, pe);
                     float x0, x1, x2, x3;
-                    if (c >= 0 && c + 3 < a.cols) {
+                    const int base = c & ~3;   // rows start at multiples of 4: c & 3 is the same for the whole CTA
+                    if (XA && base >= 0 && base + 7 < a.cols) {
+                        // x[c .. c+3] from one or two aligned 128-bit loads
+                        const float4 xa = ld_x4(a.x + base, pl);
+                        switch (c & 3) {
+                            case 0: x0 = xa.x; x1 = xa.y; x2 = xa.z; x3 = xa.w; break;
+                            case 1: { const float4 xb = ld_x4(a.x + base + 4, pl); x0 = xa.y; x1 = xa.z; x2 = xa.w; x3 = xb.x; break; }
+                            case 2: { const float4 xb = ld_x4(a.x + base + 4, pl); x0 = xa.z; x1 = xa.w; x2 = xb.x; x3 = xb.y; break; }
+                            default: { const float4 xb = ld_x4(a.x + base + 4, pl); x0 = xa.w; x1 = xb.x; x2 = xb.y; x3 = xb.z; break; }
+                        }
+                    } else if (c >= 0 && c + 3 < a.cols) {
                         x0 = ld_x(a.x + c, pl);
                         x1 = ld_x(a.x + c + 1, pl);
                         x2 = ld_x(a.x + c + 2, pl);
@@ -137,7 +148,7 @@ __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta,
 constexpr int kBdiaRowsPerPass = kBlock * 4;
 constexpr int kBdiaRun = 4;
 
-template <bool ATOMIC, class V>
+template <bool ATOMIC, class V, bool XA = false>
 __device__ __forceinline__ void bdia_cta(const BdiaArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
@@ -156,10 +167,35 @@ __device__ __forceinline__ void bdia_cta(const BdiaArgsT<V>& a, int cta, int nct
 #pragma unroll
                 for (int t = 0; t < kBdiaRun; t++)
                     if (t < n) v[t] = ldv4(a.data + (size_t)(j0 + t) * a.len + row0, pe);
+                const long long base = c0 & ~3LL;   // c0 & 3 is the same for the whole CTA
+                if (XA && base >= 0 && base + 11 < a.cols) {
+                    // the window x[c0 .. c0+6] from three aligned 128-bit loads
+                    const float4 w0 = ld_x4(a.x + base, pl), w1 = ld_x4(a.x + base + 4, pl), w2 = ld_x4(a.x + base + 8, pl);
+                    const float win[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+                    switch (c0 & 3) {
+                        case 0:
 #pragma unroll
-                for (int t = 0; t < kBdiaRun + 3; t++) {
-                    const long long c = c0 + t;
-                    xw[t] = (t < n + 3 && c >= 0 && c < a.cols) ? ld_x(a.x + c, pl) : 0.f;
+                            for (int t = 0; t < kBdiaRun + 3; t++) xw[t] = win[t];
+                            break;
+                        case 1:
+#pragma unroll
+                            for (int t = 0; t < kBdiaRun + 3; t++) xw[t] = win[t + 1];
+                            break;
+                        case 2:
+#pragma unroll
+                            for (int t = 0; t < kBdiaRun + 3; t++) xw[t] = win[t + 2];
+                            break;
+                        default:
+#pragma unroll
+                            for (int t = 0; t < kBdiaRun + 3; t++) xw[t] = win[t + 3];
+                            break;
+                    }
+                } else {
+#pragma unroll
+                    for (int t = 0; t < kBdiaRun + 3; t++) {
+                        const long long c = c0 + t;
+                        xw[t] = (t < n + 3 && c >= 0 && c < a.cols) ? ld_x(a.x + c, pl) : 0.f;
+                    }
                 }
 #pragma unroll
                 for (int t = 0; t < kBdiaRun; t++) {

@@ -2,6 +2,7 @@
 // libclspmv_b200.so: argument checks, template dispatch, launches.
 #include <atomic>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -51,15 +52,39 @@ __global__ void __launch_bounds__(kBlock) k_scale(float* y, int n, float beta)
     if (i < n) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
 }
 
-template <bool A, class V>
+template <bool A, class V, bool XA>
 __global__ void __launch_bounds__(kBlock) k_dia(DiaArgsT<V> a)
 {
     __shared__ __align__(16) char smem[kDiaSmemBytes];
-    dia_cta<A>(a, blockIdx.x, gridDim.x, smem);
+    dia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, smem);
 }
 
-template <bool A, class V>
-__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgsT<V> a) { bdia_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <bool A, class V, bool XA>
+__global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgsT<V> a) { bdia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, nullptr); }
+
+// the same, capped at the registers that keep 8 (DIA) / 5 (BDIA) CTAs of 256 threads per SM
+template <bool A, class V, bool XA>
+__global__ void __launch_bounds__(kBlock, 8) k_dia_occ(DiaArgsT<V> a)
+{
+    __shared__ __align__(16) char smem[kDiaSmemBytes];
+    dia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, smem);
+}
+template <bool A, class V, bool XA>
+__global__ void __launch_bounds__(kBlock, 5) k_bdia_occ(BdiaArgsT<V> a) { bdia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, nullptr); }
+
+// Kernel form of the diagonal formats: 0 scalar x loads, 1 aligned x
+// windows, 2 aligned x windows with the register cap. Measured on B200
+// (stencil27 128^3): DIA is fastest with form 0 (74.6 % of peak vs 60 / 72),
+// BDIA with form 1 (78 % vs 69 / 75). CLSPMV_DIA_FORM overrides both (for
+// measurements).
+int dia_form(int dflt)
+{
+    static int forced = [] {
+        const char* e = getenv("CLSPMV_DIA_FORM");
+        return e ? atoi(e) : -1;
+    }();
+    return forced >= 0 ? forced : dflt;
+}
 
 template <bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_ell(EllArgsT<V> a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
@@ -211,8 +236,17 @@ int launch_dia_v(const clspmv_dia_f32* m, const V* data, const float* scale, con
     if (m->dia_num > 0 && (!m->dia_offsets || !data)) return CLSPMV_ERR_ARG;
     if ((m->dia_length_aligned & 3) || !aligned_v4(data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
     DiaArgsT<V> a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, data, x, y, alpha, beta, scale};
-    if (atomic) k_dia<true, V><<<persistent_grid(k_dia<true, V>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
-    else k_dia<false, V><<<persistent_grid(k_dia<false, V>, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a);
+    const int form = aligned16(x) ? dia_form(0) : 0;
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a); };
+    if (atomic) {
+        if (form == 2) go(k_dia_occ<true, V, true>);
+        else if (form == 1) go(k_dia<true, V, true>);
+        else go(k_dia<true, V, false>);
+    } else {
+        if (form == 2) go(k_dia_occ<false, V, true>);
+        else if (form == 1) go(k_dia<false, V, true>);
+        else go(k_dia<false, V, false>);
+    }
     return after_launch(1);
 }
 
@@ -231,8 +265,17 @@ int launch_bdia_v(const clspmv_bdia_f32* m, const V* data, const float* scale, c
     if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !data)) return CLSPMV_ERR_ARG;
     if ((m->bdia_length_aligned & 3) || !aligned_v4(data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
     BdiaArgsT<V> a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, data, x, y, alpha, beta, scale};
-    if (atomic) k_bdia<true, V><<<persistent_grid(k_bdia<true, V>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
-    else k_bdia<false, V><<<persistent_grid(k_bdia<false, V>, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a);
+    const int form = aligned16(x) ? dia_form(1) : 0;
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a); };
+    if (atomic) {
+        if (form == 2) go(k_bdia_occ<true, V, true>);
+        else if (form == 1) go(k_bdia<true, V, true>);
+        else go(k_bdia<true, V, false>);
+    } else {
+        if (form == 2) go(k_bdia_occ<false, V, true>);
+        else if (form == 1) go(k_bdia<false, V, true>);
+        else go(k_bdia<false, V, false>);
+    }
     return after_launch(1);
 }
 
