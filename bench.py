@@ -525,6 +525,7 @@ def run_ours(args):
     }
     if not args.no_extras and not args.only and world == 1:
         line["extras"] = run_extras(args, items, mats, peak)
+        line["extras"]["cocktail_c3"] = run_cocktail_c3(args, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)
         line["cpu_baseline"] = {"value": round(f_cpu / t_cpu / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
@@ -616,6 +617,64 @@ def run_extras(args, items, mats, peak):
     del smats
     torch.cuda.empty_cache()
     out["serving"]["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
+def run_cocktail_c3(args, peak):
+    """The Cocktail matrix (4M rows: 7-diagonal band 1.5M rows, 4x4 blocks
+    1.5M rows, power-law 1M rows): benchmark tables measured on this GPU,
+    partitioned by analyze_matrix, the parts run concurrently by the
+    Cocktail runtime."""
+    import tempfile
+    import torch
+    from clspmv_mic_b200 import formats as F
+    from clspmv_mic_b200 import synth
+    from clspmv_mic_b200 import tables as T
+    from clspmv_mic_b200 import workloads as W
+    out = {}
+    t0 = time.perf_counter()
+    root = Path(tempfile.mkdtemp(prefix="clspmv_tables_"))
+    T.measure_tables(root)
+    out["tables_seconds"] = round(time.perf_counter() - t0, 1)
+    t0 = time.perf_counter()
+    arrs = synth.cocktail_mixed()
+    coo = F.coo_matrix(*arrs)
+    out["generate_seconds"] = round(time.perf_counter() - t0, 1)
+    from clspmv_mic_b200.autotune import tune
+    t0 = time.perf_counter()
+    res = tune(coo, root, cache=root / "tune.json", use_cache=False)
+    mat = res.matrix
+    out["tune_seconds"] = round(time.perf_counter() - t0, 1)
+    out["tuning"] = {"chosen_knob": res.knob, "candidates": res.report,
+                     "note": "each analyze_matrix knob setting of the reference, partition measured with the "
+                             "Cocktail runtime; the first candidate is the reference's default"}
+    out["partition"] = mat.summary()
+    dev = mat.to_device()
+    h, w = coo.shape
+    x = torch.rand(w, device="cuda") * 2 - 1
+    y = torch.zeros(h, device="cuda")
+    dev.spmv(x, y, 1.0, 0.0)
+    csr = F.DeviceMatrix(F.coo2csr(coo))
+    band, block = 1_500_000, 1_500_000
+    ref = W.Fp64Rows(csr, rows=1 << 15, starts=(0, band, band + block))
+    out["err_fp64"] = ref.error(x[:, None], y[:, None])
+    del csr, ref
+    for _ in range(5):
+        dev.spmv(x, y, 1.0, 1.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        dev.spmv(x, y, 1.0, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    stored = sum(p.stored_bytes() for p in mat.parts().values())
+    ab = stored + 4 * w + 8 * h
+    out.update(rows=h, nnz=int(coo.nnz), ms=round(ms, 4), gflops=round(2 * coo.nnz / (ms * 1e-3) / 1e9, 1),
+               alg_bytes=int(ab), gbs=round(ab / (ms * 1e-3) / 1e9, 1), frac=round(ab / (ms * 1e-3) / 1e9 / peak, 3),
+               note="alg bytes = every part's stored arrays + x once + y read and written once")
+    dev.close()
     return out
 
 

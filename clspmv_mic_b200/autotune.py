@@ -1,0 +1,126 @@
+"""Device-measured choice of a matrix's Cocktail partition.
+
+The Cocktail partitioner (analyze_matrix, src/analyze.cpp:3714-3900) picks
+formats from benchmark tables and its own cost estimates; some of those
+estimates are blind to costs that dominate on a GPU (an SBELL slice as wide
+as its widest block row, for instance, is estimated at the mean block
+count). The reference exposes three knobs for such cases
+(src/eval.cpp:83-95: the DIA priority multiplier, estimate_flat_partial,
+estimate_flat_full). tune() runs the partitioner under each knob setting,
+measures every distinct partition on the device with the Cocktail runtime,
+keeps the fastest, and caches the winning setting per matrix signature, so
+the next matrix with the same structure is partitioned once, without
+measuring.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from .cocktail import CocktailMatrix, analyze
+from .formats import HostMatrix
+
+KNOBS = [
+    {},                                   # the reference's defaults
+    {"estimate_flat_partial": False},
+    {"estimate_flat_full": True},
+    {"dia_priority_multiplier": 2.0},
+    {"dia_priority_multiplier": 2.0, "estimate_flat_partial": False},
+    {"dia_priority_multiplier": 0.5},
+]
+
+
+def signature(coo: HostMatrix) -> str:
+    """Structural fingerprint: shape, nonzeros, and log2 histograms of the
+    row lengths and of the distances |col - row| (matrices that share it
+    get the same partition setting)."""
+    a = coo.arrays()
+    h, w = coo.shape
+    r, c = a["coo_row_id"].astype(np.int64), a["coo_col_id"].astype(np.int64)
+    lens = np.bincount(r, minlength=h) if r.size else np.zeros(h, np.int64)
+    lh = np.bincount(np.log2(lens + 1).astype(np.int64), minlength=16)[:32]
+    dh = np.bincount(np.log2(np.abs(c - r) + 1).astype(np.int64), minlength=32)[:40]
+    frac = lambda v: np.round(v / max(1, v.sum()), 3).tolist()
+    key = json.dumps([h, w, int(coo.nnz), frac(lh), frac(dh)])
+    return hashlib.sha1(key.encode()).hexdigest()[:20]
+
+
+def _partition_key(m: CocktailMatrix):
+    return tuple(sorted((k, v["nnz"]) for k, v in m.summary().items() if isinstance(v, dict) and "nnz" in v))
+
+
+def measure_ms(m: CocktailMatrix, reps: int = 10) -> float:
+    """Mean time of y += A x over `reps` runs of the Cocktail runtime."""
+    import torch
+    dev = m.to_device()
+    try:
+        h, w = m.struct.mat_height, m.struct.mat_width
+        x = torch.rand(w, device="cuda")
+        y = torch.zeros(h, device="cuda")
+        for _ in range(3):
+            dev.spmv(x, y, 1.0, 1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            dev.spmv(x, y, 1.0, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+    finally:
+        dev.close()
+
+
+@dataclass
+class TuneResult:
+    matrix: CocktailMatrix
+    knob: dict
+    ms: float
+    from_cache: bool = False
+    report: list = field(default_factory=list)
+
+
+def default_cache() -> Path:
+    return Path(os.environ.get("CLSPMV_TUNE_CACHE", Path.home() / ".cache" / "clspmv_b200" / "cocktail_tune.json"))
+
+
+def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None, reps: int = 10,
+         knobs=KNOBS, use_cache: bool = True) -> TuneResult:
+    """Fastest measured partition of `coo` over the knob settings."""
+    cache = Path(cache) if cache is not None else default_cache()
+    sig = signature(coo)
+    entries = {}
+    if cache.exists():
+        try:
+            entries = json.loads(cache.read_text())
+        except (OSError, ValueError):
+            entries = {}
+    if use_cache and sig in entries:
+        knob = entries[sig]["knob"]
+        return TuneResult(analyze(coo, table_dir, **knob), knob, entries[sig]["ms"], from_cache=True)
+    best, seen, report = None, {}, []
+    for knob in knobs:
+        m = analyze(coo, table_dir, **knob)
+        key = _partition_key(m)
+        if key in seen:
+            report.append(dict(knob=knob, partition=dict(key), ms=seen[key], same_as_earlier=True))
+            continue
+        ms = measure_ms(m, reps)
+        seen[key] = ms
+        report.append(dict(knob=knob, partition=dict(key), ms=round(ms, 4)))
+        if best is None or ms < best.ms:
+            best = TuneResult(m, knob, ms)
+        else:
+            del m
+    best.report = report
+    entries[sig] = {"knob": best.knob, "ms": best.ms, "shape": list(coo.shape), "nnz": int(coo.nnz)}
+    try:
+        cache.parent.mkdir(parents=True, exist_ok=True)
+        cache.write_text(json.dumps(entries, indent=1))
+    except OSError:
+        pass
+    return best

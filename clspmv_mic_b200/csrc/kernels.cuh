@@ -253,6 +253,7 @@ __device__ __forceinline__ void ell_cta(const EllArgsT<V>& a, int cta, int ncta,
 // {4, 8, 16, 32, 64, 128} and beta already applied.
 // ---------------------------------------------------------------------------
 constexpr int kSellWarpCols = 64;
+constexpr int kSellNarrow = 12;   // mean nonzeros per row at or below which slices count as narrow
 
 template <int Q, bool ATOMIC_ALL, class V>
 __device__ __forceinline__ void sell_cta(const SellArgsT<V>& a, int cta, int ncta, char*)
@@ -314,6 +315,35 @@ __device__ __forceinline__ void sell_cta(const SellArgsT<V>& a, int cta, int nct
             c = ce;
             s++;
         }
+    }
+}
+
+// Narrow slices (few columns each): 4 rows per thread inside one slice,
+// int4 / float4 loads of each slice column, like ELL. Requires slice_height
+// a multiple of 4 and 16-byte aligned arrays.
+template <bool ATOMIC, class V>
+__device__ __forceinline__ void sell_rows4_cta(const SellArgsT<V>& a, int cta, int ncta, char*)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    long long b, e;
+    cta_share(a.rows, 4, cta, ncta, b, e);
+    const int sh = a.slice_height;
+    for (long long row0 = b + threadIdx.x * 4; row0 < e; row0 += kBlock * 4) {
+        const int s = (int)(row0 / sh), lr = (int)(row0 - (long long)s * sh);
+        const int start = a.slice_ptr[s];
+        const int width = (a.slice_ptr[s + 1] - start) / sh;
+        const size_t base = (size_t)start + lr;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+        for (int k = 0; k < width; k++) {
+            const int4 c = ld_stream_i4(a.col + base + (size_t)k * sh, pe);
+            const float4 v = ldv4(a.data + base + (size_t)k * sh, pe);
+            acc[0] = fmaf(v.x, ld_x(a.x + c.x, pl), acc[0]);
+            acc[1] = fmaf(v.y, ld_x(a.x + c.y, pl), acc[1]);
+            acc[2] = fmaf(v.z, ld_x(a.x + c.z, pl), acc[2]);
+            acc[3] = fmaf(v.w, ld_x(a.x + c.w, pl), acc[3]);
+        }
+        y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta, scl(a));
     }
 }
 

@@ -95,6 +95,9 @@ __global__ void __launch_bounds__(kBlock) k_sell(SellArgsT<V> a) { sell_cta<Q, A
 template <bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_sell_rows(SellArgsT<V> a) { sell_rows_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
+template <bool A, class V>
+__global__ void __launch_bounds__(kBlock) k_sell_rows4(SellArgsT<V> a) { sell_rows4_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
@@ -316,6 +319,14 @@ int launch_sell_v(const clspmv_sell_f32* m, const V* data, const float* scale, c
     if (sh <= 0 || (long long)m->sell_slice_num * sh < rows) return CLSPMV_ERR_ARG;
     SellArgsT<V> a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, data, x, y, alpha, beta, scale};
     const bool vec = aligned16(m->sell_col_id) && aligned_v4(data);
+    // Narrow slices (about kSellNarrow stored entries per row or fewer): 4 rows
+    // per thread. Wide or uneven slices: the column-balanced kernel, which
+    // spreads one wide slice over many warps.
+    if (vec && sh % 4 == 0 && (long long)m->matinfo.nnz <= (long long)kSellNarrow * rows) {
+        if (atomic) k_sell_rows4<true, V><<<persistent_grid(k_sell_rows4<true, V>, rows, kBlock * 4), kBlock, 0, st>>>(a);
+        else k_sell_rows4<false, V><<<persistent_grid(k_sell_rows4<false, V>, rows, kBlock * 4), kBlock, 0, st>>>(a);
+        return after_launch(1);
+    }
     if (vec && (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
         if (!atomic) {
             int rc = prescale(y, rows, beta, st);

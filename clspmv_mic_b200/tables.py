@@ -20,7 +20,8 @@ model_tables() writes a deterministic bandwidth model of this library's
 kernels on B200 (measured HBM copy bandwidth, launch overhead, x-gather
 cost); `seed` perturbs the variant factors so tests can drive the
 partitioner down different branches. measure_tables() fills the same files
-from timings of the library's kernels on the device.
+from timings of the library's kernels on the device (regular synthetic
+matrices of each format built on the device).
 """
 from __future__ import annotations
 
@@ -113,6 +114,87 @@ def model_tables(root: str | os.PathLike, seed: int = 0, hbm_gbs: float = 6000.0
                 lines["csr"].append(f"{d} {w} {g} " + " ".join(f"{v:.6f}" for v in csr))
                 lines["coo"].append(f"{d} {w} {g} " + " ".join(f"{v:.6f}" for v in coo))
 
+    for name, ls in lines.items():
+        (out / f"{name}.ben").write_text("\n".join(ls) + "\n")
+    return Path(root)
+
+
+# grids of the device-measured tables (the partitioner interpolates between
+# grid points and clamps outside them, src/analyze.cpp:294-428)
+M_DIMS = [16384, 131072, 1048576, 2097152]
+M_BLOCK_DIMS = [16384, 131072, 1048576]
+M_DIA_WIDTHS = [1, 3, 5, 7, 9, 15, 27, 31, 63]
+M_FLAT_WIDTHS = [1, 2, 4, 8, 16, 32, 64]
+M_BLOCKNUMS = [1, 2, 4, 8, 16]
+M_GROUPS = [24, 192]
+
+
+def _time_ms(run, reps: int = 10) -> float:
+    import torch
+    for _ in range(3):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def measure_tables(root: str | os.PathLike, reps: int = 10, device="cuda") -> Path:
+    """Writes <root>/benchmark/*.ben from timings of this library's kernels
+    on the current device (what the reference's bench_* programs do with
+    its OpenCL kernels, src/bench_dia.cpp:355-400 and the others): regular
+    synthetic matrices of each format built on the device
+    (device_build.py), y += A x timed with CUDA events, GFLOP/s =
+    2 nnz / time. Every kernel-variant column of a table gets the value of
+    this library's one kernel for that format, except SELL, whose two
+    columns are slice heights 32 and 128."""
+    import torch
+    from . import device_build as D
+    from .drivers import bandwidth_test
+    out = Path(root) / "benchmark"
+    out.mkdir(parents=True, exist_ok=True)
+    lines = {k: [] for k in ["overhead", "bdia", "dia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo"]}
+
+    def gflops(m, nnz, **kw):
+        x = torch.rand(m.shape[1], device=device)
+        y = torch.zeros(m.shape[0], device=device)
+        ms = _time_ms(lambda: m.spmv(x, y, 1.0, 1.0, **kw), reps)
+        return 2.0 * nnz / (ms * 1e-3) / 1e9
+
+    launch_us = bandwidth_test(1 << 20, 50)["launch_us"]
+    for g in OVH_GROUPS:
+        for th in OVH_THREADS:
+            lines["overhead"].append(f"{g} {th} {launch_us:.6f}")
+    for d in M_DIMS:
+        for w in M_DIA_WIDTHS:
+            dv = gflops(D.dia(d, w, device=device), d * w)
+            bv = gflops(D.bdia(d, w, device=device), d * w)
+            lines["dia"].append(f"{d} {w} " + " ".join(f"{dv:.6f}" for _ in range(IMP["dia"])))
+            lines["bdia"].append(f"{d} {w} " + " ".join(f"{bv:.6f}" for _ in range(IMP["bdia"])))
+            torch.cuda.empty_cache()
+    for name, build in (("sbell", D.sbell), ("bell", D.b4ell), ("bcsr", D.b4csr)):
+        for (bh, bw) in SHAPES:
+            for d in M_BLOCK_DIMS:
+                for b in M_BLOCKNUMS:
+                    v = gflops(build(d, b, bh, bw, device=device), d * b * bw)
+                    lines[name].append(f"{bh} {bw} {d} {b} " + " ".join(f"{v:.6f}" for _ in range(IMP[name])))
+                torch.cuda.empty_cache()
+    for d in M_DIMS:
+        for w in M_FLAT_WIDTHS:
+            s32 = gflops(D.sell(d, w, 32, device=device), d * w)
+            s128 = gflops(D.sell(d, w, 128, device=device), d * w)
+            ev = gflops(D.ell(d, w, device=device), d * w)
+            lines["sell"].append(f"{d} {w} {s32:.6f} {s128:.6f}")
+            lines["ell"].append(f"{d} {w} " + " ".join(f"{ev:.6f}" for _ in range(IMP["ell"])))
+            cv = gflops(D.csr(d, w, device=device), d * w, variant="merge")
+            ov = gflops(D.coo(d, w, device=device), d * w)
+            for g in M_GROUPS:
+                lines["csr"].append(f"{d} {w} {g} " + " ".join(f"{cv:.6f}" for _ in range(IMP["csr"])))
+                lines["coo"].append(f"{d} {w} {g} {ov:.6f}")
+            torch.cuda.empty_cache()
     for name, ls in lines.items():
         (out / f"{name}.ben").write_text("\n".join(ls) + "\n")
     return Path(root)

@@ -27,18 +27,33 @@ def _events(torch):
 
 
 class Fp64Rows:
-    """The first `rows` rows of a device CSR matrix kept for the FP64
-    accuracy check (row of each entry, column, FP64 value)."""
+    """Rows of a device CSR matrix kept for the FP64 accuracy check (row of
+    each entry, column, FP64 value): the first `rows` rows, or `rows` rows
+    from each start in `starts`."""
 
-    def __init__(self, dev_csr: DeviceMatrix, rows: int = 1 << 16):
+    def __init__(self, dev_csr: DeviceMatrix, rows: int = 1 << 16, starts=(0,)):
         import torch
         t = dev_csr.tensors
-        self.rows = min(rows, dev_csr.shape[0])
-        rp = t["csr_row_ptr"][: self.rows + 1].long()
-        end = int(rp[-1].item())
-        self.row_of = torch.repeat_interleave(torch.arange(self.rows, device=rp.device), rp[1:] - rp[:-1])
-        self.col = t["csr_col_id"][:end].long()
-        self.val = t["csr_data"][:end].double()
+        h = dev_csr.shape[0]
+        rp_all = t["csr_row_ptr"].long()
+        ids, cols, vals = [], [], []
+        sel = []
+        for s0 in starts:
+            s1 = min(h, s0 + rows)
+            if s1 <= s0:
+                continue
+            rp = rp_all[s0: s1 + 1]
+            a, b = int(rp[0].item()), int(rp[-1].item())
+            local = torch.repeat_interleave(torch.arange(s1 - s0, device=rp.device), rp[1:] - rp[:-1])
+            ids.append(local + len(torch.cat(sel)) if sel else local)
+            sel.append(torch.arange(s0, s1, device=rp.device))
+            cols.append(t["csr_col_id"][a:b].long())
+            vals.append(t["csr_data"][a:b].double())
+        self.sel = torch.cat(sel)
+        self.rows = int(self.sel.numel())
+        self.row_of = torch.cat(ids)
+        self.col = torch.cat(cols)
+        self.val = torch.cat(vals)
 
     def error(self, X, Y) -> float:
         """max over the kept rows of |Y - A X| / (|A| |X|), in FP64."""
@@ -50,7 +65,7 @@ class Fp64Rows:
         xr = Xd[self.col]
         ref.index_add_(0, self.row_of, self.val[:, None] * xr)
         scale.index_add_(0, self.row_of, (self.val[:, None] * xr).abs())
-        err = (Y[: self.rows].double() - ref).abs() / scale.clamp_min(1e-300)
+        err = (Y[self.sel].double() - ref).abs() / scale.clamp_min(1e-300)
         return float(err.max().item()) if err.numel() else 0.0
 
 

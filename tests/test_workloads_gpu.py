@@ -39,3 +39,44 @@ def test_serve_small():
     assert r["matrices"] == 4
     assert r["served"]["req_per_s"] > 0 and r["sequential"]["req_per_s"] > 0
     assert r["served"]["p99_ms"] >= r["served"]["p50_ms"]
+
+
+def test_measure_tables_small(tmp_path, monkeypatch):
+    """Device-measured .ben tables are readable by the partitioner and give
+    positive rates for every grid point."""
+    from clspmv_mic_b200 import tables as T
+    from clspmv_mic_b200.cocktail import analyze
+    monkeypatch.setattr(T, "M_DIMS", [4096, 65536])
+    monkeypatch.setattr(T, "M_BLOCK_DIMS", [4096, 65536])
+    monkeypatch.setattr(T, "M_DIA_WIDTHS", [1, 5, 27])
+    monkeypatch.setattr(T, "M_FLAT_WIDTHS", [1, 8, 32])
+    monkeypatch.setattr(T, "M_BLOCKNUMS", [1, 4])
+    T.measure_tables(tmp_path, reps=2)
+    for name in ["overhead", "bdia", "dia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo"]:
+        rows = [list(map(float, l.split())) for l in (tmp_path / "benchmark" / f"{name}.ben").read_text().splitlines()]
+        assert rows and all(v > 0 for r in rows for v in r), name
+    m = analyze(coo_of("blocks300"), tmp_path)
+    assert sum(v["nnz"] for k, v in m.summary().items() if isinstance(v, dict) and "nnz" in v and k != "shape") > 0
+
+
+def test_tune_measures_and_caches(tmp_path):
+    from clspmv_mic_b200 import tables as T
+    from clspmv_mic_b200.autotune import tune
+    root = T.model_tables(tmp_path / "t", seed=3, scale={"coo": 0.3})
+    coo = coo_of("powerlaw3k")
+    cache = tmp_path / "tune.json"
+    r = tune(coo, root, cache=cache, reps=2)
+    assert not r.from_cache and r.ms > 0 and r.report and r.report[0]["knob"] == {}
+    assert min(c["ms"] for c in r.report) == pytest.approx(r.ms, abs=1e-4)
+    again = tune(coo, root, cache=cache)
+    assert again.from_cache and again.knob == r.knob
+    import torch
+    dev = again.matrix.to_device()
+    x = torch.rand(coo.shape[1], device="cuda")
+    y = torch.zeros(coo.shape[0], device="cuda")
+    dev.spmv(x, y, 1.0, 0.0)
+    torch.cuda.synchronize()
+    csr = F.coo2csr(coo)
+    y64, sc = __import__("oracle.oracle", fromlist=["x"]).csr_f64(csr, x.cpu().numpy())
+    assert np.all(np.abs(y.cpu().numpy() - y64) <= 1e-5 * sc + 1e-30)
+    dev.close()
