@@ -40,6 +40,20 @@ __device__ __forceinline__ float4 load_x4_guarded(const float* x, int c, int col
     return v;
 }
 
+// x[b .. b+3] for b a multiple of 4 (x 16-byte aligned), zero outside [0, cols)
+__device__ __forceinline__ float4 load_x4_window(const float* x, int b, int cols, uint64_t pol)
+{
+    if (b >= 0 && b + 3 < cols) return ld_x4(x + b, pol);
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (b + 3 >= 0 && b < cols) {
+        if ((unsigned)b < (unsigned)cols) v.x = ld_x(x + b, pol);
+        if ((unsigned)(b + 1) < (unsigned)cols) v.y = ld_x(x + b + 1, pol);
+        if ((unsigned)(b + 2) < (unsigned)cols) v.z = ld_x(x + b + 2, pol);
+        if ((unsigned)(b + 3) < (unsigned)cols) v.w = ld_x(x + b + 3, pol);
+    }
+    return v;
+}
+
 __device__ __forceinline__ float x_or_zero(const float* x, int c, int cols, uint64_t pol)
 {
     return (unsigned)c < (unsigned)cols ? ld_x(x + c, pol) : 0.f;
@@ -72,8 +86,11 @@ __device__ __forceinline__ void y_put4(const float* acc, long long row0, long lo
 constexpr int kDiaRowsPerPass = kBlock * 4;
 constexpr int kDiaSmemBytes = kBlock * sizeof(int);
 
-// XA: x is 16-byte aligned, so x windows are read with 128-bit loads.
-template <bool ATOMIC, class V, bool XA = false>
+// XF (x form), for a 16-byte aligned x: 0 four scalar x loads per diagonal;
+// 1 one or two aligned 128-bit loads; 3 one aligned 128-bit load per thread,
+// the next 4 values taken from the neighbouring lane by shuffles (the lanes
+// of a warp own consecutive groups of 4 rows).
+template <bool ATOMIC, class V, int XF = 0>
 __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta, char* smem)
 {
     int* s_off = reinterpret_cast<int*>(smem);
@@ -96,7 +113,36 @@ __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta,
                 if (threadIdx.x < nd) s_off[threadIdx.x] = a.offsets[d0 + threadIdx.x];
                 __syncthreads();
             }
-            if (active) {
+            if (XF == 3) {
+                // every lane runs the loop (the shuffles need the whole warp); inactive lanes load nothing
+                const V* dp = a.data + (size_t)d0 * a.len + (active ? row0 : 0);
+                const int lane = threadIdx.x & 31;
+#pragma unroll 4
+                for (int k = 0; k < nd; k++) {
+                    const int c = (int)row0 + s_off[k];
+                    const int sh = c & 3;           // the same for the whole CTA
+                    const int base = c - sh;
+                    const float4 v = active ? ldv4(dp + (size_t)k * a.len, pe) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    // inactive lanes still load their window: the lane below takes it by shuffle
+                    const float4 xa = load_x4_window(a.x, base, a.cols, pl);
+                    float x0 = xa.x, x1 = xa.y, x2 = xa.z, x3 = xa.w;
+                    if (sh) {
+                        float4 xb;
+                        xb.x = __shfl_down_sync(kFull, xa.x, 1);
+                        xb.y = __shfl_down_sync(kFull, xa.y, 1);
+                        xb.z = __shfl_down_sync(kFull, xa.z, 1);
+                        xb.w = __shfl_down_sync(kFull, xa.w, 1);
+                        if (lane == 31) xb = load_x4_window(a.x, base + 4, a.cols, pl);
+                        if (sh == 1) { x0 = xa.y; x1 = xa.z; x2 = xa.w; x3 = xb.x; }
+                        else if (sh == 2) { x0 = xa.z; x1 = xa.w; x2 = xb.x; x3 = xb.y; }
+                        else { x0 = xa.w; x1 = xb.x; x2 = xb.y; x3 = xb.z; }
+                    }
+                    acc[0] = fmaf(v.x, x0, acc[0]);
+                    acc[1] = fmaf(v.y, x1, acc[1]);
+                    acc[2] = fmaf(v.z, x2, acc[2]);
+                    acc[3] = fmaf(v.w, x3, acc[3]);
+                }
+            } else if (active) {
                 const V* dp = a.data + (size_t)d0 * a.len + row0;
 #pragma unroll 4
                 for (int k = 0; k < nd; k++) {
@@ -104,7 +150,7 @@ __device__ __forceinline__ void dia_cta(const DiaArgsT<V>& a, int cta, int ncta,
                     const float4 v = ldv4(dp + (size_t)k * a.len, pe);
                     float x0, x1, x2, x3;
                     const int base = c & ~3;   // rows start at multiples of 4: c & 3 is the same for the whole CTA
-                    if (XA && base >= 0 && base + 7 < a.cols) {
+                    if (XF == 1 && base >= 0 && base + 7 < a.cols) {
                         // x[c .. c+3] from one or two aligned 128-bit loads
                         const float4 xa = ld_x4(a.x + base, pl);
                         switch (c & 3) {
@@ -794,6 +840,7 @@ __device__ __forceinline__ void b4csr_cta(const B4csrArgsT<V>& a, int cta, int n
         for (int h = 0; h < BH; h++) acc[h] = 0.f;
         if (active) {
             const int s = a.row_ptr[g], en = a.row_ptr[g + 1];
+#pragma unroll 2
             for (int i = s + l; i < en; i += T) {
                 const int c4 = ld_stream_i(a.col + i, pe);
                 const V* bi = a.data + (size_t)i * 4;

@@ -52,30 +52,31 @@ __global__ void __launch_bounds__(kBlock) k_scale(float* y, int n, float beta)
     if (i < n) y[i] = beta == 0.0f ? 0.0f : beta * y[i];
 }
 
-template <bool A, class V, bool XA>
+template <bool A, class V, int XF>
 __global__ void __launch_bounds__(kBlock) k_dia(DiaArgsT<V> a)
 {
     __shared__ __align__(16) char smem[kDiaSmemBytes];
-    dia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, smem);
+    dia_cta<A, V, XF>(a, blockIdx.x, gridDim.x, smem);
 }
 
 template <bool A, class V, bool XA>
 __global__ void __launch_bounds__(kBlock) k_bdia(BdiaArgsT<V> a) { bdia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, nullptr); }
 
 // the same, capped at the registers that keep 8 (DIA) / 5 (BDIA) CTAs of 256 threads per SM
-template <bool A, class V, bool XA>
+template <bool A, class V, int XF>
 __global__ void __launch_bounds__(kBlock, 8) k_dia_occ(DiaArgsT<V> a)
 {
     __shared__ __align__(16) char smem[kDiaSmemBytes];
-    dia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, smem);
+    dia_cta<A, V, XF>(a, blockIdx.x, gridDim.x, smem);
 }
 template <bool A, class V, bool XA>
 __global__ void __launch_bounds__(kBlock, 5) k_bdia_occ(BdiaArgsT<V> a) { bdia_cta<A, V, XA>(a, blockIdx.x, gridDim.x, nullptr); }
 
 // Kernel form of the diagonal formats: 0 scalar x loads, 1 aligned x
-// windows, 2 aligned x windows with the register cap. Measured on B200
-// (stencil27 128^3): DIA is fastest with form 0 (74.6 % of peak vs 60 / 72),
-// BDIA with form 1 (78 % vs 69 / 75). CLSPMV_DIA_FORM overrides both (for
+// windows, 2 aligned x windows with the register cap, 3 (DIA) one aligned
+// window per lane completed by shuffles. Measured on B200 (stencil27 128^3):
+// DIA is fastest with form 0 (74.6 % of peak vs 60 / 72 / 53), BDIA with
+// form 1 (78 % vs 69 / 75). CLSPMV_DIA_FORM overrides both (for
 // measurements).
 int dia_form(int dflt)
 {
@@ -242,13 +243,15 @@ int launch_dia_v(const clspmv_dia_f32* m, const V* data, const float* scale, con
     const int form = aligned16(x) ? dia_form(0) : 0;
     auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a); };
     if (atomic) {
-        if (form == 2) go(k_dia_occ<true, V, true>);
-        else if (form == 1) go(k_dia<true, V, true>);
-        else go(k_dia<true, V, false>);
+        if (form == 3) go(k_dia<true, V, 3>);
+        else if (form == 2) go(k_dia_occ<true, V, 1>);
+        else if (form == 1) go(k_dia<true, V, 1>);
+        else go(k_dia<true, V, 0>);
     } else {
-        if (form == 2) go(k_dia_occ<false, V, true>);
-        else if (form == 1) go(k_dia<false, V, true>);
-        else go(k_dia<false, V, false>);
+        if (form == 3) go(k_dia<false, V, 3>);
+        else if (form == 2) go(k_dia_occ<false, V, 1>);
+        else if (form == 1) go(k_dia<false, V, 1>);
+        else go(k_dia<false, V, 0>);
     }
     return after_launch(1);
 }
@@ -488,7 +491,13 @@ int launch_b4csr_v(const clspmv_b4csr_f32* m, const V* data, const float* scale,
     if ((long long)m->b4csr_row_num * m->b4csr_bheight < rows) return CLSPMV_ERR_ARG;
     const B4csrArgsT<V> a{rows, m->matinfo.width, m->b4csr_row_num, m->b4csr_aligned_size,
                           m->b4csr_row_ptr, m->b4csr_col_id, data, x, y, alpha, beta, scale};
-    const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num, 1, 32);
+    // lanes per block row: about one block per lane (measured best on B200 against 2 and 4;
+    // CLSPMV_BCSR_BPL overrides, for measurements)
+    static const int bpl = [] {
+        const char* e = getenv("CLSPMV_BCSR_BPL");
+        return e ? std::max(1, atoi(e)) : 1;
+    }();
+    const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num / bpl, 1, 32);
     return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
         return dispatch_lanes(lanes, [&](auto t) {
             constexpr int T = decltype(t)::value;
