@@ -613,7 +613,10 @@ def run_extras(args, items, mats, peak):
                       "mixed_k": W.serve(smats, budget, args.serving_requests, rate=20_000.0, k_lo=1, k_hi=32),
                       "k1": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1),
                       "k1_bf16": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1,
-                                         value_type="bf16")}
+                                         value_type="bf16"),
+                      # below the sequential capacity: latency without a queue
+                      "mixed_k_light": W.serve(smats, budget, max(100, args.serving_requests // 2), rate=200.0,
+                                               k_lo=1, k_hi=32)}
     del smats
     torch.cuda.empty_cache()
     out["serving"]["seconds"] = round(time.perf_counter() - t0, 1)

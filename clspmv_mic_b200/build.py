@@ -53,7 +53,8 @@ def build(verbose: bool = False) -> Path:
         objs = list(ex.map(lambda s: _compile(s, newest_header, verbose), sources))
     if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
         return LIB
-    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs)]
+    # --no-undefined: a missing definition fails the build instead of the first load
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-Xlinker", "--no-undefined", "-o", str(LIB), *map(str, objs)]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -553,12 +553,17 @@ int matrix_rows(const void* dev) { return static_cast<const clspmv_matinfo*>(dev
 
 // ---------------------------------------------------------------------------
 // Batches: many (matrix, X, Y) jobs in one persistent launch. Each job is cut
-// into warp tasks of 32 / G rows (G lanes per row for its k); the tasks of all
+// into warp tasks of 32 / G rows (G lanes per row for its k) -- or, for a CSR
+// job that adds into Y (beta 1), of 32 / G equal chunks of nonzeros, so that
+// rows of thousands of entries are shared between groups; the tasks of all
 // jobs form one index space that every warp strides through, finding its job
 // by binary search over the jobs' first task numbers.
 // ---------------------------------------------------------------------------
+constexpr int kBatchLongRow = 256;
+
 struct BatchJob {
     int format, value_type, k, lshift, vec, rows;
+    int chunk, nnz;            // CSR accumulating into Y (beta 1): nonzeros per lane group, else 0 (row mode)
     long long task_begin;
     int ldx, ldy;
     float alpha, beta;
@@ -603,6 +608,47 @@ __device__ __forceinline__ void batch_dispatch(const BatchJob& J, int r, int c0)
     }
 }
 
+// CSR job accumulating into Y: the group owns nonzeros [e0, e0 + chunk); rows
+// cut by the chunk's edges are added atomically, the others with a plain add
+// (as k_spmm_chunks, with Y already holding beta * Y = Y).
+template <int VEC, class T>
+__device__ __forceinline__ void batch_chunk(const BatchJob& J, int e0, int c0)
+{
+    const clspmv_csr_f32& m = J.m.csr;
+    const T* vals = static_cast<const T*>(J.values);
+    const int e1 = min(J.nnz, e0 + J.chunk);
+    int lo = 0, hi = J.rows;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(m.csr_row_ptr + mid) <= e0) lo = mid;
+        else hi = mid - 1;
+    }
+    int row = lo, row_end = __ldg(m.csr_row_ptr + row + 1);
+    bool first = true;
+    Acc<VEC> acc;
+    auto flush = [&](bool last) {
+        const float a = J.scale ? J.alpha * J.scale[row] : J.alpha;
+        float* y = J.Y + (size_t)row * J.ldy + c0;
+        bool cut = first && __ldg(m.csr_row_ptr + row) < e0;
+        if (last) cut = cut || row_end > e1;
+        if (cut) acc.atomic(y, a);
+        else acc.add(y, a);
+    };
+    for (int e = e0; e < e1; e++) {
+        if (e >= row_end) {
+            flush(false);
+            first = false;
+            acc = Acc<VEC>();
+            do {
+                row++;
+                row_end = __ldg(m.csr_row_ptr + row + 1);
+            } while (e >= row_end);
+        }
+        acc.fma(to_f(ld_val(vals + e)), J.X + (size_t)__ldg(m.csr_col_id + e) * J.ldx + c0);
+    }
+    flush(true);
+}
+
 __global__ void __launch_bounds__(kSpmmBlock) k_batch(const BatchJob* __restrict__ jobs, int njobs, long long tasks)
 {
     const int lane = threadIdx.x & 31;
@@ -617,6 +663,20 @@ __global__ void __launch_bounds__(kSpmmBlock) k_batch(const BatchJob* __restrict
         const BatchJob& J = jobs[lo];
         const long long r = (t - J.task_begin) * (32 >> J.lshift) + (lane >> J.lshift);
         const int c0 = (lane & ((1 << J.lshift) - 1)) * J.vec;
+        if (J.chunk > 0) {   // r counts chunks of nonzeros here
+            const long long e0 = r * J.chunk;
+            if (e0 >= J.nnz || c0 >= J.k) continue;
+            if (J.vec == 4) {
+                if (J.value_type == CLSPMV_VALUES_F32) batch_chunk<4, float>(J, (int)e0, c0);
+                else if (J.value_type == CLSPMV_VALUES_BF16) batch_chunk<4, __nv_bfloat16>(J, (int)e0, c0);
+                else batch_chunk<4, __half>(J, (int)e0, c0);
+            } else {
+                if (J.value_type == CLSPMV_VALUES_F32) batch_chunk<1, float>(J, (int)e0, c0);
+                else if (J.value_type == CLSPMV_VALUES_BF16) batch_chunk<1, __nv_bfloat16>(J, (int)e0, c0);
+                else batch_chunk<1, __half>(J, (int)e0, c0);
+            }
+            continue;
+        }
         if (r >= J.rows || c0 >= J.k) continue;
         if (J.vec == 4) {
             if (J.value_type == CLSPMV_VALUES_F32) batch_dispatch<4, float>(J, (int)r, c0);
@@ -681,6 +741,14 @@ int make_job(const clspmv_spmm_job& in, BatchJob& out)
     }
     if (in.value_type != CLSPMV_VALUES_F32) out.values = in.values;
     if (out.format == CLSPMV_FORMAT_CSR && !out.m.csr.csr_row_ptr) return CLSPMV_ERR_ARG;
+    // CSR adding into Y with long rows (mean >= kBatchLongRow entries): equal chunks of
+    // nonzeros, so long rows are shared between groups (shorter rows: one group per row
+    // is faster, measured on B200)
+    if (out.format == CLSPMV_FORMAT_CSR && in.beta == 1.0f && out.m.csr.matinfo.nnz > 0 &&
+        (long long)out.m.csr.matinfo.nnz >= (long long)kBatchLongRow * out.rows) {
+        out.chunk = in.k <= 4 ? 64 : 32;
+        out.nnz = out.m.csr.matinfo.nnz;
+    }
     return CLSPMV_OK;
 }
 
@@ -829,7 +897,8 @@ int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, cl
             return rc;
         }
         J.task_begin = tasks;
-        tasks += (J.rows + (32 >> J.lshift) - 1) / (32 >> J.lshift);
+        const long long units = J.chunk > 0 ? ((long long)J.nnz + J.chunk - 1) / J.chunk : J.rows;
+        tasks += (units + (32 >> J.lshift) - 1) / (32 >> J.lshift);
     }
     b->njobs = njobs;
     b->tasks = tasks;

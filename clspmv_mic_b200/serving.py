@@ -8,7 +8,10 @@ Y = alpha * A * X with any k; a loop thread forms batches continuously:
 * requests waiting when a slot frees up are grouped by matrix, and the X
   columns of one matrix's requests are placed side by side, so A is read
   once for all of them (up to 128 columns per job);
-* all jobs of the batch run in ONE persistent launch (clspmv_batch_run);
+* all fused jobs of the batch run in ONE persistent launch
+  (clspmv_batch_run); a request that is alone for its matrix runs in that
+  format's own load-balanced kernel on the same stream, so a lightly loaded
+  server answers as fast as a plain launch;
 * `slots` batches can be in flight at once on separate streams, so requests
   that arrive while a batch runs are admitted into the next slot and their
   work overlaps the running batch on the device.
@@ -206,18 +209,25 @@ class SpmvServer:
                         Xc = torch.cat([r.X * r.alpha for r in part], dim=1)
                     if Xc.shape[1] % 4 and Xc.shape[1] > 32:
                         Xc = torch.nn.functional.pad(Xc, (0, 4 - Xc.shape[1] % 4))
-                    Yc = torch.empty((m, Xc.shape[1]), dtype=torch.float32, device=Xc.device)
-                    jobs.append(Job(res.matrix, Xc, Yc, alpha=part[0].alpha if same_alpha else 1.0, beta=0.0,
-                                    packed=res.packed))
+                    alpha = part[0].alpha if same_alpha else 1.0
+                    if len(part) == 1 or res.matrix.fmt == "coo":
+                        # nothing to fuse: the format's own balanced kernel, on this slot's stream
+                        Yc = torch.empty((m, Xc.shape[1]), dtype=torch.float32, device=Xc.device)
+                        res.matrix.spmm(Xc, Yc, alpha, 0.0, packed=res.packed, stream=st)
+                    else:
+                        # Y += A X on a zeroed Y: CSR jobs with long rows are then split between warps
+                        Yc = torch.zeros((m, Xc.shape[1]), dtype=torch.float32, device=Xc.device)
+                        jobs.append(Job(res.matrix, Xc, Yc, alpha=alpha, beta=1.0, packed=res.packed))
                     off = 0
                     for r in part:
                         k = r.X.shape[1]
                         outputs.append(Yc[:, off:off + k])
                         order.append(r)
                         off += k
-            b = self._batches[slot]
-            b.set(jobs, st)
-            b.run(st)
+            if jobs:
+                b = self._batches[slot]
+                b.set(jobs, st)
+                b.run(st)
             ev = torch.cuda.Event()
             ev.record(st)
         self._flights[slot] = _Flight(ev, order, outputs)

@@ -159,7 +159,8 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
         Xs = [torch.rand((m.shape[1], k), generator=gen, device="cuda") * 2 - 1 for _, m in mats]
         Ys = [torch.empty((m.shape[0], k), device="cuda") for _, m in mats]
         for vt in value_types:
-            jobs = [Job(m, X, Y, 1.0, 0.0, packed=p) for (_, m), X, Y, p in zip(mats, Xs, Ys, packs[vt])]
+            # Y += A X (beta 1): CSR jobs are cut by nonzeros; Y is zeroed before the checked run
+            jobs = [Job(m, X, Y, 1.0, 1.0, packed=p) for (_, m), X, Y, p in zip(mats, Xs, Ys, packs[vt])]
             b = Batch(len(jobs))
             s.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(s):
@@ -179,6 +180,10 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
             e1.record()
             torch.cuda.synchronize()
             t_batch = e0.elapsed_time(e1) / reps
+            for Y in Ys:
+                Y.zero_()
+            g.replay()
+            torch.cuda.synchronize()
             err = max(fp64_error(a, X, Y) for a, X, Y in zip(A64, Xs, Ys))
             # the same jobs, one plain clspmv_spmm launch each
             for j in jobs:
@@ -216,6 +221,14 @@ def serving_matrices(count: int = 64, rows_lo: int = 10_000, rows_hi: int = 4_00
     return out
 
 
+def _wait_until(t: float) -> None:
+    """Sleep until perf_counter() reaches t. Sleeping (not spinning) leaves
+    the interpreter lock to the serving loop's thread."""
+    dt = t - time.perf_counter()
+    if dt > 0:
+        time.sleep(dt)
+
+
 def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.0, k_lo: int = 1, k_hi: int = 32,
           value_type: str = "f32", seed: int = 3, slots: int = 2):
     """Open-loop Poisson stream of `n_requests` at `rate` req/s, k uniform in
@@ -245,8 +258,7 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
     lat_seq = []
     t0 = time.perf_counter()
     for i in range(n_requests):
-        while time.perf_counter() - t0 < arrivals[i]:
-            pass
+        _wait_until(t0 + arrivals[i])
         res = srv.mats[names[pick[i]]]
         Y = torch.empty((res.matrix.shape[0], int(ks[i])), device="cuda")
         res.matrix.spmm(Xs[i], Y, 1.0, 0.0, packed=res.packed)
@@ -265,8 +277,7 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
     def client():
         t_start = time.perf_counter()
         for i in range(n_requests):
-            while time.perf_counter() - t_start < arrivals[i]:
-                pass
+            _wait_until(t_start + arrivals[i])
             futures[i] = srv.submit(names[pick[i]], Xs[i], keep_result=False)
 
     th = threading.Thread(target=client)

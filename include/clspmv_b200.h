@@ -445,7 +445,11 @@ typedef struct {
 
 /* A batch runs many jobs (different matrices, formats, value types and k)
  * in ONE persistent kernel launch: the rows of all jobs are cut into warp
- * tasks that every warp of a device-filling grid strides through. */
+ * tasks that every warp of a device-filling grid strides through. A CSR job
+ * with beta == 1 (Y += alpha * A * X) whose rows hold 256 entries or more on
+ * average is cut by nonzeros instead of rows, so very long rows do not
+ * serialise one warp; for such matrices prefer beta == 1 (zero Y first for a
+ * plain product). */
 typedef struct clspmv_batch clspmv_batch;
 
 /* Allocates the device job table for up to max_jobs jobs (and a pinned

@@ -143,3 +143,32 @@ def test_server_mixed_requests_match_alone():
         tol = 1e-5 * np.abs(ref).max() + 1e-6
         assert np.max(np.abs(got - ref)) <= tol, (key, dev.fmt)
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+
+
+def test_batch_csr_accumulate_splits_rows():
+    """CSR jobs with beta 1 and long rows are cut by nonzeros (rows shared
+    between warps), others by rows: Y0 + alpha A X agrees with the
+    single-matrix SpMM."""
+    import torch
+    rng = np.random.default_rng(21)
+    jobs, expect = [], []
+    from clspmv_mic_b200 import synth
+    long_rows = F.coo_matrix(*synth.random_coo(500, 4000, 0.1, seed=8, empty_row_frac=0.1))   # ~400 per row
+    for name in ["long_rows", "powerlaw3k", "long_rows", "laplace33"]:
+        dev = F.DeviceMatrix(F.coo2csr(long_rows)) if name == "long_rows" else _device(name, "csr", ())
+        for k, vt in [(1, "f32"), (6, "bf16"), (16, "f32"), (36, "f16")]:
+            packed = None if vt == "f32" else dev.pack(vt)
+            X = torch.from_numpy(rng.uniform(-1, 1, (dev.shape[1], k)).astype(np.float32)).cuda()
+            Y0 = torch.from_numpy(rng.uniform(-1, 1, (dev.shape[0], k)).astype(np.float32)).cuda()
+            ref = Y0.clone()
+            dev.spmm(X, ref, 0.75, 1.0, packed=packed)
+            jobs.append(Job(dev, X, Y0, alpha=0.75, beta=1.0, packed=packed))
+            expect.append(ref)
+    b = Batch(len(jobs))
+    b.set(jobs)
+    b.run()
+    torch.cuda.synchronize()
+    for j, ref in zip(jobs, expect):
+        got, r = j.Y.cpu().numpy(), ref.cpu().numpy()
+        assert np.max(np.abs(got - r)) <= 1e-5 * (np.abs(r).max() + 1.0), j.matrix.shape
+    b.close()
