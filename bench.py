@@ -81,9 +81,9 @@ def split_hyb(coo_arrays, k):
     return (h, w, r[head], c[head], v[head]), (h, w, r[~head], c[~head], v[~head])
 
 
-VARIANT_KEYS = {"csr_vector", "csr_scalar"}
+VARIANT_KEYS = {"csr_vector", "csr_scalar", "sell32_planned"}
 FORMAT_KEYS = {"stencil27": ["dia", "bdia"],
-               "powerlaw": ["csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32"],
+               "powerlaw": ["csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32", "sell32_planned"],
                "blocks4x4": ["bell", "sbell", "bcsr"]}
 
 
@@ -131,7 +131,9 @@ def build_workload(small: bool, only=None):
             ell_part, coo_tail = split_hyb(pl, k)
             add("ell", "powerlaw", lambda: F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell")
             add("ell_tail_coo", "powerlaw", lambda: F.coo_matrix(*coo_tail), part_of="ell")
-        add("sell32", "powerlaw", lambda: F.coo2sell(coo, 32))
+        sell = F.coo2sell(coo, 32) if ("sell32" in want or "sell32_planned" in want) else None
+        add("sell32", "powerlaw", lambda: sell)                                     # every stored slot
+        add("sell32_planned", "powerlaw", lambda: sell, {"variant": "planned"})    # real entries only (length plan)
     if "blocks4x4" in mats:
         coo = F.coo_matrix(*mats["blocks4x4"])
         add("bell", "blocks4x4", lambda: F.coo2b4ell(coo, 4, 4))
@@ -142,7 +144,11 @@ def build_workload(small: bool, only=None):
 
 def algorithmic_bytes(it) -> int:
     """Arrays the kernel must stream (values, indices, pointers, padding),
-    plus x read once and y read and written once."""
+    plus x read once and y read and written once. SELL with its length plan
+    reads each row only up to its last real entry: those entries, the row
+    lengths, the tail items and the slice pointers."""
+    if it.get("needed") is not None:
+        return int(it["needed"] + 4 * it["cols"] + 8 * it["rows"])
     return int(it["stored"] + 4 * it["cols"] + 8 * it["rows"])
 
 
@@ -367,6 +373,11 @@ def run_ours(args):
         ys[it["key"]] = torch.zeros(it["rows"], dtype=torch.float32, device=dev)
         if it["host"].fmt == "csr" and it["kw"].get("variant") == "merge":
             it["dev"].merge_plan(stream)
+        if it["host"].fmt == "sell" and it["kw"].get("variant") == "planned":
+            d = it["dev"]
+            n_items = int(F.lib().clspmv_sell_plan_items(d.sell_plan()))
+            it["needed"] = (8 * d.sell_plan_entries() + 4 * it["rows"] + 8 * n_items
+                            + 4 * (it["host"].struct.sell_slice_num + 1))
         it.pop("host")
     torch.cuda.synchronize()
 

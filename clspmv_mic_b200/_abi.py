@@ -239,6 +239,11 @@ def _declare(lib):
         "clspmv_spmm": (I32, [I32, VP, I32, VP, VP, I32, VP, I32, VP, I32, f32, f32, VP]),
         "clspmv_stored_values": (I32, [I32, VP, P(C.c_size_t)]),
         "clspmv_spmv_packed": (I32, [I32, VP, I32, VP, VP, VP, VP, VP, f32, f32, VP]),
+        "clspmv_sell_plan_create": (I32, [S["sell"], P(VP)]),
+        "clspmv_sell_plan_spmv_f32": (I32, [S["sell"], VP, VP, VP, f32, f32, VP]),
+        "clspmv_sell_plan_entries": (C.c_longlong, [VP]),
+        "clspmv_sell_plan_items": (C.c_longlong, [VP]),
+        "clspmv_sell_plan_free": (I32, [VP]),
         "clspmv_pack_values": (I32, [I32, VP, I32, VP, VP, VP]),
         "clspmv_batch_create": (I32, [I32, P(VP)]),
         "clspmv_batch_set": (I32, [VP, P(SpmmJob), I32, VP, P(I32)]),

@@ -393,6 +393,82 @@ __device__ __forceinline__ void sell_rows4_cta(const SellArgsT<V>& a, int cta, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// SELL without its padding. The converter pads every row of a slice to the
+// slice's widest row with the row's previous column id and value 0
+// (include/matrix_storage.h:1466-1491): a slot whose column equals the slot
+// before it and whose value is 0 adds nothing, and a row's trailing run of
+// such slots is padding. sell_row_length finds where a row's real entries end
+// (once per matrix). sell_head_cta then sums each row's first kSellHead
+// entries with one thread per row (consecutive rows of a slice are adjacent,
+// so a warp's loads are coalesced) and writes y; sell_tail_cta adds the rest
+// of the long rows, a warp per item of up to kSellTailCols entries of one
+// row, with red.global.add. A slice as wide as one power-law row then costs
+// that row's entries instead of slice_height times them.
+// ---------------------------------------------------------------------------
+constexpr int kSellHead = 32;
+constexpr int kSellTailCols = 256;
+
+__device__ __forceinline__ int sell_row_length(const int* slice_ptr, const int* col, const float* data, int sh, long long row)
+{
+    const int s = (int)(row / sh), lr = (int)(row - (long long)s * sh);
+    const int start = slice_ptr[s];
+    int k = (slice_ptr[s + 1] - start) / sh;
+    while (k > 1) {
+        const size_t i = (size_t)start + (size_t)(k - 1) * sh + lr;
+        if (col[i] != col[i - sh] || data[i] != 0.0f) break;
+        k--;
+    }
+    return k;
+}
+
+template <bool ATOMIC>
+__device__ __forceinline__ void sell_head_cta(const SellArgs& a, const int* __restrict__ rlen, int cta, int ncta)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    long long b, e;
+    cta_share(a.rows, 32, cta, ncta, b, e);
+    const int sh = a.slice_height;
+    for (long long row = b + threadIdx.x; row < e; row += kBlock) {
+        const int s = (int)(row / sh), lr = (int)(row - (long long)s * sh);
+        const size_t base = (size_t)__ldg(a.slice_ptr + s) + lr;
+        const int n = min(__ldg(rlen + row), kSellHead);
+        float acc = 0.f;
+#pragma unroll 4
+        for (int k = 0; k < n; k++) {
+            const size_t i = base + (size_t)k * sh;
+            acc = fmaf(ld_stream_f(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
+        }
+        y_update<ATOMIC>(a.y, row, a.alpha, a.beta, acc);
+    }
+}
+
+// items: (row, first entry) pairs, first entry >= kSellHead; y already holds
+// the row's head sum.
+__device__ __forceinline__ void sell_tail_cta(const SellArgs& a, const int* __restrict__ rlen, const int2* __restrict__ items,
+                                              long long nitems, int cta, int ncta)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)ncta * (kBlock / 32);
+    const int sh = a.slice_height;
+    for (long long it = (long long)cta * (kBlock / 32) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+        const int2 item = __ldg(items + it);
+        const int s = item.x / sh, lr = item.x - s * sh;
+        const size_t base = (size_t)__ldg(a.slice_ptr + s) + lr;
+        const int k1 = min(item.y + kSellTailCols, __ldg(rlen + item.x));
+        float acc = 0.f;
+#pragma unroll 4
+        for (int k = item.y + lane; k < k1; k += 32) {
+            const size_t i = base + (size_t)k * sh;
+            acc = fmaf(ld_stream_f(a.data + i, pe), ld_x(a.x + ld_stream_i(a.col + i, pe), pl), acc);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
+        if (lane == 0) atomicAdd(a.y + item.x, a.alpha * acc);
+    }
+}
+
 // Other slice heights: one row per thread, slice by slice.
 template <bool ATOMIC, class V>
 __device__ __forceinline__ void sell_rows_cta(const SellArgsT<V>& a, int cta, int ncta, char*)

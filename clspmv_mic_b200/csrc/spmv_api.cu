@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <mutex>
 #include <unordered_map>
+#include <vector>
+#include <new>
 #include "clspmv_b200.h"
 #include "kernels.cuh"
 #include "api_internal.h"
@@ -98,6 +100,25 @@ __global__ void __launch_bounds__(kBlock) k_sell_rows(SellArgsT<V> a) { sell_row
 
 template <bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_sell_rows4(SellArgsT<V> a) { sell_rows4_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+
+__global__ void __launch_bounds__(kBlock) k_sell_rlen(const int* __restrict__ slice_ptr, const int* __restrict__ col,
+                                                      const float* __restrict__ data, int sh, long long rows, int* rlen)
+{
+    for (long long r = blockIdx.x * (long long)kBlock + threadIdx.x; r < rows; r += (long long)gridDim.x * kBlock)
+        rlen[r] = sell_row_length(slice_ptr, col, data, sh, r);
+}
+
+template <bool A>
+__global__ void __launch_bounds__(kBlock) k_sell_head(SellArgs a, const int* __restrict__ rlen)
+{
+    sell_head_cta<A>(a, rlen, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(kBlock) k_sell_tail(SellArgs a, const int* __restrict__ rlen, const int2* __restrict__ items,
+                                                      long long nitems)
+{
+    sell_tail_cta(a, rlen, items, nitems, blockIdx.x, gridDim.x);
+}
 
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
@@ -351,6 +372,24 @@ int launch_sell_v(const clspmv_sell_f32* m, const V* data, const float* scale, c
 int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
 {
     return launch_sell_v<float>(m, m ? m->sell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
+}
+
+// Padding-free SELL: heads (plain y update, or atomic), then the long rows' tails (atomic).
+int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* items, long long nitems, const float* x,
+                        float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !x || !y || !m->sell_slice_ptr || !rlen || (nitems > 0 && !items)) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (m->sell_slice_height == 0) return CLSPMV_ERR_ARG;
+    SellArgs a{rows, (int)m->sell_slice_height, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data,
+               x, y, alpha, beta, nullptr};
+    if (atomic) k_sell_head<true><<<persistent_grid(k_sell_head<true>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
+    else k_sell_head<false><<<persistent_grid(k_sell_head<false>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
+    int rc = after_launch(1);
+    if (rc || nitems == 0) return rc;
+    k_sell_tail<<<persistent_grid(k_sell_tail, nitems, kBlock / 32), kBlock, 0, st>>>(a, rlen, items, nitems);
+    return after_launch(1);
 }
 
 int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
@@ -615,6 +654,66 @@ int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float
 { return launch_ell(m, x, y, alpha, beta, S(s), false); }
 int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_sell(m, x, y, alpha, beta, S(s), false); }
+struct clspmv_sell_plan {
+    int* rlen = nullptr;       // device: stored length of every row (padding excluded)
+    int2* items = nullptr;     // device: (row, first entry) of each tail item
+    long long rows = 0, nitems = 0, entries = 0;
+};
+
+int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
+{
+    if (!m || !out || !m->sell_slice_ptr || m->sell_slice_height == 0) return CLSPMV_ERR_ARG;
+    *out = nullptr;
+    clspmv_sell_plan* p = new (std::nothrow) clspmv_sell_plan();
+    if (!p) return CLSPMV_ERR_ALLOC;
+    const long long rows = std::max(0, m->matinfo.height);
+    p->rows = rows;
+    std::vector<int> rlen((size_t)rows);
+    std::vector<int2> items;
+    int rc = cuda_status(cudaMalloc(&p->rlen, sizeof(int) * (size_t)std::max(1LL, rows)));
+    if (!rc && rows) {
+        k_sell_rlen<<<(unsigned)std::min<long long>((rows + kBlock - 1) / kBlock, 148LL * 32), kBlock>>>(
+            m->sell_slice_ptr, m->sell_col_id, m->sell_data, (int)m->sell_slice_height, rows, p->rlen);
+        rc = after_launch(1);
+        if (!rc) rc = cuda_status(cudaMemcpy(rlen.data(), p->rlen, sizeof(int) * rows, cudaMemcpyDeviceToHost));
+    }
+    if (!rc) {
+        for (long long r = 0; r < rows; r++) {
+            p->entries += rlen[r];
+            for (int k = kSellHead; k < rlen[r]; k += kSellTailCols) items.push_back(make_int2((int)r, k));
+        }
+        p->nitems = (long long)items.size();
+        rc = cuda_status(cudaMalloc(&p->items, sizeof(int2) * std::max<size_t>(1, items.size())));
+        if (!rc && !items.empty())
+            rc = cuda_status(cudaMemcpy(p->items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+    }
+    if (rc) {
+        clspmv_sell_plan_free(p);
+        return rc;
+    }
+    *out = p;
+    return CLSPMV_OK;
+}
+
+int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* p, const float* x, float* y, float alpha,
+                              float beta, clspmv_stream_t s)
+{
+    if (!p) return CLSPMV_ERR_ARG;
+    return launch_sell_planned(m, p->rlen, p->items, p->nitems, x, y, alpha, beta, S(s), false);
+}
+
+long long clspmv_sell_plan_entries(const clspmv_sell_plan* p) { return p ? p->entries : -1; }
+long long clspmv_sell_plan_items(const clspmv_sell_plan* p) { return p ? p->nitems : -1; }
+
+int clspmv_sell_plan_free(clspmv_sell_plan* p)
+{
+    if (!p) return CLSPMV_ERR_ARG;
+    if (p->rlen) cudaFree(p->rlen);
+    if (p->items) cudaFree(p->items);
+    delete p;
+    return CLSPMV_OK;
+}
+
 int clspmv_csr_scalar_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_csr_scalar(m, x, y, alpha, beta, S(s), false); }
 int clspmv_csr_vector_spmv_f32(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, clspmv_stream_t s)

@@ -272,6 +272,28 @@ class DeviceMatrix:
         self._plan = None
         return self
 
+    def sell_plan(self):
+        """Row lengths and tail items of a SELL matrix for the padding-free
+        SpMV (clspmv_sell_plan_create, made once)."""
+        if getattr(self, "_sell_plan", None) is None:
+            h = C.c_void_p()
+            check(lib().clspmv_sell_plan_create(C.byref(self.struct), C.byref(h)), "sell_plan_create")
+            self._sell_plan = h
+        return self._sell_plan
+
+    def sell_plan_entries(self) -> int:
+        """Stored entries the padding-free SELL SpMV reads."""
+        return int(lib().clspmv_sell_plan_entries(self.sell_plan()))
+
+    def __del__(self):
+        p = getattr(self, "_sell_plan", None)
+        if p:
+            try:
+                lib().clspmv_sell_plan_free(p)
+            except Exception:
+                pass
+            self._sell_plan = None
+
     def merge_plan(self, stream=None):
         """Tile coordinates for the merge-path CSR kernel (computed once)."""
         import torch
@@ -285,7 +307,11 @@ class DeviceMatrix:
     def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None, variant: str = "merge",
              threads_per_row: int = 0, packed: "PackedValues | None" = None) -> None:
         """y <- alpha * A x + beta * y on the device (asynchronous on `stream`);
-        with `packed`, from the 16-bit values of self.pack()."""
+        with `packed`, from the 16-bit values of self.pack(). `variant`: CSR
+        "merge" (default), "vector" or "scalar"; SELL "planned" reads only each
+        row's real entries (its length plan), which on B200 is slower than the
+        padded read for power-law slices: the tails of long rows are strided
+        column-major reads."""
         L = lib()
         s = _stream_handle(stream)
         if packed is not None:
@@ -307,6 +333,10 @@ class DeviceMatrix:
                       "csr_scalar_spmv")
             else:
                 raise ValueError(variant)
+            return
+        if self.fmt == "sell" and variant == "planned":
+            check(L.clspmv_sell_plan_spmv_f32(C.byref(self.struct), self.sell_plan(), x.data_ptr(), y.data_ptr(),
+                                              alpha, beta, s), "sell_plan_spmv")
             return
         name = _SPMV[self.fmt]
         check(getattr(L, name)(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s), name)

@@ -355,6 +355,32 @@ int clspmv_ell_spmv_f32(const clspmv_ell_f32* dev, const float* x, float* y,
 int clspmv_sell_spmv_f32(const clspmv_sell_f32* dev, const float* x, float* y,
                          float alpha, float beta, clspmv_stream_t stream);
 
+/* SELL without reading its padding. The converter pads each row of a slice
+ * to the slice's widest row with the row's previous column id and value 0
+ * (include/matrix_storage.h:1466-1491), so a slot equal to its predecessor's
+ * column with value 0 adds nothing and a row's trailing run of such slots is
+ * padding. clspmv_sell_plan_create finds where every row's real entries end
+ * and lists the long rows' tails (synchronous, once per matrix; it allocates
+ * device memory, released with clspmv_sell_plan_free). The planned SpMV sums
+ * each row's first 32 entries with a thread per row and the tails of longer
+ * rows with a warp per 256 entries, so a slice as wide as one power-law row
+ * costs that row's entries, not slice_height times them. Any slice height.
+ * Measured on B200 it is slower than clspmv_sell_spmv_f32 for power-law
+ * slices (a long row's tail is a strided, column-major read: one 32-byte
+ * sector per 4-byte entry in each array), so the padded read stays the
+ * default everywhere in this library.
+ * Same y as clspmv_sell_spmv_f32 up to summation order, except where x
+ * holds Inf or NaN at a skipped padding column. No counterpart in the
+ * reference. */
+typedef struct clspmv_sell_plan clspmv_sell_plan;
+int clspmv_sell_plan_create(const clspmv_sell_f32* dev, clspmv_sell_plan** out);
+int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* dev, const clspmv_sell_plan* plan, const float* x, float* y,
+                              float alpha, float beta, clspmv_stream_t stream);
+/* stored entries the plan reads (real entries and explicit zeros before them), and its tail items */
+long long clspmv_sell_plan_entries(const clspmv_sell_plan* plan);
+long long clspmv_sell_plan_items(const clspmv_sell_plan* plan);
+int clspmv_sell_plan_free(clspmv_sell_plan* plan);
+
 /* BELL = b4ell, block shapes {1,2,4,8} x {4,8}. Replaces the 32 kernels of
  * kernels/spmv_bell.cl, driver src/spmv_bell.cpp:345-399. */
 int clspmv_b4ell_spmv_f32(const clspmv_b4ell_f32* dev, const float* x, float* y,

@@ -146,3 +146,35 @@ def test_launch_counter_moves():
     coo = coo_of("laplace16")
     run_device(F.coo2csr(coo), synth.x_vector(coo.shape[1]), np.zeros(coo.shape[0], np.float32), variant="merge")
     assert F.launch_count() >= before + 2   # plan + spmv
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sh", [4, 20, 32, 128])
+@pytest.mark.parametrize("name", ["powerlaw3k", "random_empty_rows", "explicit_zeros", "one_entry"])
+def test_sell_planned_matches_padded(name, sh):
+    """SELL read only up to each row's last real entry (heads per thread,
+    long tails per warp) equals the padded read and the oracle, with
+    explicit zero values inside and at the end of rows and empty rows."""
+    if name == "explicit_zeros":
+        rng = np.random.default_rng(12)
+        h = 301
+        lens = rng.integers(0, 120, h)
+        lens[::7] = 0
+        rows = np.repeat(np.arange(h), lens)
+        cols = np.concatenate([np.sort(rng.choice(900, l, replace=False)) for l in lens])
+        vals = rng.standard_normal(rows.size).astype(np.float32)
+        vals[::5] = 0.0
+        coo = F.coo_matrix(h, 900, rows, cols, vals)
+    else:
+        coo = coo_of(name)
+    m, n = coo.shape
+    x = synth.x_vector(n, seed=4) * 1e3
+    y0 = np.random.default_rng(1).uniform(-1, 1, m).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (0.5, -1.5)]:
+        ref, _, bound = reference_y(coo, x, y0, alpha, beta)
+        for variant in ("planned", "padded"):
+            y = run_device(F.coo2sell(coo, sh), x, y0, alpha, beta, variant=variant)
+            assert_close(y, ref, bound, f"sell{sh} {variant}")
+    dev = F.DeviceMatrix(F.coo2sell(coo, sh))
+    host = F.coo2sell(coo, sh)                   # kept alive while its array is read
+    assert coo.nnz <= dev.sell_plan_entries() <= int(host.array("sell_slice_ptr")[-1])
