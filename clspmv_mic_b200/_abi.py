@@ -257,6 +257,17 @@ def _declare(lib):
     for fmt in ("coo", "csr", "dia", "bdia", "ell", "sell", "b4csr", "b4ell", "sbell"):
         sigs[f"clspmv_upload_{fmt}_f32"] = (I32, [S[fmt], S[fmt]])
         sigs[f"clspmv_device_free_{fmt}_f32"] = (I32, [S[fmt]])
+    sigs.update({
+        "clspmv_device_sort_coo_f32": (I32, [S["coo"], VP]),
+        "clspmv_device_coo2csr_f32": (I32, [S["coo"], S["csr"], VP]),
+        "clspmv_device_coo2dia_f32": (I32, [S["coo"], S["dia"], I32, VP]),
+        "clspmv_device_coo2bdia_f32": (I32, [S["coo"], S["bdia"], I32, VP]),
+        "clspmv_device_coo2ell_f32": (I32, [S["coo"], S["ell"], I32, I32, VP]),
+        "clspmv_device_coo2sell_f32": (I32, [S["coo"], S["sell"], U32, VP]),
+        "clspmv_device_coo2b4csr_f32": (I32, [S["coo"], S["b4csr"], U32, U32, I32, VP]),
+        "clspmv_device_coo2b4ell_f32": (I32, [S["coo"], S["b4ell"], U32, U32, I32, I32, VP]),
+        "clspmv_device_coo2sbell_f32": (I32, [S["coo"], S["sbell"], U32, U32, U32, VP]),
+    })
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
         fn.restype = res

@@ -351,6 +351,106 @@ class DeviceMatrix:
         device_spmm(self, X, Y, alpha, beta, packed, stream)
 
 
+class _DeviceArrays:
+    """Arrays a device converter cudaMalloc'ed, released with
+    clspmv_device_free_<fmt>_f32 when the last tensor viewing them is gone."""
+
+    def __init__(self, fmt: str, struct):
+        self.fmt = fmt
+        self.struct = struct
+
+    def __del__(self):
+        try:
+            getattr(lib(), f"clspmv_device_free_{self.fmt}_f32")(C.byref(self.struct))
+        except Exception:
+            pass
+
+
+class _CudaView:
+    """__cuda_array_interface__ of one converter-owned array; keeps the owner alive."""
+
+    def __init__(self, owner: _DeviceArrays, ptr: int, count: int, dt):
+        self._owner = owner
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4" if dt == np.int32 else "<f4",
+                                         "data": (ptr, False), "version": 3, "strides": None}
+
+
+# format -> (C entry point, default trailing arguments after the required ones)
+_DEVICE_CONVERT = {
+    "csr": ("clspmv_device_coo2csr_f32", 0, ()),
+    "dia": ("clspmv_device_coo2dia_f32", 0, (GPU_ALIGNMENT,)),
+    "bdia": ("clspmv_device_coo2bdia_f32", 0, (GPU_ALIGNMENT,)),
+    "ell": ("clspmv_device_coo2ell_f32", 0, (GPU_ALIGNMENT, 0)),
+    "sell": ("clspmv_device_coo2sell_f32", 0, (WARPSIZE,)),
+    "b4csr": ("clspmv_device_coo2b4csr_f32", 2, (GPU_ALIGNMENT,)),
+    "b4ell": ("clspmv_device_coo2b4ell_f32", 2, (GPU_ALIGNMENT, 0)),
+    "sbell": ("clspmv_device_coo2sbell_f32", 2, (WARPSIZE,)),
+}
+
+
+def device_convert_raw(coo: DeviceMatrix, fmt: str, *args, stream=None):
+    """(status, struct) of clspmv_device_coo2<fmt>_f32 on a device COO; the
+    arguments after the format are those of the host coo2<fmt> (bwidth,
+    bheight first for the block formats; the rest default as there)."""
+    if coo.fmt != "coo":
+        raise ValueError("device conversion starts from a device COO")
+    name, required, defaults = _DEVICE_CONVERT[fmt]
+    if len(args) < required:
+        raise TypeError(f"device coo2{fmt} needs {required} leading arguments")
+    full = tuple(args) + defaults[len(args) - required:]
+    out = FORMATS[fmt][0]()
+    status = getattr(lib(), name)(C.byref(coo.struct), C.byref(out), *full, _stream_handle(stream))
+    return status, out
+
+
+def device_convert(coo: DeviceMatrix, fmt: str, *args, stream=None) -> DeviceMatrix:
+    """coo2<fmt> on the device: a DeviceMatrix equal array for array to
+    DeviceMatrix(coo2<fmt>(host COO, *args)), converted where the COO already
+    is (clspmv_device_coo2<fmt>_f32). Raises ClspmvError with the host
+    converter's status where it would refuse or reject the input."""
+    import torch
+    status, out = device_convert_raw(coo, fmt, *args, stream=stream)
+    check(status, f"device_coo2{fmt}")
+    owner = _DeviceArrays(fmt, out)
+    dev = coo.tensors["coo_row_id"].device
+    self = DeviceMatrix.__new__(DeviceMatrix)
+    self.fmt, self.struct, self.tensors, self._plan = fmt, out, {}, None
+    total = None   # slots of a sliced format: its last slice pointer, read from the device
+    for field, dt, n in FORMATS[fmt][1]:
+        if field.endswith("_slice_ptr"):
+            ns = out.sell_slice_num if fmt == "sell" else out.sbell_slice_num
+            count = ns + 1
+        elif fmt in ("sell", "sbell") and field.endswith("_col_id"):
+            count = total
+        elif fmt == "sell" and field == "sell_data":
+            count = total
+        elif fmt == "sbell" and field == "sbell_data":
+            count = total * out.sbell_bwidth * out.sbell_bheight
+        elif field == "bdia_data":
+            ndiag = int(self.tensors["bdia_bptr"][-1].item()) if out.bdia_band_num > 0 else 0
+            count = ndiag * out.bdia_length_aligned
+        else:
+            count = int(n(out))
+        if count > 0:
+            t = torch.as_tensor(_CudaView(owner, getattr(out, field), count, dt), device=dev)
+        else:
+            t = torch.empty(0, dtype=_torch_dtype(dt), device=dev)
+        if field.endswith("_slice_ptr"):
+            total = int(t[-1].item())
+        self.tensors[field] = t
+    self.shape = (out.matinfo.height, out.matinfo.width)
+    self.nnz = out.matinfo.nnz
+    self.stored_bytes = int(sum(t.numel() * t.element_size() for t in self.tensors.values()))
+    self._owner = owner
+    return self
+
+
+def device_sort_coo(coo: DeviceMatrix, stream=None) -> DeviceMatrix:
+    """Stable in-place sort of a device COO by (row, col) (clspmv_device_sort_coo_f32)."""
+    check(lib().clspmv_device_sort_coo_f32(C.byref(coo.struct), _stream_handle(stream)), "device_sort_coo")
+    return coo
+
+
 class PackedValues:
     """16-bit copy of a device matrix's values with per-row power-of-two
     scales (clspmv_pack_values); indices stay those of the FP32 matrix."""

@@ -277,6 +277,41 @@ int clspmv_device_free_b4ell_f32(clspmv_b4ell_f32* dev);
 int clspmv_device_free_sbell_f32(clspmv_sbell_f32* dev);
 
 /* ------------------------------------------------------------------------ */
+/* Converters on the device. `coo` holds device arrays; the output struct   */
+/* gets cudaMalloc'ed device arrays (release with clspmv_device_free_<fmt>) */
+/* equal byte for byte to what the host converter of the same name without  */
+/* `device_` makes from the same COO, with the same statuses (argument      */
+/* checks, CLSPMV_ERR_NOT_SORTED, refusals). The COO is not modified. Each  */
+/* call synchronises `stream`. They replace the host-side conversion the    */
+/* reference does before every upload (include/matrix_storage.h:936-2409);  */
+/* the reference has no device converter.                                   */
+/* ------------------------------------------------------------------------ */
+/* Stable sort of a device COO by (row, col), in place (sort_coo,
+ * include/matrix_storage.h:744-815). */
+int clspmv_device_sort_coo_f32(clspmv_coo_f32* coo, clspmv_stream_t stream);
+/* coo2csr (include/matrix_storage.h:1268-1307). */
+int clspmv_device_coo2csr_f32(const clspmv_coo_f32* coo, clspmv_csr_f32* dev, clspmv_stream_t stream);
+/* coo2dia (:936-1014); any COO order, the last of a repeated (row, col) wins. */
+int clspmv_device_coo2dia_f32(const clspmv_coo_f32* coo, clspmv_dia_f32* dev, int alignment, clspmv_stream_t stream);
+/* coo2bdia (:1184-1236). */
+int clspmv_device_coo2bdia_f32(const clspmv_coo_f32* coo, clspmv_bdia_f32* dev, int alignment, clspmv_stream_t stream);
+/* coo2ell (:1339-1394); ellnum 0 = longest row. */
+int clspmv_device_coo2ell_f32(const clspmv_coo_f32* coo, clspmv_ell_f32* dev, int alignment, int ellnum,
+                              clspmv_stream_t stream);
+/* coo2sell (:1397-1513). */
+int clspmv_device_coo2sell_f32(const clspmv_coo_f32* coo, clspmv_sell_f32* dev, unsigned int slice_height,
+                               clspmv_stream_t stream);
+/* coo2b4csr (:1740-1897). */
+int clspmv_device_coo2b4csr_f32(const clspmv_coo_f32* coo, clspmv_b4csr_f32* dev, unsigned int bwidth,
+                                unsigned int bheight, int alignment, clspmv_stream_t stream);
+/* coo2b4ell (:2008-2200); ellnum 0 = most blocks in a block row. */
+int clspmv_device_coo2b4ell_f32(const clspmv_coo_f32* coo, clspmv_b4ell_f32* dev, unsigned int bwidth,
+                                unsigned int bheight, int alignment, int ellnum, clspmv_stream_t stream);
+/* coo2sbell (:2202-2409). */
+int clspmv_device_coo2sbell_f32(const clspmv_coo_f32* coo, clspmv_sbell_f32* dev, unsigned int bwidth,
+                                unsigned int bheight, unsigned int slice_height, clspmv_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Compute entry points (device structs, device x and y).                    */
 /* x has matinfo.width entries, y has matinfo.height entries; both 16-byte  */
 /* aligned. All launches are asynchronous on `stream`.                      */
