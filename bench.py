@@ -105,40 +105,52 @@ def build_workload(small: bool, only=None):
     items = []
     meta = {"ell_width": None}
 
-    def add(key, mat, make, kw=None, part_of=None):
+    def add(key, mat, make, kw=None, part_of=None, conv=None):
+        """conv = (source COO arrays, format, converter arguments): how the
+        host matrix was converted, for the device-conversion comparison."""
         if key not in want:
             return
+        t0 = time.perf_counter()
         host = make()
+        host_s = time.perf_counter() - t0
         h, w = mats[mat][0], mats[mat][1]
         items.append(dict(key=key, matrix=mat, host=host, kw=kw or {}, rows=h, cols=w, nnz=int(host.nnz),
-                          stored=host.stored_bytes(), part_of=part_of))
+                          stored=host.stored_bytes(), part_of=part_of, conv=conv,
+                          host_convert_s=host_s if conv else None))
+
+    def once(make):
+        box = []
+        return lambda: box[0] if box else (box.append(make()) or box[0])
 
     if "stencil27" in mats:
-        coo = F.coo_matrix(*mats["stencil27"])
-        add("dia", "stencil27", lambda: F.coo2dia(coo))
-        add("bdia", "stencil27", lambda: F.coo2bdia(coo))
+        st = mats["stencil27"]
+        coo = F.coo_matrix(*st)
+        add("dia", "stencil27", lambda: F.coo2dia(coo), conv=(st, "dia", ()))
+        add("bdia", "stencil27", lambda: F.coo2bdia(coo), conv=(st, "bdia", ()))
     if "powerlaw" in mats:
         pl = mats["powerlaw"]
         coo = F.coo_matrix(*pl)
-        csr = F.coo2csr(coo)
-        add("csr_merge", "powerlaw", lambda: csr, {"variant": "merge"})
-        add("csr_vector", "powerlaw", lambda: csr, {"variant": "vector"})
-        add("csr_scalar", "powerlaw", lambda: csr, {"variant": "scalar"})
+        csr = once(lambda: F.coo2csr(coo))
+        add("csr_merge", "powerlaw", csr, {"variant": "merge"}, conv=(pl, "csr", ()))
+        add("csr_vector", "powerlaw", csr, {"variant": "vector"})
+        add("csr_scalar", "powerlaw", csr, {"variant": "scalar"})
         add("coo", "powerlaw", lambda: coo)
         if "ell" in want:
-            k = hyb_width(np.diff(csr.array("csr_row_ptr")))
+            k = hyb_width(np.diff(csr().array("csr_row_ptr")))
             meta["ell_width"] = k
             ell_part, coo_tail = split_hyb(pl, k)
-            add("ell", "powerlaw", lambda: F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell")
+            add("ell", "powerlaw", lambda: F.coo2ell(F.coo_matrix(*ell_part), 32, k), part_of="ell",
+                conv=(ell_part, "ell", (32, k)))
             add("ell_tail_coo", "powerlaw", lambda: F.coo_matrix(*coo_tail), part_of="ell")
-        sell = F.coo2sell(coo, 32) if ("sell32" in want or "sell32_planned" in want) else None
-        add("sell32", "powerlaw", lambda: sell)                                     # every stored slot
-        add("sell32_planned", "powerlaw", lambda: sell, {"variant": "planned"})    # real entries only (length plan)
+        sell = once(lambda: F.coo2sell(coo, 32))
+        add("sell32", "powerlaw", sell, conv=(pl, "sell", (32,)))                # every stored slot
+        add("sell32_planned", "powerlaw", sell, {"variant": "planned"})          # real entries only (length plan)
     if "blocks4x4" in mats:
-        coo = F.coo_matrix(*mats["blocks4x4"])
-        add("bell", "blocks4x4", lambda: F.coo2b4ell(coo, 4, 4))
-        add("sbell", "blocks4x4", lambda: F.coo2sbell(coo, 4, 4, 32))
-        add("bcsr", "blocks4x4", lambda: F.coo2b4csr(coo, 4, 4))
+        bl = mats["blocks4x4"]
+        coo = F.coo_matrix(*bl)
+        add("bell", "blocks4x4", lambda: F.coo2b4ell(coo, 4, 4), conv=(bl, "b4ell", (4, 4)))
+        add("sbell", "blocks4x4", lambda: F.coo2sbell(coo, 4, 4, 32), conv=(bl, "sbell", (4, 4, 32)))
+        add("bcsr", "blocks4x4", lambda: F.coo2b4csr(coo, 4, 4), conv=(bl, "b4csr", (4, 4)))
     return mats, items, meta
 
 
@@ -548,6 +560,48 @@ def run_ours(args):
     return 0
 
 
+def run_device_convert(items):
+    """Each sweep matrix converted again on the device from its COO
+    (clspmv_device_coo2<fmt>_f32, COO already resident) against the host
+    converter that built it: seconds, and the converted arrays compared bit
+    for bit with the uploaded host result."""
+    import torch
+    from clspmv_mic_b200 import formats as F
+    res = {}
+    coos = {}
+    for it in items:
+        if not it.get("conv"):
+            continue
+        src, fmt, cargs = it["conv"]
+        key = id(src)
+        if key not in coos:
+            coos.clear()
+            torch.cuda.empty_cache()
+            coos[key] = F.DeviceMatrix(F.coo_matrix(*src))
+        dcoo = coos[key]
+        times = []
+        for _ in range(2):   # the first call also warms the allocator and the sort's scratch sizes
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            m = F.device_convert(dcoo, fmt, *cargs)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+            if len(times) < 2:
+                del m
+        ref = it["dev"].tensors
+        equal = all(torch.equal(m.tensors[f].view(torch.int32), ref[f].view(torch.int32)) for f in m.tensors)
+        dev_s = min(times)
+        res[it["key"]] = {"format": fmt, "args": list(cargs), "nnz": int(dcoo.nnz), "host_s": round(it["host_convert_s"], 3),
+                          "device_s": round(dev_s, 4), "speedup": round(it["host_convert_s"] / dev_s, 1),
+                          "equal_to_host": bool(equal)}
+        del m
+    coos.clear()
+    torch.cuda.empty_cache()
+    return {"note": "host_s = the library's host converter (one core) that built the sweep's matrix; device_s = "
+                    "clspmv_device_coo2<fmt>_f32 from a resident device COO incl. output allocation, best of 2; "
+                    "equal_to_host = every array identical bit for bit", "results": res}
+
+
 def run_extras(args, items, mats, peak):
     """Several right-hand sides with FP32 / BF16 / FP16 values on the sweep's
     matrices, 256 uneven matrices as one batched launch, and the serving
@@ -555,7 +609,7 @@ def run_extras(args, items, mats, peak):
     import torch
     from clspmv_mic_b200 import formats as F
     from clspmv_mic_b200 import workloads as W
-    out = {}
+    out = {"device_convert": run_device_convert(items)}
     t0 = time.perf_counter()
     by_key = {it["key"]: it for it in items}
     csr64 = {}
