@@ -229,6 +229,7 @@ def _declare(lib):
         "clspmv_cocktail_upload_f32": (I32, [P(Cocktail), P(VP)]),
         "clspmv_cocktail_spmv_f32": (I32, [VP, VP, VP, f32, f32, VP]),
         "clspmv_cocktail_device_view": (I32, [VP, P(Cocktail)]),
+        "clspmv_cocktail_iterate_f32": (I32, [VP, VP, VP, f32, f32, I32, VP]),
         "clspmv_cocktail_free": (I32, [VP]),
         "clspmv_run_method_f32": (I32, [S["coo"], I32, I32, I32, P(BenchResult)]),
         "clspmv_bandwidth_test": (I32, [C.c_size_t, I32, I32, P(C.c_double), P(C.c_double)]),

@@ -99,6 +99,14 @@ class DeviceCocktail:
         check(lib().clspmv_cocktail_spmv_f32(self.handle, x.data_ptr(), y.data_ptr(), alpha, beta,
                                              _stream_handle(stream)), "cocktail_spmv")
 
+    def iterate(self, x, y, iterations: int, alpha: float = 1.0, beta: float = 1.0, stream=None) -> None:
+        """`iterations` steps of y <- alpha * A x + beta * y; x[:rows] <- y
+        (the reference's A^k x loop, src/eval.cpp:19-72), asynchronous on
+        `stream`, replayed from a cached CUDA graph (clspmv_cocktail_iterate_f32)."""
+        from .formats import _stream_handle
+        check(lib().clspmv_cocktail_iterate_f32(self.handle, x.data_ptr(), y.data_ptr(), alpha, beta, int(iterations),
+                                                _stream_handle(stream)), "cocktail_iterate")
+
     def close(self):
         if self.handle:
             lib().clspmv_cocktail_free(self.handle)

@@ -28,6 +28,13 @@ struct clspmv_cocktail_handle {
     cudaStream_t streams[9] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[9] = {};
+    // A^k x iteration: a graph of kIterUnroll steps, captured on `cap` for
+    // one (x, y, alpha, beta) and replayed on the caller's stream
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t iter_exec = nullptr;
+    const float* iter_x = nullptr;
+    const float* iter_y = nullptr;
+    float iter_alpha = 0.f, iter_beta = 0.f;
 };
 
 namespace {
@@ -86,6 +93,56 @@ void release(clspmv_cocktail_handle* h)
         if (h->join[i]) cudaEventDestroy(h->join[i]);
     }
     if (h->fork) cudaEventDestroy(h->fork);
+    if (h->iter_exec) cudaGraphExecDestroy(h->iter_exec);
+    if (h->cap) cudaStreamDestroy(h->cap);
+}
+
+constexpr int kIterUnroll = 16;   // steps per replayed graph
+
+// n steps of the reference's loop (src/eval.cpp:44-50): y <- alpha*A*x + beta*y,
+// then the first mat_height entries of x <- y (cpy_vector_from_gpu,
+// src/spmv_cocktail.cpp:1510-1556), stream ordered, no host synchronisation.
+int iterate_steps(clspmv_cocktail_handle* h, float* x, float* y, float alpha, float beta, int n, cudaStream_t st)
+{
+    const size_t bytes = sizeof(float) * (size_t)h->dev.mat_height;
+    for (int i = 0; i < n; i++) {
+        int rc = clspmv_cocktail_spmv_f32(h, x, y, alpha, beta, st);
+        if (!rc && bytes) rc = cuda_status(cudaMemcpyAsync(x, y, bytes, cudaMemcpyDeviceToDevice, st));
+        if (rc) return rc;
+    }
+    return CLSPMV_OK;
+}
+
+int iteration_graph(clspmv_cocktail_handle* h, float* x, float* y, float alpha, float beta)
+{
+    if (h->iter_exec && h->iter_x == x && h->iter_y == y && h->iter_alpha == alpha && h->iter_beta == beta)
+        return CLSPMV_OK;
+    if (h->iter_exec) {
+        cudaGraphExecDestroy(h->iter_exec);
+        h->iter_exec = nullptr;
+    }
+    int rc = CLSPMV_OK;
+    if (!h->cap) rc = cuda_status(cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking));
+    if (rc) return rc;
+    if ((rc = cuda_status(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal)))) return rc;
+    const int rc_steps = iterate_steps(h, x, y, alpha, beta, kIterUnroll, h->cap);
+    cudaGraph_t g = nullptr;
+    rc = cuda_status(cudaStreamEndCapture(h->cap, &g));   // always ends the capture
+    if (rc_steps || rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc_steps ? rc_steps : rc;
+    }
+    rc = cuda_status(cudaGraphInstantiate(&h->iter_exec, g, 0));
+    cudaGraphDestroy(g);
+    if (rc) {
+        h->iter_exec = nullptr;
+        return rc;
+    }
+    h->iter_x = x;
+    h->iter_y = y;
+    h->iter_alpha = alpha;
+    h->iter_beta = beta;
+    return CLSPMV_OK;
 }
 
 }  // namespace
@@ -164,6 +221,23 @@ int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y
         if (!rc) rc = cuda_status(cudaEventRecord(h->join[p], h->streams[p]));
         if (!rc) rc = cuda_status(cudaStreamWaitEvent(st, h->join[p], 0));
     }
+    return rc;
+}
+
+int clspmv_cocktail_iterate_f32(clspmv_cocktail_handle* h, float* x, float* y, float alpha, float beta, int iterations,
+                                clspmv_stream_t stream)
+{
+    if (!h || !x || !y || x == y || iterations < 0) return CLSPMV_ERR_ARG;
+    if (h->dev.mat_width < h->dev.mat_height) return CLSPMV_ERR_ARG;   // x must hold a copy of y
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int full = iterations / kIterUnroll, rest = iterations % kIterUnroll;
+    int rc = CLSPMV_OK;
+    if (full > 0) {
+        rc = iteration_graph(h, x, y, alpha, beta);
+        for (int i = 0; !rc && i < full; i++) rc = cuda_status(cudaGraphLaunch(h->iter_exec, st));
+        if (!rc) rc = after_launch(0);
+    }
+    if (!rc) rc = iterate_steps(h, x, y, alpha, beta, rest, st);
     return rc;
 }
 

@@ -559,6 +559,16 @@ int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_
  * the last bits of y) may differ from run to run within the 1e-5 bound. */
 int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y, float alpha, float beta,
                              clspmv_stream_t stream);
+/* The reference's A^k x loop (src/eval.cpp:19-72) kept on the device:
+ * `iterations` times y <- alpha*A*x + beta*y, then the first mat_height
+ * entries of x <- y (cpy_vector_from_gpu, src/spmv_cocktail.cpp:1510-1556).
+ * Stream ordered with no host synchronisation (the reference waits after
+ * every step): whole groups of 16 steps replay one CUDA graph captured once
+ * per (x, y, alpha, beta) and cached in the handle, the rest launch directly.
+ * Requires mat_width >= mat_height and x != y. alpha = beta = 1 is the
+ * reference's loop. */
+int clspmv_cocktail_iterate_f32(clspmv_cocktail_handle* h, float* x, float* y, float alpha, float beta, int iterations,
+                                clspmv_stream_t stream);
 /* The device-side part structs (device pointers), e.g. to launch one part. */
 int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail_f32* out);
 /* Releases the device parts (replaces free_mat_kernels, :1613-1618). */

@@ -99,3 +99,75 @@ def test_cocktail_parts_alone_sum_to_whole(setup):
         total += yd.cpu().numpy()
     y_ref, _, bound = reference_y(coo, x)
     assert_close(total.astype(np.float32), y_ref, bound * 2, "sum of parts")
+
+
+def _iterate_by_steps(dev, x, y, k, alpha, beta):
+    """The reference's loop (src/eval.cpp:44-50): one SpMV, then x[:rows] <- y."""
+    rows = y.shape[0]
+    for _ in range(k):
+        dev.spmv(x, y, alpha, beta)
+        x[:rows].copy_(y)
+
+
+@pytest.mark.parametrize("cfg,mname", [("plain", "laplace128"), ("block_partial", "mixed"),
+                                       ("sell_ell_fast", "powerlaw")])
+@pytest.mark.parametrize("k", [1, 5, 16, 21, 48])
+def test_cocktail_iterate_matches_step_loop(setup, cfg, mname, k):
+    """clspmv_cocktail_iterate_f32 (graph-replayed groups of 16 steps plus
+    direct steps) against the step-by-step loop on the same device: equal
+    bit for bit for a single part whose kernel has no atomics, within FP32
+    summation-order noise otherwise."""
+    import torch
+    coo, ck = setup[(cfg, mname)]
+    dev = ck.to_device()
+    h, w = coo.shape
+    a = coo.arrays()
+    rowsum = np.zeros(h)
+    np.add.at(rowsum, a["coo_row_id"], np.abs(a["coo_data"]))
+    alpha = float(1.0 / max(rowsum.max(), 1.0))          # keeps ||x|| bounded over the steps
+    x0 = torch.from_numpy(synth.x_vector(w)).cuda()
+    y0 = torch.from_numpy(np.random.default_rng(7).standard_normal(h).astype(np.float32)).cuda()
+    x1, y1 = x0.clone(), y0.clone()
+    dev.iterate(x1, y1, k, alpha, 0.5)
+    x2, y2 = x0.clone(), y0.clone()
+    _iterate_by_steps(dev, x2, y2, k, alpha, 0.5)
+    torch.cuda.synchronize()
+    assert torch.equal(x1[:h], y1)
+    exact = len(dev.parts) == 1 and dev.parts[0] in ("dia", "bdia", "ell", "bell", "sbell", "bcsr")
+    if exact:
+        assert torch.equal(y1, y2), dev.parts
+    else:
+        scale = float(y2.abs().max()) + 1e-30
+        assert float((y1 - y2).abs().max()) <= 1e-4 * scale, dev.parts
+
+
+def test_cocktail_iterate_against_oracle(setup):
+    """Three reference steps (alpha = beta = 1) against the oracle's csr_spmv
+    run three times on the host."""
+    import torch
+    coo, ck = setup[("block_partial", "mixed")]
+    dev = ck.to_device()
+    h, w = coo.shape
+    x = synth.x_vector(w) * np.float32(0.05)
+    y = np.zeros(h, np.float32)
+    xd, yd = torch.from_numpy(x.copy()).cuda(), torch.from_numpy(y.copy()).cuda()
+    dev.iterate(xd, yd, 3)
+    torch.cuda.synchronize()
+    xs, ys = x.copy(), y.copy()
+    for _ in range(3):
+        y_ref, _, bound = reference_y(coo, xs, ys)
+        ys = y_ref.astype(np.float32)
+        xs[:h] = ys
+    scale = np.abs(ys).max() + 1e-30
+    assert np.abs(yd.cpu().numpy() - ys).max() <= 1e-4 * scale
+
+
+def test_cocktail_iterate_rejects_aliasing(setup):
+    import torch
+    from clspmv_mic_b200 import _abi
+    coo, ck = setup[("plain", "laplace128")]
+    dev = ck.to_device()
+    v = torch.zeros(max(coo.shape), device="cuda")
+    with pytest.raises(_abi.ClspmvError) as e:
+        dev.iterate(v, v, 2)
+    assert e.value.status == _abi.ERR_ARG
