@@ -81,9 +81,9 @@ def split_hyb(coo_arrays, k):
     return (h, w, r[head], c[head], v[head]), (h, w, r[~head], c[~head], v[~head])
 
 
-VARIANT_KEYS = {"csr_vector", "csr_scalar", "sell32_planned"}
+VARIANT_KEYS = {"csr_merge", "csr_vector", "csr_scalar", "sell32_planned"}
 FORMAT_KEYS = {"stencil27": ["dia", "bdia"],
-               "powerlaw": ["csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32", "sell32_planned"],
+               "powerlaw": ["csr_chunk", "csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32", "sell32_planned"],
                "blocks4x4": ["bell", "sbell", "bcsr"]}
 
 
@@ -131,7 +131,8 @@ def build_workload(small: bool, only=None):
         pl = mats["powerlaw"]
         coo = F.coo_matrix(*pl)
         csr = once(lambda: F.coo2csr(coo))
-        add("csr_merge", "powerlaw", csr, {"variant": "merge"}, conv=(pl, "csr", ()))
+        add("csr_chunk", "powerlaw", csr, {"variant": "chunk"}, conv=(pl, "csr", ()))
+        add("csr_merge", "powerlaw", csr, {"variant": "merge"})
         add("csr_vector", "powerlaw", csr, {"variant": "vector"})
         add("csr_scalar", "powerlaw", csr, {"variant": "scalar"})
         add("coo", "powerlaw", lambda: coo)
@@ -385,6 +386,8 @@ def run_ours(args):
         ys[it["key"]] = torch.zeros(it["rows"], dtype=torch.float32, device=dev)
         if it["host"].fmt == "csr" and it["kw"].get("variant") == "merge":
             it["dev"].merge_plan(stream)
+        if it["host"].fmt == "csr" and it["kw"].get("variant") == "chunk":
+            it["dev"].chunk_plan(stream)
         if it["host"].fmt == "sell" and it["kw"].get("variant") == "planned":
             d = it["dev"]
             n_items = int(F.lib().clspmv_sell_plan_items(d.sell_plan()))
@@ -615,14 +618,14 @@ def run_extras(args, items, mats, peak):
     by_key = {it["key"]: it for it in items}
     csr64 = {}
     for name, arrs in mats.items():
-        csr_dev = by_key["csr_merge"]["dev"] if name == "powerlaw" else F.DeviceMatrix(F.coo2csr(F.coo_matrix(*arrs)))
+        csr_dev = by_key["csr_chunk"]["dev"] if name == "powerlaw" else F.DeviceMatrix(F.coo2csr(F.coo_matrix(*arrs)))
         csr64[name] = W.fp64_of_csr(csr_dev)
         del csr_dev
     # single-vector SpMV with 16-bit values in each format's own kernel
     spmv16 = {}
     gen = torch.Generator(device="cuda")
     gen.manual_seed(11)
-    for key in ("dia", "bdia", "csr_merge", "coo", "sell32", "bell", "sbell", "bcsr"):
+    for key in ("dia", "bdia", "csr_chunk", "coo", "sell32", "bell", "sbell", "bcsr"):
         if key not in by_key:
             continue
         it = by_key[key]
@@ -650,7 +653,7 @@ def run_extras(args, items, mats, peak):
     out["spmv16"] = {"note": "y = A x with values stored as BF16 / FP16 (per-row power-of-two scale, FP32 "
                              "accumulation) in each format's own kernel; GB/s over the bytes at 2-byte values",
                      "results": spmv16}
-    entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_merge", "bcsr", "sbell")
+    entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_chunk", "bcsr", "sbell")
                if k in by_key]
     out["spmm"] = {"note": "Y = A X, beta 0; GB/s over matrix bytes at the stored value width + k (4n + 4m); "
                            "err_fp64 = max |Y - Y64| / (|A| |X|); CUDA cores (no tensor-core path)",

@@ -21,6 +21,9 @@ int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float a
 int launch_csr_vector(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, cudaStream_t st, bool atomic);
 int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_csr_merge_plan(const clspmv_csr_f32* m, int* tc, cudaStream_t st);
+int launch_csr_chunk(const clspmv_csr_f32* m, const int* chunk_row, const float* x, float* y, float alpha, float beta,
+                     cudaStream_t st, bool atomic);
+int launch_csr_chunk_plan(const clspmv_csr_f32* m, int* chunk_row, cudaStream_t st);
 int launch_coo(const clspmv_coo_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_b4ell(const clspmv_b4ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);

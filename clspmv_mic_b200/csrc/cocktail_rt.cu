@@ -23,7 +23,7 @@ using namespace clspmv;
 
 struct clspmv_cocktail_handle {
     clspmv_cocktail_f32 dev;          // part structs with device pointers
-    int* merge_plan = nullptr;        // tile coordinates of the CSR part
+    int* chunk_plan = nullptr;        // first row of every nonzero chunk of the CSR part
     int nparts = 0;
     cudaStream_t streams[9] = {};
     cudaEvent_t fork = nullptr;
@@ -69,7 +69,7 @@ int launch_part(const clspmv_cocktail_handle* h, int p, const float* x, float* y
         case P_BCSR: return launch_b4csr(&d.bcsr, x, y, alpha, beta, st, atomic);
         case P_SELL: return launch_sell(&d.sell, x, y, alpha, beta, st, atomic);
         case P_ELL: return launch_ell(&d.ell, x, y, alpha, beta, st, atomic);
-        case P_CSR: return launch_csr_merge(&d.csr, h->merge_plan, x, y, alpha, beta, st, atomic);
+        case P_CSR: return launch_csr_chunk(&d.csr, h->chunk_plan, x, y, alpha, beta, st, atomic);
         case P_COO: return launch_coo(&d.coo, x, y, alpha, beta, st, atomic);
     }
     return CLSPMV_ERR_ARG;
@@ -87,7 +87,7 @@ void release(clspmv_cocktail_handle* h)
     if (d.ifuseell) clspmv_device_free_ell_f32(&d.ell);
     if (d.ifusecsr) clspmv_device_free_csr_f32(&d.csr);
     if (d.ifusecoo) clspmv_device_free_coo_f32(&d.coo);
-    if (h->merge_plan) cudaFree(h->merge_plan);
+    if (h->chunk_plan) cudaFree(h->chunk_plan);
     for (int i = 0; i < P_COUNT; i++) {
         if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
         if (h->join[i]) cudaEventDestroy(h->join[i]);
@@ -179,9 +179,9 @@ int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_
     UP(ifusecoo, coo, clspmv_upload_coo_f32)
 #undef UP
     if (!rc && d.ifusecsr) {
-        const int ntiles = clspmv_csr_merge_tiles(d.csr.matinfo.height, d.csr.matinfo.nnz);
-        rc = cuda_status(cudaMalloc(&h->merge_plan, sizeof(int) * 2 * ((size_t)ntiles + 1)));
-        if (!rc) rc = launch_csr_merge_plan(&d.csr, h->merge_plan, 0);
+        const int nplan = clspmv_csr_chunk_plan_size(d.csr.matinfo.nnz);
+        rc = cuda_status(cudaMalloc(&h->chunk_plan, sizeof(int) * (size_t)(nplan > 0 ? nplan : 1)));
+        if (!rc) rc = launch_csr_chunk_plan(&d.csr, h->chunk_plan, 0);
         if (!rc) rc = cuda_status(cudaStreamSynchronize(0));
     }
     for (int p = 0; !rc && p < P_COUNT; p++) {

@@ -688,11 +688,14 @@ constexpr int kCooCtaNnz = kCooWarpNnz * (kBlock / 32);
 constexpr int kCooNoRow = INT_MAX;
 
 // adds alpha * v (times the row's scale for 16-bit values) to y[row]
-template <class V>
-__device__ __forceinline__ void coo_red(const CooArgsT<V>& a, int row, float v)
+template <template <class> class ArgsT, class V>
+__device__ __forceinline__ void coo_red(const ArgsT<V>& a, int row, float v)
 {
     if (row != kCooNoRow) atomicAdd(a.y + row, row_alpha(a.alpha, scl(a), row) * v);
 }
+
+template <template <class> class ArgsT, class V>
+__device__ __forceinline__ void warp_segments(const ArgsT<V>& a, const int (&r)[kCooSteps][4], const float (&p)[kCooSteps][4]);
 
 template <class V>
 __device__ __forceinline__ void coo_warp_chunk(const CooArgsT<V>& a, long long base, uint64_t pe, uint64_t pl)
@@ -728,6 +731,18 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgsT<V>& a, long long b
             for (int j = 0; j < 4; j++)
                 if (r[s][j] != kCooNoRow) p[s][j] *= ld_x(a.x + c[s][j], pl);
     }
+    warp_segments(a, r, p);
+}
+
+// The reduction of a warp's kCooSteps x 128 (row, product) pairs in
+// nonzero order (rows non-decreasing, kCooNoRow past the end): per-lane runs
+// in registers, lane-boundary partials by a segmented scan, the trailing row
+// carried across steps; every finished row segment is added to y with
+// red.global.add.
+template <template <class> class ArgsT, class V>
+__device__ __forceinline__ void warp_segments(const ArgsT<V>& a, const int (&r)[kCooSteps][4], const float (&p)[kCooSteps][4])
+{
+    const int lane = threadIdx.x & 31;
     float carry = 0.f;
     int carry_row = -1;
 #pragma unroll
@@ -803,6 +818,106 @@ __device__ __forceinline__ void coo_cta(const CooArgsT<V>& a, int cta, int ncta,
     long long b, e;
     cta_share(nchunks, 1, cta, ncta, b, e);
     for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) coo_warp_chunk(a, ch * kCooWarpNnz, pe, pl);
+}
+
+// ---------------------------------------------------------------------------
+// CSR by nonzero chunks: the COO kernel's mapping (a warp per kCooWarpNnz
+// consecutive nonzeros, 4 per lane with 128-bit loads of col_id / data, the
+// x gathers issued at once, the same segmented reduction) on CSR arrays,
+// without a row id per nonzero: the rows come from row_ptr. A per-matrix
+// plan holds, for every chunk, the row of its first nonzero (chunk_row); a
+// lane finds the row of its first nonzero of a step by binary search of
+// row_ptr between this chunk's and the next chunk's first rows (a few
+// L1-resident loads), then steps over row ends for the other three.
+// Matrix bytes are CSR's 8 nnz + 4 (m + 1) instead of COO's 12 nnz.
+// beta must already be applied; col_id and data 16-byte aligned.
+// ---------------------------------------------------------------------------
+template <class V>
+__device__ __forceinline__ void csr_chunk_warp(const CsrArgsT<V>& a, const int* __restrict__ chunk_row, long long ch,
+                                               uint64_t pe, uint64_t pl)
+{
+    const int lane = threadIdx.x & 31;
+    const long long base = ch * kCooWarpNnz;
+    int r[kCooSteps][4];
+    float p[kCooSteps][4];
+    {
+        int c[kCooSteps][4];
+#pragma unroll
+        for (int s = 0; s < kCooSteps; s++) {
+            const long long idx = base + s * 128 + lane * 4;
+            if (idx + 3 < a.nnz) {
+                const int4 cv = ld_stream_i4(a.col + idx, pe);
+                const float4 vv = ldv4(a.val + idx, pe);
+                c[s][0] = cv.x; c[s][1] = cv.y; c[s][2] = cv.z; c[s][3] = cv.w;
+                p[s][0] = vv.x; p[s][1] = vv.y; p[s][2] = vv.z; p[s][3] = vv.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const bool in = idx + j < a.nnz;
+                    c[s][j] = in ? ld_stream_i(a.col + idx + j, pe) : 0;
+                    p[s][j] = in ? ldv(a.val + idx + j, pe) : 0.f;
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < kCooSteps; s++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (base + s * 128 + lane * 4 + j < a.nnz) p[s][j] *= ld_x(a.x + c[s][j], pl);
+    }
+    const int ra = __ldg(chunk_row + ch), rb = __ldg(chunk_row + ch + 1);
+#pragma unroll
+    for (int s = 0; s < kCooSteps; s++) {
+        const long long q0 = base + s * 128 + lane * 4;
+        if (q0 >= a.nnz) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) r[s][j] = kCooNoRow;
+            continue;
+        }
+        // largest row in [ra, rb] starting at or before q0
+        int lo = ra, hi = rb;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(a.row_ptr + mid) <= q0) lo = mid;
+            else hi = mid - 1;
+        }
+        int row = lo;
+        r[s][0] = row;
+#pragma unroll
+        for (int j = 1; j < 4; j++) {
+            const long long q = q0 + j;
+            if (q < a.nnz) {
+                while (__ldg(a.row_ptr + row + 1) <= q) row++;
+                r[s][j] = row;
+            } else {
+                r[s][j] = kCooNoRow;
+            }
+        }
+    }
+    warp_segments(a, r, p);
+}
+
+template <class V>
+__device__ __forceinline__ void csr_chunk_cta(const CsrArgsT<V>& a, const int* __restrict__ chunk_row, int cta, int ncta)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    const long long nchunks = ((long long)a.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
+    long long b, e;
+    cta_share(nchunks, 1, cta, ncta, b, e);
+    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) csr_chunk_warp(a, chunk_row, ch, pe, pl);
+}
+
+// chunk_row[c] = row of nonzero c * kCooWarpNnz (the largest row whose start
+// is at or before it), for c < nchunks; chunk_row[nchunks] = rows - 1.
+__device__ __forceinline__ int csr_row_of(const int* __restrict__ row_ptr, int rows, long long q)
+{
+    int lo = 0, hi = rows - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (row_ptr[mid] <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 // ---------------------------------------------------------------------------

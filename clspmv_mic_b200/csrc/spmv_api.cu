@@ -143,6 +143,19 @@ __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, co
 template <class V>
 __global__ void __launch_bounds__(kBlock) k_coo(CooArgsT<V> a) { coo_cta(a, blockIdx.x, gridDim.x, nullptr); }
 
+template <class V>
+__global__ void __launch_bounds__(kBlock) k_csr_chunk(CsrArgsT<V> a, const int* __restrict__ chunk_row)
+{
+    csr_chunk_cta(a, chunk_row, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(kBlock) k_csr_chunk_plan(const int* __restrict__ row_ptr, int rows, long long nchunks,
+                                                           int* chunk_row)
+{
+    for (long long c = blockIdx.x * (long long)kBlock + threadIdx.x; c <= nchunks; c += (long long)gridDim.x * kBlock)
+        chunk_row[c] = c < nchunks ? csr_row_of(row_ptr, rows, c * kCooWarpNnz) : rows - 1;
+}
+
 template <int BW4, int BH, bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_b4ell(B4ellArgsT<V> a) { b4ell_cta<BW4, BH, A>(a, blockIdx.x, gridDim.x, nullptr); }
 
@@ -445,6 +458,40 @@ int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, flo
 }
 
 template <class V>
+int launch_csr_chunk_v(const clspmv_csr_f32* m, const V* data, const float* scale, const int* chunk_row, const float* x,
+                       float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+{
+    if (!m || !chunk_row || !x || !y || !m->csr_row_ptr) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    if (!atomic) {
+        int rc = prescale(y, rows, beta, st);
+        if (rc) return rc;
+    }
+    if (m->matinfo.nnz <= 0) return CLSPMV_OK;
+    if (!m->csr_col_id || !data) return CLSPMV_ERR_ARG;
+    if (!aligned16(m->csr_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
+    CsrArgsT<V> a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, data, x, y, alpha, 1.0f, scale};
+    const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
+    k_csr_chunk<V><<<persistent_grid(k_csr_chunk<V>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
+    return after_launch(1);
+}
+
+int launch_csr_chunk(const clspmv_csr_f32* m, const int* chunk_row, const float* x, float* y, float alpha, float beta,
+                     cudaStream_t st, bool atomic)
+{
+    return launch_csr_chunk_v<float>(m, m ? m->csr_data : nullptr, nullptr, chunk_row, x, y, alpha, beta, st, atomic);
+}
+
+int launch_csr_chunk_plan(const clspmv_csr_f32* m, int* chunk_row, cudaStream_t st)
+{
+    if (!m || !chunk_row || !m->csr_row_ptr || m->matinfo.height <= 0 || m->matinfo.nnz < 0) return CLSPMV_ERR_ARG;
+    const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
+    k_csr_chunk_plan<<<grid_for(nchunks + 1, kBlock), kBlock, 0, st>>>(m->csr_row_ptr, m->matinfo.height, nchunks, chunk_row);
+    return after_launch(1);
+}
+
+template <class V>
 int launch_coo_v(const clspmv_coo_f32* m, const V* data, const float* scale, const float* x, float* y, float alpha, float beta,
                  cudaStream_t st, bool atomic)
 {
@@ -644,6 +691,23 @@ int clspmv_csr_merge_tiles(int rows, int nnz)
 {
     if (rows < 0 || nnz < 0) return -1;
     return (int)(((long long)rows + nnz + kMergeTile - 1) / kMergeTile);
+}
+
+int clspmv_csr_chunk_plan_size(int nnz)
+{
+    if (nnz < 0) return -1;
+    return (int)(((long long)nnz + kCooWarpNnz - 1) / kCooWarpNnz + 1);
+}
+
+int clspmv_csr_chunk_plan(const clspmv_csr_f32* m, int* chunk_row, clspmv_stream_t s)
+{
+    return launch_csr_chunk_plan(m, chunk_row, S(s));
+}
+
+int clspmv_csr_chunk_spmv_f32(const clspmv_csr_f32* m, const int* chunk_row, const float* x, float* y, float alpha,
+                              float beta, clspmv_stream_t s)
+{
+    return launch_csr_chunk(m, chunk_row, x, y, alpha, beta, S(s), false);
 }
 
 int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)

@@ -304,11 +304,22 @@ class DeviceMatrix:
             self._plan = plan
         return self._plan
 
-    def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None, variant: str = "merge",
+    def chunk_plan(self, stream=None):
+        """First row of every 256-nonzero chunk for the chunked CSR kernel (computed once)."""
+        import torch
+        if getattr(self, "_chunk_plan", None) is None:
+            n = lib().clspmv_csr_chunk_plan_size(self.nnz)
+            plan = torch.empty(max(n, 1), dtype=torch.int32, device=self.tensors["csr_row_ptr"].device)
+            check(lib().clspmv_csr_chunk_plan(C.byref(self.struct), plan.data_ptr(), _stream_handle(stream)), "csr_chunk_plan")
+            self._chunk_plan = plan
+        return self._chunk_plan
+
+    def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None, variant: str = "chunk",
              threads_per_row: int = 0, packed: "PackedValues | None" = None) -> None:
         """y <- alpha * A x + beta * y on the device (asynchronous on `stream`);
         with `packed`, from the 16-bit values of self.pack(). `variant`: CSR
-        "merge" (default), "vector" or "scalar"; SELL "planned" reads only each
+        "chunk" (default; "merge" when col_id / data are not 16-byte aligned),
+        "merge", "vector" or "scalar"; SELL "planned" reads only each
         row's real entries (its length plan), which on B200 is slower than the
         padded read for power-law slices: the tails of long rows are strided
         column-major reads."""
@@ -325,6 +336,12 @@ class DeviceMatrix:
                 plan = self.merge_plan(stream)
                 check(L.clspmv_csr_merge_spmv_f32(C.byref(self.struct), plan.data_ptr(), x.data_ptr(), y.data_ptr(),
                                                   alpha, beta, s), "csr_merge_spmv")
+            elif variant == "chunk":
+                if (self.struct.csr_col_id or 0) % 16 or (self.struct.csr_data or 0) % 16:
+                    return self.spmv(x, y, alpha, beta, stream, variant="merge")
+                plan = self.chunk_plan(stream)
+                check(L.clspmv_csr_chunk_spmv_f32(C.byref(self.struct), plan.data_ptr(), x.data_ptr(), y.data_ptr(),
+                                                  alpha, beta, s), "csr_chunk_spmv")
             elif variant == "vector":
                 check(L.clspmv_csr_vector_spmv_f32(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta,
                                                    threads_per_row, s), "csr_vector_spmv")

@@ -342,6 +342,19 @@ int clspmv_csr_merge_spmv_f32(const clspmv_csr_f32* dev, const int* tile_coord,
                               const float* x, float* y, float alpha, float beta,
                               clspmv_stream_t stream);
 
+/* CSR SpMV by nonzero chunks (replaces the same kernels as the merge path,
+ * kernels/spmv_csr_scalar.cl and spmv_csr_vector.cl): a warp per 256
+ * consecutive nonzeros, 128-bit loads of col_id / data, the rows recovered
+ * from row_ptr and reduced with a warp segmented scan, rows cut by a chunk
+ * edge added atomically (summation order differs from the reference's
+ * serial one within the 1e-5 bound). The plan holds the first row of every
+ * chunk: clspmv_csr_chunk_plan_size(nnz) ints, filled once per matrix by
+ * clspmv_csr_chunk_plan. col_id and data must be 16-byte aligned. */
+int clspmv_csr_chunk_plan_size(int nnz);
+int clspmv_csr_chunk_plan(const clspmv_csr_f32* dev, int* chunk_row, clspmv_stream_t stream);
+int clspmv_csr_chunk_spmv_f32(const clspmv_csr_f32* dev, const int* chunk_row, const float* x, float* y, float alpha,
+                              float beta, clspmv_stream_t stream);
+
 /* The same merge-path SpMV for callers that cannot allocate device memory at
  * the call (a running loop that must not call cudaMalloc/cudaFree, which can
  * wait for the whole device; a binding with no device allocator; a service

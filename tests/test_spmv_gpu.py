@@ -36,7 +36,7 @@ def _check(coo, host, what, alpha=1.0, beta=1.0, y0=None, **kw):
 
 
 @pytest.mark.parametrize("name", ALL_RECT)
-@pytest.mark.parametrize("variant", ["merge", "vector", "scalar"])
+@pytest.mark.parametrize("variant", ["merge", "chunk", "vector", "scalar"])
 def test_csr(name, variant):
     coo = coo_of(name)
     _check(coo, F.coo2csr(coo), f"csr-{variant}", variant=variant)
@@ -50,7 +50,7 @@ def test_csr_vector_lanes(name, tpr):
 
 
 @pytest.mark.parametrize("name", ["powerlaw3k", "laplace33", "random_empty_rows"])
-@pytest.mark.parametrize("align,variant", [(4, "scalar"), (16, "vector"), (4, "merge")])
+@pytest.mark.parametrize("align,variant", [(4, "scalar"), (16, "vector"), (4, "merge"), (4, "chunk")])
 def test_csr_padded(name, align, variant):
     """pad_csr input (the reference's padded CSR drivers) takes the 128-bit path."""
     coo = coo_of(name)
@@ -98,10 +98,10 @@ def test_block_formats(name, bh, bw):
 
 
 @pytest.mark.parametrize("alpha,beta", [(2.5, -0.5), (1.0, 0.0), (-1.0, 1.0), (0.5, 2.0)])
-@pytest.mark.parametrize("fmt", ["csr-merge", "csr-vector", "csr-scalar", "coo", "dia", "bdia", "ell", "sell",
+@pytest.mark.parametrize("fmt", ["csr-merge", "csr-chunk", "csr-vector", "csr-scalar", "coo", "dia", "bdia", "ell", "sell",
                                  "b4csr", "b4ell", "sbell"])
 def test_alpha_beta(fmt, alpha, beta):
-    coo = coo_of("powerlaw3k" if fmt in ("csr-merge", "coo", "ell", "sell") else "stencil9" if "dia" in fmt else
+    coo = coo_of("powerlaw3k" if fmt in ("csr-merge", "csr-chunk", "coo", "ell", "sell") else "stencil9" if "dia" in fmt else
                  "blocks_odd" if fmt[:2] in ("b4", "sb") else "laplace33")
     y0 = np.random.default_rng(8).standard_normal(coo.shape[0]).astype(np.float32)
     kw = {}
@@ -178,3 +178,29 @@ def test_sell_planned_matches_padded(name, sh):
     dev = F.DeviceMatrix(F.coo2sell(coo, sh))
     host = F.coo2sell(coo, sh)                   # kept alive while its array is read
     assert coo.nnz <= dev.sell_plan_entries() <= int(host.array("sell_slice_ptr")[-1])
+
+
+@pytest.mark.parametrize("rows,lens", [
+    (300, "empty_runs"),      # long runs of empty rows inside a chunk
+    (5, "one_long"),          # one row spanning many chunks
+    (4097, "ones"),           # a chunk spanning 256 rows
+])
+def test_csr_chunk_row_shapes(rows, lens):
+    """The chunked CSR kernel recovers rows from row_ptr: rows that span
+    many chunks, chunks that span hundreds of rows, and empty rows."""
+    rng = np.random.default_rng(12)
+    if lens == "empty_runs":
+        ln = np.zeros(rows, int)
+        ln[::37] = rng.integers(1, 700, ln[::37].size)
+    elif lens == "one_long":
+        ln = np.array([0, 3, 5000, 0, 1])
+    else:
+        ln = np.ones(rows, int)
+    w = 6000
+    r = np.repeat(np.arange(rows), ln)
+    c = np.concatenate([np.sort(rng.choice(w, k, replace=False)) for k in ln if k > 0])
+    v = rng.standard_normal(r.size).astype(np.float32)
+    coo = F.coo_matrix(rows, w, r, c, v)
+    for alpha, beta in [(1.0, 1.0), (0.5, 0.0)]:
+        y0 = rng.standard_normal(rows).astype(np.float32)
+        _check(coo, F.coo2csr(coo), f"csr-chunk {lens}", alpha, beta, y0, variant="chunk")
