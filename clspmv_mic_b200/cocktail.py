@@ -49,6 +49,25 @@ class CocktailMatrix:
     def parts(self) -> dict:
         return {p: self.part(p) for p, _ in COCKTAIL_PARTS if self.uses(p)}
 
+    def with_flat_as_csr(self) -> "CocktailMatrix | None":
+        """The same partition with its COO part stored as CSR instead (same
+        nonzeros; the chunked CSR kernel reads 8 bytes per nonzero where COO
+        reads 12), or None when there is no COO part or a CSR part exists
+        already. The parts are shared with this matrix, which the result
+        keeps alive."""
+        if not self.uses("coo") or self.uses("csr"):
+            return None
+        from .formats import coo2csr
+        csr = coo2csr(self.part("coo"))
+        st = _abi.Cocktail.from_buffer_copy(self.struct)
+        st.ifusecoo = False
+        st.ifusecsr = True
+        st.csr = _abi.Csr.from_buffer_copy(csr.struct)
+        st.coo = _abi.Coo()
+        out = CocktailMatrix(st, owner=None)
+        out._base, out._csr = self, csr
+        return out
+
     def to_device(self) -> "DeviceCocktail":
         return DeviceCocktail(self)
 

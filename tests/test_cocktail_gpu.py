@@ -171,3 +171,22 @@ def test_cocktail_iterate_rejects_aliasing(setup):
     with pytest.raises(_abi.ClspmvError) as e:
         dev.iterate(v, v, 2)
     assert e.value.status == _abi.ERR_ARG
+
+
+@pytest.mark.parametrize("cfg,mname", [("block_partial", "mixed"), ("dia_flat", "band_noise")])
+def test_cocktail_flat_part_as_csr(setup, cfg, mname):
+    """The tuner's CSR storage of the flat part runs through the Cocktail
+    runtime (chunked CSR kernel) to the same y within the 1e-5 row bound."""
+    import torch
+    coo, ck = setup[(cfg, mname)]
+    alt = ck.with_flat_as_csr()
+    if alt is None:
+        pytest.skip(f"no COO part: {ck.summary()}")
+    dev = alt.to_device()
+    x = synth.x_vector(coo.shape[1])
+    y0 = np.random.default_rng(5).standard_normal(coo.shape[0]).astype(np.float32)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+    dev.spmv(xd, yd, 1.0, 1.0)
+    torch.cuda.synchronize()
+    y_ref, _, bound = reference_y(coo, x, y0, 1.0, 1.0)
+    assert_close(yd.cpu().numpy(), y_ref, bound, f"flat as csr {cfg}/{mname} parts={dev.parts}")

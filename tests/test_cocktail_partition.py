@@ -138,3 +138,33 @@ def test_missing_tables_rejected(tmp_path, matrices):
     with pytest.raises(_abi.ClspmvError) as e:
         CK.analyze(matrices["laplace128"], tmp_path)
     assert e.value.status == _abi.ERR_ARG
+
+
+def test_flat_part_as_csr(table_dirs):
+    """The tuner's "flat_as": "csr" candidate: the same partition with the
+    COO part stored as CSR (the library's coo2csr of that part), every other
+    part untouched."""
+    mats = _matrices()
+    found = 0
+    for cfg, mname in [("block_partial", "mixed"), ("block_partial", "blocks_noise"), ("dia_flat", "band_noise"),
+                       ("random0", "band_blocks_noise")]:
+        coo = F.coo_matrix(*mats[mname])
+        m = CK.analyze(coo, table_dirs[cfg])
+        alt = m.with_flat_as_csr()
+        if alt is None:
+            assert not m.uses("coo") or m.uses("csr")
+            continue
+        found += 1
+        assert alt.uses("csr") and not alt.uses("coo")
+        ref = F.coo2csr(m.part("coo"))
+        for field in ("csr_row_ptr", "csr_col_id", "csr_data"):
+            np.testing.assert_array_equal(alt.part("csr").array(field), ref.array(field))
+        for p, _ in CK.COCKTAIL_PARTS:
+            if p in ("coo", "csr") or not m.uses(p):
+                continue
+            assert alt.uses(p)
+            for field, a in m.part(p).arrays().items():
+                np.testing.assert_array_equal(alt.part(p).array(field), a)
+        assert sum(v["nnz"] for v in alt.summary().values() if isinstance(v, dict)) == \
+            sum(v["nnz"] for v in m.summary().values() if isinstance(v, dict))
+    assert found >= 1
