@@ -9,6 +9,10 @@
         spmv_cocktail (src/eval.cpp:100-131): read, print the matrix info,
         partition with the benchmark tables of table_dir (default
         $CLSPMVPATH, else the tables shipped with the package), evaluate.
+    python -m clspmv_mic_b200 spmm <b4csr|b4ell|sbell> <k> [reps] [block_rows] [f32|bf16|f16]
+        Y = A X with k right-hand sides on the synthetic 4x4-block matrix
+        (block_rows x 8 dense blocks, default 500,000): prints the mean time
+        and GFLOP/s. The command the SpMM kernel profiles are taken with.
 """
 from __future__ import annotations
 
@@ -46,6 +50,8 @@ def main(argv: list[str]) -> int:
         coo = read_mmf(path)
         run_method(coo, _BY_NUMBER[method], ntimes, verbose=True)
         return 0
+    if cmd == "spmm":
+        return _spmm(path, argv[2:])
     if cmd == "cocktail":
         coo = read_mmf(path)
         table_dir = argv[2] if len(argv) > 2 else os.environ.get("CLSPMVPATH") or str(ensure_default_tables())
@@ -60,6 +66,37 @@ def main(argv: list[str]) -> int:
         evaluate(mat, vec, res, coores, 1000, verbose=True)
         return 0
     return _usage()
+
+
+def _spmm(fmt: str, rest: list[str]) -> int:
+    import torch
+    from . import formats as F
+    from . import synth
+    k = int(rest[0]) if rest else 32
+    reps = int(rest[1]) if len(rest) > 1 else 20
+    brows = int(rest[2]) if len(rest) > 2 else 500_000
+    vt = rest[3] if len(rest) > 3 else "f32"
+    coo = F.coo_matrix(*synth.block_rows(brows, 8))
+    host = {"b4csr": lambda: F.coo2b4csr(coo, 4, 4), "b4ell": lambda: F.coo2b4ell(coo, 4, 4),
+            "sbell": lambda: F.coo2sbell(coo, 4, 4, 32)}[fmt]()
+    m = F.DeviceMatrix(host)
+    rows, cols = m.shape
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    X = torch.rand((cols, k), generator=g, device="cuda") * 2 - 1
+    Y = torch.empty((rows, k), device="cuda")
+    p = None if vt == "f32" else m.pack(vt)
+    for _ in range(3):
+        m.spmm(X, Y, 1.0, 0.0, packed=p)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        m.spmm(X, Y, 1.0, 0.0, packed=p)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    print(f"{fmt} k={k} {vt}: {ms:.4f} ms, {2.0 * m.nnz * k / (ms * 1e-3) / 1e9:.1f} GFLOP/s")
+    return 0
 
 
 if __name__ == "__main__":
