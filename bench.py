@@ -786,8 +786,12 @@ def run_cocktail_c3(args, peak):
     mat = res.matrix
     out["tune_seconds"] = round(time.perf_counter() - t0, 1)
     out["tuning"] = {"chosen_knob": res.knob, "candidates": res.report,
-                     "note": "each analyze_matrix knob setting of the reference, partition measured with the "
-                             "Cocktail runtime; the first candidate is the reference's default"}
+                     "part_layouts": res.parts, "ms_before_part_refinement": res.ms_partition,
+                     "part_candidates": res.part_report,
+                     "note": "each analyze_matrix knob setting of the reference (and the COO part as CSR), partition "
+                             "measured with the Cocktail runtime; the first candidate is the reference's default; "
+                             "then each SELL / block part re-stored in every slice height / block shape, timed alone, "
+                             "the fastest kept when the whole partition gets faster"}
     out["partition"] = mat.summary()
     dev = mat.to_device()
     h, w = coo.shape

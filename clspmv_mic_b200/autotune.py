@@ -13,7 +13,10 @@ the next matrix with the same structure is partitioned once, without
 measuring. Beyond the reference's knobs, each partition with a COO part is
 also measured with that part stored as CSR ("flat_as": "csr"), since on this
 GPU the chunked CSR kernel and the COO kernel reach the same gather rate and
-CSR moves a third fewer bytes.
+CSR moves a third fewer bytes. The winning partition is then refined part
+by part (refine_parts): the SELL part over slice heights and the block
+parts over the eight block shapes, each candidate converted on the device
+and timed alone, the fastest kept and cached with the knob.
 """
 from __future__ import annotations
 
@@ -25,6 +28,7 @@ from pathlib import Path
 
 import numpy as np
 
+from . import formats as F
 from .cocktail import CocktailMatrix, analyze
 from .formats import HostMatrix
 
@@ -65,6 +69,86 @@ def partition(coo: HostMatrix, table_dir, knob: dict) -> CocktailMatrix:
     return m
 
 
+# part -> candidate layouts of its nonzeros: (converter, arguments after the COO)
+SELL_HEIGHTS = (8, 16, 32, 64, 128)
+PART_LAYOUTS = {
+    "sell": [("sell", (sh,)) for sh in SELL_HEIGHTS],
+    "sbell": [("sbell", (bw, bh, 32)) for bh, bw in F.BLOCK_SHAPES],
+    "bell": [("b4ell", (bw, bh)) for bh, bw in F.BLOCK_SHAPES],
+    "bcsr": [("b4csr", (bw, bh)) for bh, bw in F.BLOCK_SHAPES],
+}
+
+
+def _layout_of(m: CocktailMatrix, part: str):
+    st = getattr(m.struct, part)
+    if part == "sell":
+        return ("sell", (int(st.sell_slice_height),))
+    if part == "sbell":
+        return ("sbell", (int(st.sbell_bwidth), int(st.sbell_bheight), int(st.sbell_slice_height)))
+    if part == "bell":
+        return ("b4ell", (int(st.b4ell_bwidth), int(st.b4ell_bheight)))
+    return ("b4csr", (int(st.b4csr_bwidth), int(st.b4csr_bheight)))
+
+
+def _time_alone(dev, reps: int) -> float:
+    import torch
+    h, w = dev.shape
+    x = torch.rand(w, device="cuda")
+    y = torch.zeros(h, device="cuda")
+    for _ in range(3):
+        dev.spmv(x, y, 1.0, 1.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        dev.spmv(x, y, 1.0, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def apply_part_layouts(m: CocktailMatrix, layouts: dict) -> CocktailMatrix:
+    """Re-stores the listed parts in the given layouts ({part: [converter,
+    [args]]}), converting each part's nonzeros on the host."""
+    for part, (conv, args) in layouts.items():
+        if not m.uses(part) or _layout_of(m, part) == (conv, tuple(args)):
+            continue
+        coo = F.to_coo(m.part(part))
+        m = m.with_part(part, getattr(F, f"coo2{conv}")(coo, *args))
+    return m
+
+
+def refine_parts(m: CocktailMatrix, reps: int = 10, report: list | None = None) -> dict:
+    """Fastest layout of each refinable part, each candidate converted on the
+    device from the part's nonzeros (clspmv_device_coo2<fmt>_f32) and timed
+    alone; returns {part: [converter, [args]]} for the parts whose best
+    layout differs from the partitioner's."""
+    from . import _abi
+    chosen = {}
+    for part, cands in PART_LAYOUTS.items():
+        if not m.uses(part):
+            continue
+        dcoo = F.DeviceMatrix(F.to_coo(m.part(part)))
+        current = _layout_of(m, part)
+        best, best_ms, tried = None, None, []
+        for conv, args in cands:
+            try:
+                d = F.device_convert(dcoo, conv, *args)
+            except _abi.ClspmvError:
+                tried.append(dict(layout=[conv, list(args)], refused=True))
+                continue
+            ms = _time_alone(d, reps)
+            del d
+            tried.append(dict(layout=[conv, list(args)], ms=round(ms, 4)))
+            if best_ms is None or ms < best_ms:
+                best, best_ms = (conv, args), ms
+        if report is not None:
+            report.append(dict(part=part, partitioner=[current[0], list(current[1])], candidates=tried))
+        if best is not None and best != current:
+            chosen[part] = [best[0], list(best[1])]
+        del dcoo
+    return chosen
+
+
 def _partition_key(m: CocktailMatrix):
     return tuple(sorted((k, v["nnz"]) for k, v in m.summary().items() if isinstance(v, dict) and "nnz" in v))
 
@@ -97,6 +181,9 @@ class TuneResult:
     ms: float
     from_cache: bool = False
     report: list = field(default_factory=list)
+    parts: dict = field(default_factory=dict)        # refined part layouts
+    part_report: list = field(default_factory=list)
+    ms_partition: float | None = None                 # before the part refinement
 
 
 def default_cache() -> Path:
@@ -104,7 +191,7 @@ def default_cache() -> Path:
 
 
 def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None, reps: int = 10,
-         knobs=KNOBS, use_cache: bool = True) -> TuneResult:
+         knobs=KNOBS, use_cache: bool = True, refine: bool = True) -> TuneResult:
     """Fastest measured partition of `coo` over the knob settings."""
     cache = Path(cache) if cache is not None else default_cache()
     sig = signature(coo)
@@ -115,8 +202,9 @@ def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None
         except (OSError, ValueError):
             entries = {}
     if use_cache and sig in entries:
-        knob = entries[sig]["knob"]
-        return TuneResult(partition(coo, table_dir, knob), knob, entries[sig]["ms"], from_cache=True)
+        knob, parts = entries[sig]["knob"], entries[sig].get("parts", {})
+        m = apply_part_layouts(partition(coo, table_dir, knob), parts)
+        return TuneResult(m, knob, entries[sig]["ms"], from_cache=True, parts=parts)
     best, seen, report = None, {}, []
     for ref_knob in knobs:
         base = analyze(coo, table_dir, **ref_knob)
@@ -132,7 +220,16 @@ def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None
             if best is None or ms < best.ms:
                 best = TuneResult(m, knob, ms)
     best.report = report
-    entries[sig] = {"knob": best.knob, "ms": best.ms, "shape": list(coo.shape), "nnz": int(coo.nnz)}
+    best.ms_partition = best.ms
+    if refine:
+        layouts = refine_parts(best.matrix, reps, best.part_report)
+        if layouts:
+            m = apply_part_layouts(best.matrix, layouts)
+            ms = measure_ms(m, reps)
+            if ms < best.ms:
+                best.matrix, best.ms, best.parts = m, ms, layouts
+    entries[sig] = {"knob": best.knob, "parts": best.parts, "ms": best.ms, "shape": list(coo.shape),
+                    "nnz": int(coo.nnz)}
     try:
         cache.parent.mkdir(parents=True, exist_ok=True)
         cache.write_text(json.dumps(entries, indent=1))

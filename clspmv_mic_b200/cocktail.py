@@ -68,6 +68,19 @@ class CocktailMatrix:
         out._base, out._csr = self, csr
         return out
 
+    def with_part(self, part: str, host: HostMatrix) -> "CocktailMatrix":
+        """The same partition with part `part` replaced by `host` (the same
+        nonzeros in another layout of that slot's format, e.g. another block
+        shape or slice height). Shares the other parts with this matrix,
+        which the result keeps alive."""
+        if not self.uses(part):
+            raise ValueError(f"part {part} is not used")
+        st = _abi.Cocktail.from_buffer_copy(self.struct)
+        setattr(st, part, type(getattr(st, part)).from_buffer_copy(host.struct))
+        out = CocktailMatrix(st, owner=None)
+        out._base, out._part = self, host
+        return out
+
     def to_device(self) -> "DeviceCocktail":
         return DeviceCocktail(self)
 

@@ -168,3 +168,33 @@ def test_flat_part_as_csr(table_dirs):
         assert sum(v["nnz"] for v in alt.summary().values() if isinstance(v, dict)) == \
             sum(v["nnz"] for v in m.summary().values() if isinstance(v, dict))
     assert found >= 1
+
+
+def test_part_layout_change_keeps_nonzeros(table_dirs):
+    """The tuner's part refinement re-stores a block part in another block
+    shape: same nonzeros (inverse conversion), other parts untouched."""
+    from clspmv_mic_b200 import autotune as A
+    mats = _matrices()
+    done = 0
+    for cfg, mname in [("block_partial", "mixed"), ("sbell_bell", "blocks_noise"), ("fl1_bl8_dia6", "mixed")]:
+        coo = F.coo_matrix(*mats[mname])
+        m = CK.analyze(coo, table_dirs[cfg])
+        for part in ("sbell", "bell", "bcsr", "sell"):
+            if not m.uses(part):
+                continue
+            conv, args = A._layout_of(m, part)
+            new = ("sell", (64,)) if part == "sell" else (conv, (8, 2) + tuple(args[2:]))
+            if (conv, tuple(args)) == new:
+                new = (conv, (4, 1) + tuple(args[2:]))
+            alt = A.apply_part_layouts(m, {part: [new[0], list(new[1])]})
+            assert A._layout_of(alt, part) == new
+            c0, c1 = F.to_coo(m.part(part)), F.to_coo(alt.part(part))   # keep the owners alive
+            a0, a1 = c0.arrays(), c1.arrays()
+            for k in a0:
+                np.testing.assert_array_equal(a0[k], a1[k])
+            for p, _ in CK.COCKTAIL_PARTS:
+                if p != part and m.uses(p):
+                    for field, arr in m.part(p).arrays().items():
+                        np.testing.assert_array_equal(alt.part(p).array(field), arr)
+            done += 1
+    assert done >= 1

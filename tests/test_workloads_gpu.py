@@ -67,9 +67,10 @@ def test_tune_measures_and_caches(tmp_path):
     cache = tmp_path / "tune.json"
     r = tune(coo, root, cache=cache, reps=2)
     assert not r.from_cache and r.ms > 0 and r.report and r.report[0]["knob"] == {}
-    assert min(c["ms"] for c in r.report) == pytest.approx(r.ms, abs=1e-4)
+    assert min(c["ms"] for c in r.report) == pytest.approx(r.ms_partition, abs=1e-4)
+    assert r.ms <= r.ms_partition + 1e-9
     again = tune(coo, root, cache=cache)
-    assert again.from_cache and again.knob == r.knob
+    assert again.from_cache and again.knob == r.knob and again.parts == r.parts
     import torch
     dev = again.matrix.to_device()
     x = torch.rand(coo.shape[1], device="cuda")
@@ -80,3 +81,30 @@ def test_tune_measures_and_caches(tmp_path):
     y64, sc = __import__("oracle.oracle", fromlist=["x"]).csr_f64(csr, x.cpu().numpy())
     assert np.all(np.abs(y.cpu().numpy() - y64) <= 1e-5 * sc + 1e-30)
     dev.close()
+
+
+def test_tune_refines_block_part(tmp_path):
+    """A partition with a block part: every block shape is tried for it on
+    the device, and the tuned (possibly re-shaped) matrix still gives y."""
+    from clspmv_mic_b200 import tables as T
+    from clspmv_mic_b200.autotune import tune
+    import torch
+    root = T.model_tables(tmp_path / "t", seed=5, scale={"bcsr": 0.2, "sbell": 2.0, "bell": 1.8})
+    coo = F.coo_matrix(*__import__("clspmv_mic_b200.synth", fromlist=["x"]).block_rows(3000, 6, seed=2))
+    r = tune(coo, root, cache=tmp_path / "tune.json", reps=3)
+    block_parts = [p for p in ("sbell", "bell", "bcsr", "sell") if r.matrix.uses(p)]
+    assert block_parts, r.matrix.summary()
+    tried = {e["part"]: e for e in r.part_report}
+    for p in block_parts:
+        assert len(tried[p]["candidates"]) >= 5
+    dev = r.matrix.to_device()
+    x = torch.rand(coo.shape[1], device="cuda")
+    y = torch.zeros(coo.shape[0], device="cuda")
+    dev.spmv(x, y, 1.0, 0.0)
+    torch.cuda.synchronize()
+    csr = F.coo2csr(coo)
+    y64, sc = __import__("oracle.oracle", fromlist=["x"]).csr_f64(csr, x.cpu().numpy())
+    assert np.all(np.abs(y.cpu().numpy() - y64) <= 1e-5 * sc + 1e-30)
+    dev.close()
+    again = tune(coo, root, cache=tmp_path / "tune.json")
+    assert again.from_cache and again.parts == r.parts
