@@ -54,3 +54,26 @@ def test_two_ranks_gloo():
         assert rc == 0
         if r == 1:
             assert text == ""
+
+
+@pytest.mark.parametrize("parts", [1, 3, 8])
+def test_reference_arm_row_blocks_give_the_same_y(parts):
+    """The reference arm runs csr_spmv on nnz-balanced row blocks in host
+    threads; the blocks cover every row once and give y bit for bit."""
+    import numpy as np
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from clspmv_mic_b200 import formats as F
+    from oracle import oracle as O
+    from tests.matrices import coo_of
+    csr = F.coo2csr(coo_of("powerlaw3k"))
+    x = np.random.default_rng(1).uniform(-1, 1, csr.shape[1]).astype(np.float32)
+    fn = O.spmv_ref if O.ref() is not None else O.spmv_port
+    full = fn(csr, x)
+    y = np.zeros(csr.shape[0], np.float32)
+    blocks = bench.row_blocks(csr, parts)
+    assert blocks[0][0] == 0 and blocks[-1][1] == csr.shape[0]
+    for (r0, r1, slab), nxt in zip(blocks, blocks[1:] + [(csr.shape[0], None, None)]):
+        assert r1 == nxt[0]
+        y[r0:r1] = fn(slab, x)
+    assert np.array_equal(y.view(np.uint32), full.view(np.uint32))
