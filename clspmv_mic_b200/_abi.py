@@ -219,6 +219,7 @@ def _declare(lib):
         "clspmv_csr_chunk_plan_size": (I32, [I32]),
         "clspmv_csr_chunk_plan": (I32, [S["csr"], VP, VP]),
         "clspmv_csr_chunk_spmv_f32": (I32, [S["csr"], VP, VP, VP, f32, f32, VP]),
+        "clspmv_csr_chunk_spmv_packed": (I32, [S["csr"], I32, VP, VP, VP, VP, VP, f32, f32, VP]),
         "clspmv_coo_spmv_f32": (I32, [S["coo"], VP, VP, f32, f32, VP]),
         "clspmv_dia_spmv_f32": (I32, [S["dia"], VP, VP, f32, f32, VP]),
         "clspmv_bdia_spmv_f32": (I32, [S["bdia"], VP, VP, f32, f32, VP]),

@@ -797,5 +797,18 @@ int clspmv_b4csr_spmv_f32(const clspmv_b4csr_f32* m, const float* x, float* y, f
 int clspmv_spmv_packed(int format, const void* dev, int value_type, const void* values, const float* row_scale,
                        const int* tile_coord, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_packed(format, dev, value_type, values, row_scale, tile_coord, x, y, alpha, beta, S(s), false); }
+int clspmv_csr_chunk_spmv_packed(const clspmv_csr_f32* m, int value_type, const void* values, const float* row_scale,
+                                 const int* chunk_row, const float* x, float* y, float alpha, float beta,
+                                 clspmv_stream_t s)
+{
+    if (!values || !row_scale) return CLSPMV_ERR_ARG;
+    if (value_type == CLSPMV_VALUES_BF16)
+        return launch_csr_chunk_v(m, static_cast<const __nv_bfloat16*>(values), row_scale, chunk_row, x, y, alpha, beta,
+                                  S(s), false);
+    if (value_type == CLSPMV_VALUES_F16)
+        return launch_csr_chunk_v(m, static_cast<const __half*>(values), row_scale, chunk_row, x, y, alpha, beta, S(s),
+                                  false);
+    return CLSPMV_ERR_ARG;
+}
 
 }  // extern "C"

@@ -326,6 +326,13 @@ class DeviceMatrix:
         L = lib()
         s = _stream_handle(stream)
         if packed is not None:
+            if self.fmt == "csr" and variant == "chunk" and not ((self.struct.csr_col_id or 0) % 16
+                                                                 or packed.values.data_ptr() % 8):
+                check(L.clspmv_csr_chunk_spmv_packed(C.byref(self.struct), _abi.VALUE_TYPES[packed.value_type],
+                                                     packed.values.data_ptr(), packed.row_scale.data_ptr(),
+                                                     self.chunk_plan(stream).data_ptr(), x.data_ptr(), y.data_ptr(),
+                                                     alpha, beta, s), "csr_chunk_spmv_packed")
+                return
             plan = self.merge_plan(stream).data_ptr() if self.fmt == "csr" else None
             check(L.clspmv_spmv_packed(_abi.FORMAT_IDS[self.fmt], C.byref(self.struct), _abi.VALUE_TYPES[packed.value_type],
                                        packed.values.data_ptr(), packed.row_scale.data_ptr(), plan, x.data_ptr(),

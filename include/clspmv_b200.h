@@ -501,6 +501,11 @@ int clspmv_pack_values(int format, const void* dev, int value_type, void* values
 int clspmv_spmv_packed(int format, const void* dev, int value_type, const void* values, const float* row_scale,
                        const int* tile_coord, const float* x, float* y, float alpha, float beta,
                        clspmv_stream_t stream);
+/* The same for CSR in the nonzero-chunk kernel (`chunk_row` from
+ * clspmv_csr_chunk_plan); col_id 16-byte and values 8-byte aligned. */
+int clspmv_csr_chunk_spmv_packed(const clspmv_csr_f32* dev, int value_type, const void* values,
+                                 const float* row_scale, const int* chunk_row, const float* x, float* y,
+                                 float alpha, float beta, clspmv_stream_t stream);
 
 /* One Y <- alpha * A * X + beta * Y of a batch (fields as in clspmv_spmm). */
 typedef struct {

@@ -172,3 +172,22 @@ def test_spmv_packed_dedicated(name, fmt, args, value_type):
         err = np.abs(yd.cpu().numpy().astype(np.float64) - ref[:, 0])
         lim = RTOL[value_type] * bound[:, 0] + 1e-6 * abs(beta) * np.abs(y0) + 1e-30
         assert np.all(err <= lim), (name, fmt, args, value_type, alpha, beta, float((err / (bound[:, 0] + 1e-30)).max()))
+
+
+@pytest.mark.parametrize("value_type", ["bf16", "f16"])
+@pytest.mark.parametrize("variant", ["chunk", "merge"])
+def test_csr_packed_both_kernels(value_type, variant):
+    """16-bit CSR values in the chunked and the merge-path kernel."""
+    import torch
+    coo = coo_of("powerlaw3k")
+    m, n = coo.shape
+    dev = device_of(coo, "csr")
+    p = dev.pack(value_type)
+    x = synth.x_vector(n, seed=4)
+    y0 = np.random.default_rng(3).uniform(-1, 1, m).astype(np.float32)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+    dev.spmv(xd, yd, 0.5, 1.0, packed=p, variant=variant)
+    torch.cuda.synchronize()
+    ref, bound = spmm_reference(coo, x[:, None], y0[:, None], 0.5, 1.0)
+    err = np.abs(yd.cpu().numpy().astype(np.float64) - ref[:, 0])
+    assert np.all(err <= RTOL[value_type] * bound[:, 0] + 1e-6 * np.abs(y0) + 1e-30)
