@@ -371,7 +371,14 @@ class DeviceMatrix:
 
     def spmm(self, X, Y, alpha: float = 1.0, beta: float = 0.0, packed: "PackedValues | None" = None,
              stream=None) -> None:
-        """Y <- alpha * A X + beta * Y for k = X.shape[1] right-hand sides."""
+        """Y <- alpha * A X + beta * Y for k = X.shape[1] right-hand sides.
+        A CSR product with one contiguous column runs the single-vector
+        chunked kernel (the fastest CSR kernel; the SpMM kernels split each
+        row's k columns between lanes, which at k = 1 leaves lanes idle)."""
+        if (self.fmt == "csr" and X.dim() == 2 and Y.dim() == 2 and X.shape[1] == 1 and Y.shape[1] == 1
+                and X.is_contiguous() and Y.is_contiguous()):
+            self.spmv(X.view(-1), Y.view(-1), alpha, beta, stream=stream, packed=packed)
+            return
         device_spmm(self, X, Y, alpha, beta, packed, stream)
 
 
