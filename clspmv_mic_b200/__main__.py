@@ -9,10 +9,11 @@
         spmv_cocktail (src/eval.cpp:100-131): read, print the matrix info,
         partition with the benchmark tables of table_dir (default
         $CLSPMVPATH, else the tables shipped with the package), evaluate.
-    python -m clspmv_mic_b200 spmm <b4csr|b4ell|sbell> <k> [reps] [block_rows] [f32|bf16|f16]
+    python -m clspmv_mic_b200 spmm <b4csr|b4ell|sbell|csr|coo> <k> [reps] [block_rows] [f32|bf16|f16]
         Y = A X with k right-hand sides on the synthetic 4x4-block matrix
-        (block_rows x 8 dense blocks, default 500,000): prints the mean time
-        and GFLOP/s. The command the SpMM kernel profiles are taken with.
+        (block_rows x 8 dense blocks, default 500,000) or, for csr / coo, the
+        power-law matrix (2^20 rows): prints the mean time and GFLOP/s. The
+        command the SpMM kernel profiles are taken with.
 """
 from __future__ import annotations
 
@@ -76,9 +77,13 @@ def _spmm(fmt: str, rest: list[str]) -> int:
     reps = int(rest[1]) if len(rest) > 1 else 20
     brows = int(rest[2]) if len(rest) > 2 else 500_000
     vt = rest[3] if len(rest) > 3 else "f32"
-    coo = F.coo_matrix(*synth.block_rows(brows, 8))
-    host = {"b4csr": lambda: F.coo2b4csr(coo, 4, 4), "b4ell": lambda: F.coo2b4ell(coo, 4, 4),
-            "sbell": lambda: F.coo2sbell(coo, 4, 4, 32)}[fmt]()
+    if fmt in ("csr", "coo"):   # the power-law matrix (2^20 rows, Zipf 2.0, mean 16)
+        coo = F.coo_matrix(*synth.powerlaw(1 << 20))
+        host = F.coo2csr(coo) if fmt == "csr" else coo
+    else:
+        coo = F.coo_matrix(*synth.block_rows(brows, 8))
+        host = {"b4csr": lambda: F.coo2b4csr(coo, 4, 4), "b4ell": lambda: F.coo2b4ell(coo, 4, 4),
+                "sbell": lambda: F.coo2sbell(coo, 4, 4, 32)}[fmt]()
     m = F.DeviceMatrix(host)
     rows, cols = m.shape
     g = torch.Generator(device="cuda")

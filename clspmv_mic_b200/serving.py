@@ -8,10 +8,13 @@ Y = alpha * A * X with any k; a loop thread forms batches continuously:
 * requests waiting when a slot frees up are grouped by matrix, and the X
   columns of one matrix's requests are placed side by side, so A is read
   once for all of them (up to 128 columns per job);
-* all fused jobs of the batch run in ONE persistent launch
+* the fused jobs of the batch run in ONE persistent launch
   (clspmv_batch_run); a request that is alone for its matrix runs in that
   format's own load-balanced kernel on the same stream, so a lightly loaded
-  server answers as fast as a plain launch;
+  server answers as fast as a plain launch; registration times a fused
+  product both ways for each matrix and sends that matrix's fused groups to
+  its own kernel when that is faster (long rows split by nonzeros beat the
+  shared launch's row walk; short rows the other way round);
 * `slots` batches can be in flight at once on separate streams, so requests
   that arrive while a batch runs are admitted into the next slot and their
   work overlaps the running batch on the device.
@@ -48,6 +51,7 @@ class Resident:
     packed: Optional[PackedValues]
     nbytes: int
     last_used: float = 0.0
+    standalone: bool = False   # fused groups run the matrix's own SpMM kernel, not the shared launch
 
 
 @dataclass
@@ -72,7 +76,7 @@ class _Flight:
 
 class SpmvServer:
     def __init__(self, budget_bytes: int, slots: int = 2, max_jobs: int = 256, max_requests: int = 1024,
-                 max_batch_bytes: int = 8 << 30, device: str = "cuda"):
+                 max_batch_bytes: int = 8 << 30, device: str = "cuda", tune_k: int = 8):
         import torch
         self.torch = torch
         self.budget = int(budget_bytes)
@@ -81,6 +85,10 @@ class SpmvServer:
         self.device = torch.device("cuda", torch.cuda.current_device()) if dev.index is None else dev
         self.max_requests = max_requests
         self.max_batch_bytes = int(max_batch_bytes)
+        # width of the fused product timed at registration to choose, per
+        # matrix, between the shared persistent launch and the matrix's own
+        # SpMM kernel for its fused groups (0: always the shared launch)
+        self.tune_k = int(tune_k)
         self.mats: dict[str, Resident] = {}
         self._pending: deque[Request] = deque()
         self._cv = threading.Condition()
@@ -104,7 +112,45 @@ class SpmvServer:
                 return False
             self.mats[name] = Resident(name, matrix, packed, nbytes)
             self.used += nbytes
+        if self.tune_k > 0:
+            self.mats[name].standalone = self._standalone_faster(matrix, packed)
         return True
+
+    def _standalone_faster(self, matrix: DeviceMatrix, packed: Optional[PackedValues], reps: int = 3) -> bool:
+        """Times a fused product of `tune_k` columns both ways a group can
+        run (one job of the shared persistent launch, or the matrix's own
+        SpMM kernel) and tells whether the second is faster. Row-walked
+        short rows favour the shared launch; long rows split by nonzeros
+        favour the matrix's kernel."""
+        torch = self.torch
+        m, n = matrix.shape
+        with torch.cuda.device(self.device):
+            X = torch.rand((n, self.tune_k), device=self.device)
+            Y = torch.zeros((m, self.tune_k), device=self.device)
+            b = Batch(1)
+            try:
+                def shared():
+                    b.set([Job(matrix, X, Y, alpha=1.0, beta=1.0, packed=packed)])
+                    b.run()
+
+                def own():
+                    matrix.spmm(X, Y, 1.0, 0.0, packed=packed)
+
+                times = []
+                for fn in (shared, own):
+                    fn()
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(reps):
+                        fn()
+                    e1.record()
+                    torch.cuda.synchronize()
+                    times.append(e0.elapsed_time(e1))
+            finally:
+                b.close()
+            del X, Y
+        return times[1] < times[0]
 
     def unregister(self, name: str) -> None:
         with self._cv:
@@ -210,8 +256,8 @@ class SpmvServer:
                     if Xc.shape[1] % 4 and Xc.shape[1] > 32:
                         Xc = torch.nn.functional.pad(Xc, (0, 4 - Xc.shape[1] % 4))
                     alpha = part[0].alpha if same_alpha else 1.0
-                    if len(part) == 1 or res.matrix.fmt == "coo":
-                        # nothing to fuse: the format's own balanced kernel, on this slot's stream
+                    if len(part) == 1 or res.matrix.fmt == "coo" or res.standalone:
+                        # a lone request, or a matrix whose own kernel is faster: on this slot's stream
                         Yc = torch.empty((m, Xc.shape[1]), dtype=torch.float32, device=Xc.device)
                         res.matrix.spmm(Xc, Yc, alpha, 0.0, packed=res.packed, stream=st)
                     else:
