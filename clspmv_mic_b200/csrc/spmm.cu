@@ -564,6 +564,71 @@ __global__ void __launch_bounds__(kSpmmBlock) k_spmm_seg(int rows, int nnz, cons
         seg_chunk<T, IS_CSR>(rows, nnz, row_ptr, row_id, col_id, vals, d, ch, lane);
 }
 
+// ---------------------------------------------------------------------------
+// Long CSR rows at k a multiple of 4: a warp per row. The warp's lanes form
+// 32 / G nonzero slots of G = k / 4 lanes (4 columns each); a step covers
+// 32 / G consecutive nonzeros of the row with coalesced col_id / value loads
+// and one float4 X load per lane, and the slots' partial sums are combined
+// once per row by shuffles. The row is owned by its warp, so Y is written
+// directly (alpha, beta applied there). Used when rows average
+// kWarpRowMin nonzeros or more: the nonzero-chunk kernel walks a long row's
+// nonzeros one after another per lane group.
+// ---------------------------------------------------------------------------
+constexpr int kWarpRowMin = 128;
+
+template <class T>
+__global__ void __launch_bounds__(kSpmmBlock) k_spmm_warp_rows(int rows, const int* __restrict__ row_ptr,
+                                                               const int* __restrict__ col_id, const T* __restrict__ vals,
+                                                               Dense d)
+{
+    const int lane = threadIdx.x & 31;
+    const int G = d.k >> 2;                     // lanes per nonzero slot, 1..32 (k <= 128)
+    const int lg = 31 - __clz(G);               // G is a power of two (checked by the launcher)
+    const int slots = 32 >> lg;
+    const int slot = lane >> lg, c0 = (lane & (G - 1)) * 4;
+    const long long nwarps = (long long)gridDim.x * (kSpmmBlock / 32);
+    for (long long r = (long long)blockIdx.x * (kSpmmBlock / 32) + (threadIdx.x >> 5); r < rows; r += nwarps) {
+        const int j0 = __ldg(row_ptr + r), j1 = __ldg(row_ptr + r + 1);
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        int j = j0 + slot;
+        // two nonzeros per slot in flight
+        for (; j + slots < j1; j += 2 * slots) {
+            const int ca = __ldg(col_id + j), cb = __ldg(col_id + j + slots);
+            const float va = to_f(ld_val(vals + j)), vb = to_f(ld_val(vals + j + slots));
+            const float4 xa = __ldg(reinterpret_cast<const float4*>(d.X + (size_t)ca * d.ldx + c0));
+            const float4 xb = __ldg(reinterpret_cast<const float4*>(d.X + (size_t)cb * d.ldx + c0));
+            acc.x = fmaf(va, xa.x, acc.x); acc.y = fmaf(va, xa.y, acc.y);
+            acc.z = fmaf(va, xa.z, acc.z); acc.w = fmaf(va, xa.w, acc.w);
+            acc.x = fmaf(vb, xb.x, acc.x); acc.y = fmaf(vb, xb.y, acc.y);
+            acc.z = fmaf(vb, xb.z, acc.z); acc.w = fmaf(vb, xb.w, acc.w);
+        }
+        if (j < j1) {
+            const int ca = __ldg(col_id + j);
+            const float va = to_f(ld_val(vals + j));
+            const float4 xa = __ldg(reinterpret_cast<const float4*>(d.X + (size_t)ca * d.ldx + c0));
+            acc.x = fmaf(va, xa.x, acc.x); acc.y = fmaf(va, xa.y, acc.y);
+            acc.z = fmaf(va, xa.z, acc.z); acc.w = fmaf(va, xa.w, acc.w);
+        }
+        for (int off = 16; off >= G; off >>= 1) {
+            acc.x += __shfl_xor_sync(kWarpAll, acc.x, off);
+            acc.y += __shfl_xor_sync(kWarpAll, acc.y, off);
+            acc.z += __shfl_xor_sync(kWarpAll, acc.z, off);
+            acc.w += __shfl_xor_sync(kWarpAll, acc.w, off);
+        }
+        if (slot == 0) {
+            const float a = d.scale ? d.alpha * d.scale[r] : d.alpha;
+            float4* y = reinterpret_cast<float4*>(d.Y + (size_t)r * d.ldy + c0);
+            float4 o = make_float4(a * acc.x, a * acc.y, a * acc.z, a * acc.w);
+            if (d.beta != 0.0f) {
+                const float4 p = *y;
+                o.x = fmaf(d.beta, p.x, o.x); o.y = fmaf(d.beta, p.y, o.y);
+                o.z = fmaf(d.beta, p.z, o.z); o.w = fmaf(d.beta, p.w, o.w);
+            }
+            *y = o;
+        }
+    }
+}
+
 __global__ void k_scale_rows(float* Y, int rows, int k, int ldy, float beta)
 {
     const long long n = (long long)rows * k;
@@ -679,6 +744,16 @@ int launch_rows(const M& m, const void* vals, Dense d, int vec, cudaStream_t st)
     return after_launch(1);
 }
 
+// CLSPMV_SPMM_WARP_ROWS=0 keeps the nonzero-chunk kernel for long CSR rows (measurements).
+bool warp_rows_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("CLSPMV_SPMM_WARP_ROWS");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 // CLSPMV_SPMM_SEG=0 keeps the nonzero-chunk kernel for CSR / COO (measurements).
 bool seg_enabled()
 {
@@ -727,6 +802,15 @@ int spmm_typed(int format, const void* dev, const void* vals, Dense d, int vec, 
         case CLSPMV_FORMAT_CSR: {
             const auto& m = *static_cast<const clspmv_csr_f32*>(dev);
             if (!m.csr_row_ptr) return CLSPMV_ERR_ARG;
+            const int G = d.k / 4;
+            if (vec == 4 && (G & (G - 1)) == 0 && m.matinfo.height > 0 &&
+                (long long)m.matinfo.nnz >= (long long)kWarpRowMin * m.matinfo.height && warp_rows_enabled()) {
+                const long long warps = m.matinfo.height;
+                const int grid = (int)std::min<long long>((warps + kSpmmBlock / 32 - 1) / (kSpmmBlock / 32), 148LL * 16);
+                k_spmm_warp_rows<T><<<grid, kSpmmBlock, 0, st>>>(m.matinfo.height, m.csr_row_ptr, m.csr_col_id,
+                                                                 static_cast<const T*>(vals ? vals : m.csr_data), d);
+                return after_launch(1);
+            }
             return launch_chunks<T, true>(m.matinfo.height, m.matinfo.nnz, m.csr_row_ptr, nullptr, m.csr_col_id,
                                           vals ? vals : m.csr_data, d, vec, st);
         }

@@ -248,13 +248,17 @@ class SpmvServer:
                         st.wait_event(r.ready)
                     same_alpha = all(r.alpha == part[0].alpha for r in part)
                     if len(part) > 1:
-                        Xc = torch.cat([r.X for r in part], dim=1)
+                        # fused columns padded with zeros to a multiple of 4: the 16-byte row
+                        # kernels (warp per long row, float4 gathers) need it
+                        srcs = [r.X if same_alpha else r.X * r.alpha for r in part]
+                        pad = -sum(x.shape[1] for x in srcs) % 4
+                        if pad:
+                            srcs.append(torch.zeros((srcs[0].shape[0], pad), dtype=torch.float32, device=srcs[0].device))
+                        Xc = torch.cat(srcs, dim=1)
                     else:   # a lone request's X is used in place (any row stride)
                         Xc = part[0].X if part[0].X.stride(1) == 1 else part[0].X.contiguous()
-                    if not same_alpha:
-                        Xc = torch.cat([r.X * r.alpha for r in part], dim=1)
-                    if Xc.shape[1] % 4 and Xc.shape[1] > 32:
-                        Xc = torch.nn.functional.pad(Xc, (0, 4 - Xc.shape[1] % 4))
+                        if Xc.shape[1] % 4 and Xc.shape[1] > 32:
+                            Xc = torch.nn.functional.pad(Xc, (0, 4 - Xc.shape[1] % 4))
                     alpha = part[0].alpha if same_alpha else 1.0
                     if len(part) == 1 or res.matrix.fmt == "coo" or res.standalone:
                         # a lone request, or a matrix whose own kernel is faster: on this slot's stream

@@ -191,3 +191,27 @@ def test_csr_packed_both_kernels(value_type, variant):
     ref, bound = spmm_reference(coo, x[:, None], y0[:, None], 0.5, 1.0)
     err = np.abs(yd.cpu().numpy().astype(np.float64) - ref[:, 0])
     assert np.all(err <= RTOL[value_type] * bound[:, 0] + 1e-6 * np.abs(y0) + 1e-30)
+
+
+@pytest.mark.parametrize("k", [4, 8, 16, 32, 64])
+@pytest.mark.parametrize("value_type", ["f32", "bf16"])
+def test_csr_long_rows_warp_kernel(k, value_type):
+    """CSR rows averaging 128 or more nonzeros take the warp-per-row kernel
+    at k a power of two times 4: against the FP64 oracle, with alpha / beta,
+    empty rows included."""
+    import torch
+    coo = F.coo_matrix(*synth.random_coo(300, 4000, 0.08, seed=21, empty_row_frac=0.1))
+    assert coo.nnz >= 128 * coo.shape[0]
+    m, n = coo.shape
+    dev = device_of(coo, "csr")
+    p = None if value_type == "f32" else dev.pack(value_type)
+    rng = np.random.default_rng(k)
+    X = rng.uniform(-1, 1, (n, k)).astype(np.float32)
+    Y0 = rng.uniform(-1, 1, (m, k)).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (0.5, -1.5)]:
+        Xd, Yd = torch.from_numpy(X).cuda(), torch.from_numpy(Y0.copy()).cuda()
+        dev.spmm(Xd, Yd, alpha, beta, packed=p)
+        torch.cuda.synchronize()
+        ref, bound = spmm_reference(coo, X, Y0, alpha, beta)
+        err = np.abs(Yd.cpu().numpy().astype(np.float64) - ref)
+        assert np.all(err <= RTOL[value_type] * bound + 1e-6 * abs(beta) * np.abs(Y0) + 1e-30), (k, value_type, alpha, beta)
