@@ -466,7 +466,11 @@ typedef enum { CLSPMV_VALUES_F32 = 0, CLSPMV_VALUES_BF16 = 1, CLSPMV_VALUES_F16 
  * `row_scale` ignored); BF16 / F16 use the 16-bit array and per-row scales
  * made by clspmv_pack_values. CSR and COO must be row sorted; their rows
  * cut between work chunks are added atomically, so the last bits of Y may
- * differ between runs (within the FP32 bound). */
+ * differ between runs (within the FP32 bound). Kernel by case: at k = 4
+ * (16-byte rows) CSR / COO take a warp per 256 nonzeros with a segmented
+ * reduction; CSR rows averaging >= 128 nonzeros at k = 4 * 2^j take a warp
+ * per row; otherwise lane groups per nonzero chunk (CSR / COO) or per row
+ * (the other formats). */
 int clspmv_spmm(int format, const void* dev, int value_type, const void* values, const float* row_scale, int k,
                 const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
 
