@@ -714,8 +714,13 @@ def run_extras(args, items, mats, peak):
     entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_chunk", "bcsr", "sbell")
                if k in by_key]
     out["spmm"] = {"note": "Y = A X, beta 0; GB/s over matrix bytes at the stored value width + k (4n + 4m); "
-                           "err_fp64 = max |Y - Y64| / (|A| |X|); CUDA cores (no tensor-core path)",
+                           "err_fp64 = max |Y - Y64| / (|A| |X|); CUDA-core kernels",
                    "results": W.spmm_sweep(entries, hbm_gbs=peak)}
+    if "bcsr" in by_key:
+        out["spmm_tc"] = {"note": "b4csr 4x4 blocks (500k block rows x 8), Y = A X: tcgen05 kind::tf32 with a "
+                                  "head/remainder split of A and X (FP32 accuracy) against the CUDA-core kernel",
+                          "results": W.spmm_tc_sweep(by_key["bcsr"]["dev"], csr64[by_key["bcsr"]["matrix"]],
+                                                     hbm_gbs=peak)}
     del csr64, entries
     torch.cuda.empty_cache()
     out["spmm"]["seconds"] = round(time.perf_counter() - t0, 1)

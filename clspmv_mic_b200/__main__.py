@@ -9,11 +9,12 @@
         spmv_cocktail (src/eval.cpp:100-131): read, print the matrix info,
         partition with the benchmark tables of table_dir (default
         $CLSPMVPATH, else the tables shipped with the package), evaluate.
-    python -m clspmv_mic_b200 spmm <b4csr|b4ell|sbell|csr|coo> <k> [reps] [block_rows] [f32|bf16|f16]
+    python -m clspmv_mic_b200 spmm <b4csr|b4ell|sbell|csr|coo> <k> [reps] [block_rows] [f32|bf16|f16|tc]
         Y = A X with k right-hand sides on the synthetic 4x4-block matrix
         (block_rows x 8 dense blocks, default 500,000) or, for csr / coo, the
-        power-law matrix (2^20 rows): prints the mean time and GFLOP/s. The
-        command the SpMM kernel profiles are taken with.
+        power-law matrix (2^20 rows): prints the mean time and GFLOP/s. "tc"
+        runs b4csr on the tensor cores (FP32 values). The command the SpMM
+        kernel profiles are taken with.
 """
 from __future__ import annotations
 
@@ -90,17 +91,24 @@ def _spmm(fmt: str, rest: list[str]) -> int:
     g.manual_seed(5)
     X = torch.rand((cols, k), generator=g, device="cuda") * 2 - 1
     Y = torch.empty((rows, k), device="cuda")
-    p = None if vt == "f32" else m.pack(vt)
+    if vt == "tc":
+        run = lambda: F.device_spmm_tc(m, X, Y, 1.0, 0.0)
+    else:
+        p = None if vt == "f32" else m.pack(vt)
+        run = lambda: m.spmm(X, Y, 1.0, 0.0, packed=p)
     for _ in range(3):
-        m.spmm(X, Y, 1.0, 0.0, packed=p)
+        run()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(reps):
-        m.spmm(X, Y, 1.0, 0.0, packed=p)
+        run()
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
     print(f"{fmt} k={k} {vt}: {ms:.4f} ms, {2.0 * m.nnz * k / (ms * 1e-3) / 1e9:.1f} GFLOP/s")
+    if vt == "tc" and F.tensor_timeouts():
+        print("tensor-core kernel: a bounded wait ran out")
+        return 1
     return 0
 
 

@@ -242,6 +242,8 @@ def _declare(lib):
                                                P(C.c_double)]),
         "clspmv_read_mmf_f32": (I32, [C.c_char_p, S["coo"]]),
         "clspmv_spmm": (I32, [I32, VP, I32, VP, VP, I32, VP, I32, VP, I32, f32, f32, VP]),
+        "clspmv_b4csr_spmm_tc_f32": (I32, [VP, I32, VP, I32, VP, I32, f32, f32, VP]),
+        "clspmv_tensor_timeouts": (I32, [P(C.c_uint)]),
         "clspmv_stored_values": (I32, [I32, VP, P(C.c_size_t)]),
         "clspmv_spmv_packed": (I32, [I32, VP, I32, VP, VP, VP, VP, VP, f32, f32, VP]),
         "clspmv_sell_plan_create": (I32, [S["sell"], P(VP)]),

@@ -531,5 +531,27 @@ def device_spmm(m: "DeviceMatrix", X, Y, alpha: float = 1.0, beta: float = 0.0, 
                             Y.data_ptr(), Y.stride(0), alpha, beta, _stream_handle(stream)), "spmm")
 
 
+def device_spmm_tc(m: "DeviceMatrix", X, Y, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+    """Y <- alpha * A X + beta * Y for a b4csr matrix of 4 x 4 blocks on the
+    tensor cores (tcgen05, TF32 head and remainder of every value, FP32
+    accumulation); k = X.shape[1] a multiple of 16 up to 128."""
+    if m.fmt != "b4csr":
+        raise ValueError("the tensor-core product takes b4csr matrices")
+    if X.dim() != 2 or Y.dim() != 2 or X.stride(1) != 1 or Y.stride(1) != 1:
+        raise ValueError("X and Y must be 2-D with unit column stride")
+    k = X.shape[1]
+    if Y.shape[1] != k or X.shape[0] < m.shape[1] or Y.shape[0] < m.shape[0]:
+        raise ValueError("shape mismatch")
+    check(lib().clspmv_b4csr_spmm_tc_f32(C.byref(m.struct), k, X.data_ptr(), X.stride(0), Y.data_ptr(), Y.stride(0),
+                                         alpha, beta, _stream_handle(stream)), "spmm_tc")
+
+
+def tensor_timeouts() -> int:
+    """Bounded waits of the tensor-core kernels that ran out since the last call (synchronous; resets)."""
+    n = C.c_uint(0)
+    check(lib().clspmv_tensor_timeouts(C.byref(n)), "tensor_timeouts")
+    return int(n.value)
+
+
 def launch_count() -> int:
     return int(lib().clspmv_launch_count())

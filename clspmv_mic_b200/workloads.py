@@ -125,6 +125,44 @@ def spmm_sweep(entries, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), r
     return out
 
 
+def spmm_tc_sweep(m, A64, ks=(16, 32, 64), reps: int = 10, hbm_gbs=None):
+    """A b4csr matrix of 4 x 4 blocks times k right-hand sides (beta 0) on
+    the tensor cores (tcgen05, TF32 head and remainder) and in the CUDA-core
+    lane-group kernel, per k: time, GFLOP/s, GB/s over matrix bytes +
+    k (4n + 4m), error against FP64."""
+    import torch
+    from . import formats as F
+    out = {}
+    rows, cols = m.shape
+    nnz = int(m.nnz)
+    rng = torch.Generator(device="cuda")
+    rng.manual_seed(6)
+    for k in ks:
+        X = torch.rand((cols, k), generator=rng, device="cuda") * 2 - 1
+        Y = torch.empty((rows, k), device="cuda")
+        runs = {"tensor_cores": lambda: F.device_spmm_tc(m, X, Y, 1.0, 0.0), "cuda_cores": lambda: m.spmm(X, Y, 1.0, 0.0)}
+        for name, run in runs.items():
+            for _ in range(3):
+                run()
+            e0, e1 = _events(torch)
+            e0.record()
+            for _ in range(reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            ab = matrix_bytes(m, "f32") + k * (4 * cols + 4 * rows)
+            r = dict(ms=round(ms, 4), gflops=round(2.0 * nnz * k / (ms * 1e-3) / 1e9, 1),
+                     gbs=round(ab / (ms * 1e-3) / 1e9, 1), err_fp64=fp64_error(A64, X, Y, rows=min(rows, 1 << 18)))
+            if hbm_gbs:
+                r["frac"] = round(r["gbs"] / hbm_gbs, 3)
+            out[f"k{k}/{name}"] = r
+        out[f"k{k}/tensor_speedup"] = round(out[f"k{k}/cuda_cores"]["ms"] / out[f"k{k}/tensor_cores"]["ms"], 3)
+        del X, Y
+    out["timeouts"] = F.tensor_timeouts()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # Batches of uneven matrices (one persistent launch, captured in a graph)
 # ---------------------------------------------------------------------------

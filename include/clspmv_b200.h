@@ -485,6 +485,20 @@ int clspmv_b4csr_spmm_f32(const clspmv_b4csr_f32* dev, int k, const float* X, in
 int clspmv_b4ell_spmm_f32(const clspmv_b4ell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
 int clspmv_sbell_spmm_f32(const clspmv_sbell_f32* dev, int k, const float* X, int ldx, float* Y, int ldy, float alpha, float beta, clspmv_stream_t stream);
 
+/* clspmv_b4csr_spmm_f32 on the tensor cores (tcgen05.mma kind::tf32,
+ * accumulators in tensor memory), for 4 x 4 blocks and k a multiple of 16 up
+ * to 128 (CLSPMV_ERR_UNSUPPORTED otherwise). Every value of A and X is split
+ * into a TF32 head and its remainder, so the products keep FP32 accuracy
+ * (about 2^-21 of sum |a x|). X 16-byte aligned with ldx a multiple of 4
+ * (CLSPMV_ERR_ALIGN otherwise); Y has no alignment rule. Up to 64 right-hand
+ * sides per launch. */
+int clspmv_b4csr_spmm_tc_f32(const clspmv_b4csr_f32* dev, int k, const float* X, int ldx, float* Y, int ldy,
+                             float alpha, float beta, clspmv_stream_t stream);
+/* Number of bounded device waits in the tensor-core kernels that ran out
+ * since the last call (each ends its kernel early with Y incomplete);
+ * synchronous, resets the count. */
+int clspmv_tensor_timeouts(unsigned int* count);
+
 /* Number of stored values (padding included) of the device matrix, i.e. the
  * length of its value array; reads one int from the device for BDIA, SELL
  * and SBELL. */
