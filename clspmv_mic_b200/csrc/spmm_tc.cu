@@ -18,32 +18,32 @@
 // |a x| (lo is rounded to TF32 once more: 2^-11 of 2^-11).
 //
 // Shared-memory operands (no swizzle, canonical core matrices of 8 rows x
-// 16 bytes):
-//   A (M = 64 right-hand sides x K = 8), K-major: element (j, kk) at
+// 16 bytes, both K-major):
+//   A (M = 64 right-hand sides x K = 8): element (j, kk) at
 //     (j / 8) * 256 + (kk / 4) * 128 + (j % 8) * 16 + (kk % 4) * 4; only
 //     j < KC is written, the rest of the 2 KB a descriptor spans belongs to
 //     the next block's slice and only feeds accumulator lanes that are never
-//     read. A lane loads four consecutive right-hand sides of one X row, so
-//     the four lanes holding rows 0-3 of a slice swap elements (a 4 x 4
-//     transpose by shuffles) and each stores one right-hand side's four
-//     columns. (MN-major TF32 operands without swizzle, which would take the
-//     X rows as loaded, read as zeros on sm_100a.)
-//   B (K = 8 x N = 8), K-major: element (kk, n) at (kk / 4) * 128 + n * 16 +
+//     read. Lane j of a slice loads X[4 bc + 0..3][j] (four coalesced scalar
+//     loads, one per X row) and stores its head and remainder as two 16-byte
+//     rows, so no transpose is needed. (MN-major TF32 operands without
+//     swizzle, which would take the X rows as loaded, read as zeros on
+//     sm_100a.)
+//   B (K = 8 x N = 8): element (kk, n) at (kk / 4) * 128 + n * 16 +
 //     (kk % 4) * 4, i.e. [hi rows | lo rows] twice (the x_hi and x_lo halves
 //     of K see the same block).
 // Accumulators: a tile of 32 block rows owns 8 tensor-memory columns per
-// block row (256 columns per CTA, two CTAs per SM); right-hand side j sits in
-// lane (j % 16) + 32 * (j / 16), the M = 64 layout, so warp w reads columns
-// 16w .. 16w + 15 back with tcgen05.ld.
+// block row (256 columns per CTA, at most two CTAs per SM); right-hand side j
+// sits in lane (j % 16) + 32 * (j / 16), the M = 64 layout, so warp w < 4
+// reads right-hand sides 16w .. 16w + 15 back with tcgen05.ld.
 //
-// Pipeline per CTA (4 warps): each step gathers 16 blocks (4 per warp) — the
+// Pipeline per CTA (8 warps): each step gathers 32 blocks (4 per warp) — the
 // block's column id, its four value rows and its 4 x KC slice of X, loaded a
 // step ahead into registers — splits them into (hi, lo) while writing the
-// stage's operands, and thread 0 issues the 16 MMAs and commits them to the
-// stage's mbarrier, which the producers wait on before they reuse the stage
-// (four stages). Every wait is bounded (about 2 s on %globaltimer); a wait
-// that runs out ends the kernel cleanly, tensor memory released, and is
-// counted in a device word that clspmv_tensor_timeouts reads.
+// stage's operands, and thread 0 issues the 32 MMAs and commits them to the
+// stage's mbarrier, which the producers wait on before they reuse the stage.
+// Every wait is bounded (about 2 s on %globaltimer); a wait that runs out
+// ends the kernel cleanly, tensor memory released, and is counted in a device
+// word that clspmv_tensor_timeouts reads.
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
@@ -55,12 +55,12 @@ using namespace clspmv;
 
 namespace {
 
-constexpr int kTcThreads = 128;
-constexpr int kTcTileRows = 32;   // block rows per tile, 8 tensor-memory columns each
-constexpr int kTcCols = 256;      // tensor-memory columns per CTA
-constexpr int kTcPer = 16;        // blocks per pipeline step, 4 per warp
-constexpr int kTcStages = 4;
-constexpr int kTcMaxKc = 64;      // right-hand sides per pass (MMA M = 64)
+constexpr int kTcWarps = 8;
+constexpr int kTcThreads = 32 * kTcWarps;
+constexpr int kTcTileRows = 32;            // block rows per tile, 8 tensor-memory columns each
+constexpr int kTcCols = 256;               // tensor-memory columns per CTA
+constexpr int kTcPer = 4 * kTcWarps;       // blocks per pipeline step, 4 per warp
+constexpr int kTcMaxKc = 64;               // right-hand sides per pass (MMA M = 64)
 constexpr unsigned kFullMask = 0xffffffffu;
 
 // Instruction descriptor: D F32 (bits 4-5 = 1), A TF32 (7-9 = 2), B TF32
@@ -70,20 +70,28 @@ constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 17) | (4
 
 __device__ unsigned int g_tc_timeouts;
 
+// Pipeline stages: as many as keep two CTAs (2 x 256 of the 512
+// tensor-memory columns) on an SM for k <= 32, three above.
+template <int KC> constexpr int tc_stages() { return KC == 16 ? 3 : KC == 32 ? 2 : 3; }
+
 template <int KC>
 struct TcSmem {
+    static constexpr int kStages = tc_stages<KC>();
     static constexpr int kATile = KC * 32;            // KC / 8 groups of 8 rows x 32 bytes
     static constexpr int kAStage = kTcPer * kATile;
-    static constexpr int kAPad = 2048;                // an M = 64 descriptor spans 16 core matrices
+    static constexpr int kAPad = 2048;                // an M = 64 descriptor spans 2 KB from its start
     static constexpr int kBTile = 256;
     static constexpr int kBStage = kTcPer * kBTile;
     static constexpr int kA = 0;
-    static constexpr int kB = kA + kTcStages * kAStage + kAPad;
-    static constexpr int kMeta = kB + kTcStages * kBStage;
-    static constexpr int kPtr = kMeta + kTcStages * kTcPer * 4;
+    static constexpr int kB = kA + kStages * kAStage + kAPad;
+    static constexpr int kMeta = kB + kStages * kBStage;
+    static constexpr int kPtr = kMeta + kStages * kTcPer * 4;
     static constexpr int kBar = (kPtr + (kTcTileRows + 1) * 4 + 7) / 8 * 8;
-    static constexpr int kTmem = kBar + kTcStages * 8;
+    static constexpr int kTmem = kBar + kStages * 8;
     static constexpr int kBytes = kTmem + 16;
+    // at least 80 KB so that no third CTA (without tensor-memory columns) lands on an SM
+    static constexpr int kLaunch = kBytes > 80 * 1024 ? kBytes : 80 * 1024;
+    static constexpr int kPerSm = 2 * (kLaunch + 1024) <= 228 * 1024 ? 2 : 1;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -93,25 +101,6 @@ __device__ __forceinline__ float tf32_rna(float v)
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
     return __uint_as_float(r);
-}
-
-// Lanes 4t .. 4t+3 hold rows 0-3 of four right-hand sides (v = X[c][j0 .. j0+3]
-// in lane 4t + c); afterwards lane 4t + c holds X[0..3][j0 + c].
-__device__ __forceinline__ float4 quad_transpose(float4 v)
-{
-    const int c = threadIdx.x & 3, base = threadIdx.x & 28;
-    float w0 = 0.f, w1 = 0.f, w2 = 0.f, w3 = 0.f;
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const int si = (c - s) & 3, ri = (c + s) & 3;   // send element c - s, receive row c + s's element c
-        const float send = si == 0 ? v.x : si == 1 ? v.y : si == 2 ? v.z : v.w;
-        const float got = __shfl_sync(kFullMask, send, base | ri);
-        w0 = ri == 0 ? got : w0;
-        w1 = ri == 1 ? got : w1;
-        w2 = ri == 2 ? got : w2;
-        w3 = ri == 3 ? got : w3;
-    }
-    return make_float4(w0, w1, w2, w3);
 }
 
 __device__ __forceinline__ void split4(float4 v, float4& hi, float4& lo)
@@ -202,12 +191,13 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// One step's loads for one lane: its share of the warp's four X slices
-// (KC float4 per block), and for lanes 0-15 row (lane & 3) of block
+// One step's loads for one lane: for the warp's four blocks, KC / 8 (block,
+// right-hand side) pairs e = lane + 32 i, each the four X rows of the block's
+// slice at that right-hand side; lanes 0-15 also load row (lane & 3) of block
 // (lane >> 2).
 template <int KC>
 struct StepLoads {
-    float4 x[KC / 8];
+    float x[KC / 2];
     float4 v;
 };
 
@@ -219,14 +209,17 @@ __device__ __forceinline__ void load_step(StepLoads<KC>& f, int col_lane, int gw
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int i = 0; i < KC / 8; i++) {
-        const int e = lane + 32 * i, q = e / KC, rem = e % KC, c = rem & 3, jg = rem >> 2;
+        const int e = lane + 32 * i, q = e / KC, j = e % KC;
         const int c4 = __shfl_sync(kFullMask, col_lane, q);
-        const int xr = 4 * c4 + c;
-        f.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (gw + q < b1 && xr < width) f.x[i] = ld_x4(X + (size_t)xr * ldx + 4 * jg, pl);
+        const bool ok = gw + q < b1;
+        const float* xp = X + (size_t)(4 * c4) * ldx + j;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            f.x[4 * i + c] = (ok && 4 * c4 + c < width) ? ld_x(xp + (size_t)c * ldx, pl) : 0.f;
     }
     f.v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (lane < 16 && gw + (lane >> 2) < b1) f.v = ld_stream_f4(data + (size_t)(lane & 3) * len + 4 * (size_t)(gw + (lane >> 2)), pe);
+    if (lane < 16 && gw + (lane >> 2) < b1)
+        f.v = ld_stream_f4(data + (size_t)(lane & 3) * len + 4 * (size_t)(gw + (lane >> 2)), pe);
 }
 
 __device__ __forceinline__ int load_col(const int* __restrict__ col, int gw, int b1, uint64_t pe)
@@ -243,6 +236,7 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
                                                               int ntiles)
 {
     using S = TcSmem<KC>;
+    constexpr int kStages = S::kStages;
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = smem_addr(smem);
@@ -251,7 +245,7 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
     const uint32_t bar0 = sbase + S::kBar;
 
     if (tid == 0) {
-        for (int s = 0; s < kTcStages; s++) mbar_init(bar0 + 8 * s, 1);
+        for (int s = 0; s < kStages; s++) mbar_init(bar0 + 8 * s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -266,7 +260,7 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(smem + S::kTmem);
 
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
-    unsigned it = 0;     // steps this CTA has run; stage = it % kTcStages
+    unsigned it = 0;     // steps this CTA has run; stage = it % kStages
     bool bad = false;    // a bounded wait ran out (the same on every thread)
     for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x) {
         const int br0 = tile * kTcTileRows;
@@ -284,8 +278,8 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
             if (nsteps > 1) col_next = load_col(col, gw + kTcPer, b1, pe);
         }
         for (int step = 0; step < nsteps; step++, it++) {
-            const int s = (int)(it % kTcStages);
-            const unsigned use = it / kTcStages;
+            const int s = (int)(it % kStages);
+            const unsigned use = it / kStages;
             bool late = false;
             if (use > 0) late = !mbar_wait(bar0 + 8 * s, (use - 1) & 1);   // the stage's previous MMAs are done
             late = __any_sync(kFullMask, late);   // the shuffles below need the whole warp
@@ -295,11 +289,10 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
             if (!late) {
 #pragma unroll
                 for (int i = 0; i < KC / 8; i++) {
-                    const int e = lane + 32 * i, q = e / KC, rem = e % KC, j = rem;   // the quad's 4 lanes share q
-                    const float4 xt = quad_transpose(cur.x[i]);                       // X[0..3][j] (j = 4 jg + c)
+                    const int e = lane + 32 * i, q = e / KC, j = e % KC;
                     if (gw + q < b1) {
                         float4 hi, lo;
-                        split4(xt, hi, lo);
+                        split4(make_float4(cur.x[4 * i], cur.x[4 * i + 1], cur.x[4 * i + 2], cur.x[4 * i + 3]), hi, lo);
                         unsigned char* t = as + (4 * warp + q) * S::kATile + (j >> 3) * 256 + (j & 7) * 16;
                         *reinterpret_cast<float4*>(t) = hi;
                         *reinterpret_cast<float4*>(t + 128) = lo;
@@ -342,12 +335,14 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
             }
             if (tid == 0) {
                 tc_fence_after();
-                const uint32_t a0 = sbase + S::kA + s * S::kAStage, bb = sbase + S::kB + s * S::kBStage;
+                // descriptors of the stage's first tiles; the next tiles are whole 16-byte steps further
+                const uint64_t ad = smem_desc(sbase + S::kA + s * S::kAStage, 128, 256);
+                const uint64_t bd = smem_desc(sbase + S::kB + s * S::kBStage, 128, 256);
                 for (int b = 0; b < kTcPer; b++) {
                     const int m = meta[s * kTcPer + b];
                     if (m & 512)
-                        tc_mma(tmem + (uint32_t)(m & 255) * 8, smem_desc(a0 + b * S::kATile, 128, 256),
-                               smem_desc(bb + b * S::kBTile, 128, 256), kIdesc, (m & 256) ? 0u : 1u);
+                        tc_mma(tmem + (uint32_t)(m & 255) * 8, ad + (uint64_t)(b * (S::kATile >> 4)),
+                               bd + (uint64_t)(b * (S::kBTile >> 4)), kIdesc, (m & 256) ? 0u : 1u);
                 }
                 tc_commit(bar0 + 8 * s);
             }
@@ -358,14 +353,14 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
         bool late = false;
         if (nsteps > 0) {
             const unsigned last = it - 1;
-            late = !mbar_wait(bar0 + 8 * (last % kTcStages), (last / kTcStages) & 1);
+            late = !mbar_wait(bar0 + 8 * (last % kStages), (last / kStages) & 1);
         }
         if (__syncthreads_or(late)) {
             bad = true;
             break;
         }
         tc_fence_after();
-        if (warp * 16 < KC) {
+        if (warp * 16 < KC) {   // warps 0-3: lane quarter w holds right-hand sides 16w .. 16w + 15
             const int j = warp * 16 + (lane & 15);
             for (int lr0 = 0; lr0 < nbr; lr0 += 4) {
                 float d[32];
@@ -397,7 +392,7 @@ __global__ void __launch_bounds__(kTcThreads) k_b4csr_spmm_tc(int nbrow, int row
     if (bad && tid == 0) {
         atomicAdd(&g_tc_timeouts, 1u);
         // give MMAs still in flight a bounded chance to finish before the columns are released
-        if (it > 0) mbar_wait(bar0 + 8 * ((it - 1) % kTcStages), ((it - 1) / kTcStages) & 1);
+        if (it > 0) mbar_wait(bar0 + 8 * ((it - 1) % kStages), ((it - 1) / kStages) & 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -420,23 +415,16 @@ template <int KC>
 int launch_tc(const clspmv_b4csr_f32& m, const float* X, int ldx, float* Y, int ldy, float alpha, float beta,
               cudaStream_t st)
 {
-    // at least 80 KB so that no more than two CTAs (2 x 256 of the 512 tensor-memory columns) share an SM
-    constexpr int kSmem = TcSmem<KC>::kBytes > 80 * 1024 ? TcSmem<KC>::kBytes : 80 * 1024;
+    using S = TcSmem<KC>;
     static const cudaError_t attr =
-        cudaFuncSetAttribute(k_b4csr_spmm_tc<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+        cudaFuncSetAttribute(k_b4csr_spmm_tc<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kLaunch);
     if (attr != cudaSuccess) return CLSPMV_ERR_CUDA;
-    static const int per_sm = [] {
-        int n = 1;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_b4csr_spmm_tc<KC>, kTcThreads, kSmem) != cudaSuccess)
-            n = 1;
-        return std::max(1, std::min(n, 2));
-    }();
     const int ntiles = (m.b4csr_row_num + kTcTileRows - 1) / kTcTileRows;
-    const int grid = std::max(1, std::min(ntiles, sm_count() * per_sm));
-    k_b4csr_spmm_tc<KC><<<grid, kTcThreads, kSmem, st>>>(m.b4csr_row_num, m.matinfo.height, m.matinfo.width,
-                                                         m.b4csr_row_ptr, m.b4csr_col_id, m.b4csr_data,
-                                                         (size_t)m.b4csr_aligned_size, X, ldx, Y, ldy, alpha, beta,
-                                                         ntiles);
+    const int grid = std::max(1, std::min(ntiles, sm_count() * S::kPerSm));
+    k_b4csr_spmm_tc<KC><<<grid, kTcThreads, S::kLaunch, st>>>(m.b4csr_row_num, m.matinfo.height, m.matinfo.width,
+                                                              m.b4csr_row_ptr, m.b4csr_col_id, m.b4csr_data,
+                                                              (size_t)m.b4csr_aligned_size, X, ldx, Y, ldy, alpha, beta,
+                                                              ntiles);
     return after_launch(1);
 }
 
