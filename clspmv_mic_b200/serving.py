@@ -26,6 +26,9 @@ alone, the same values may be summed in another order (CSR splits rows by
 nonzeros, k = 1 uses the format's single-vector kernel)
 (tests/test_serving_gpu.py).
 
+ShardedServer runs one such server per GPU of a node, with every matrix
+resident whole on one device and its requests routed there.
+
 The reference has no serving path; its runtime runs one matrix per call and
 waits for it (src/spmv_cocktail.cpp:1088-1132).
 """
@@ -344,3 +347,123 @@ def latency_stats(requests: list) -> dict:
     span = max(r.t_done for r in requests) - min(r.t_submit for r in requests)
     return dict(requests=len(requests), p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
                 mean_ms=float(lat.mean()), req_per_s=len(requests) / span if span > 0 else float("inf"))
+
+
+# ---------------------------------------------------------------------------
+# Several GPUs of one node: matrices placed whole, requests routed, no exchange
+# ---------------------------------------------------------------------------
+def resident_bytes(host, value_type: Optional[str] = None) -> int:
+    """Device bytes a host matrix takes once registered: its arrays as
+    uploaded, plus the 16-bit values (2 bytes per stored value) and per-row
+    scales of the packed copy when `value_type` is "bf16" / "f16"."""
+    nbytes = int(host.stored_bytes())
+    if value_type is not None:
+        values = sum(a.nbytes for k, a in host.arrays().items() if k.endswith("_data"))
+        nbytes += values // 2 + 4 * int(host.shape[0])
+    return nbytes
+
+
+def place(sizes: dict, budgets: list) -> dict:
+    """Whole matrices onto devices: largest first, each onto the device with
+    the most budget left, if it fits there (longest-processing-time greedy,
+    which keeps the most loaded device within one matrix of the best split).
+    Returns name -> device index; names that fit on no device are left out."""
+    free = [int(b) for b in budgets]
+    out = {}
+    for name, nbytes in sorted(sizes.items(), key=lambda kv: (-kv[1], str(kv[0]))):
+        dev = max(range(len(free)), key=lambda i: (free[i], -i))
+        if free[dev] >= nbytes:
+            out[name] = dev
+            free[dev] -= nbytes
+    return out
+
+
+def _upload(host, device, value_type: Optional[str]):
+    import torch
+    with torch.cuda.device(torch.device(device)):
+        m = DeviceMatrix(host, device=device)
+        return m, (m.pack(value_type) if value_type is not None else None)
+
+
+class ShardedServer:
+    """Serving on the GPUs of one node as independent units: each matrix is
+    resident whole on one device, its requests go to that device's
+    SpmvServer (own loop thread, streams and batches), and nothing crosses
+    between devices except a request's X when the caller made it on another
+    one. A matrix goes to the device with the most budget left that fits it,
+    so devices fill evenly; registration past every device's budget is
+    refused. With one device it is one SpmvServer.
+
+    `make_server(device)` and `upload(host, device, value_type)` default to
+    SpmvServer(budget_per_device, device=..., **server_kw) built on that
+    device and to DeviceMatrix(host, device) (+ its packed copy)."""
+
+    def __init__(self, budget_per_device: int, devices=None, make_server=None, upload=None, **server_kw):
+        if devices is None:
+            import torch
+            devices = [f"cuda:{i}" for i in range(torch.cuda.device_count())]
+        self.devices = list(devices)
+        if not self.devices:
+            raise ValueError("no devices to serve on")
+        if make_server is None:
+            def make_server(dev):
+                import torch
+                with torch.cuda.device(torch.device(dev)):   # the server's batches live on its device
+                    return SpmvServer(budget_per_device, device=dev, **server_kw)
+        self.servers = [make_server(d) for d in self.devices]
+        self._upload = upload or _upload
+        self.owner: dict = {}
+        self._lock = threading.Lock()
+
+    def free_bytes(self) -> list:
+        return [s.budget - s.used for s in self.servers]
+
+    def register(self, name: str, host, value_type: Optional[str] = None) -> Optional[int]:
+        """Uploads `host` to the device with the most budget left and keeps it
+        resident there; returns that device's index, or None (nothing kept)
+        when it fits no device."""
+        need = resident_bytes(host, value_type)
+        with self._lock:
+            if name in self.owner:
+                raise KeyError(f"{name} is already registered")
+            free = self.free_bytes()
+            dev = max(range(len(free)), key=lambda i: (free[i], -i))
+            if free[dev] < need:
+                return None
+            matrix, packed = self._upload(host, self.devices[dev], value_type)
+            if not self.servers[dev].register(name, matrix, packed):
+                return None
+            self.owner[name] = dev
+        return dev
+
+    def unregister(self, name: str) -> None:
+        with self._lock:
+            dev = self.owner.pop(name)
+        self.servers[dev].unregister(name)
+
+    def submit(self, name: str, X, alpha: float = 1.0, keep_result: bool = True) -> Future:
+        """Routes Y = alpha * A_name * X to the device holding A_name; the
+        future resolves to Y on that device."""
+        dev = self.owner.get(name)
+        if dev is None:
+            raise KeyError(name)
+        server = self.servers[dev]
+        device = getattr(server, "device", None)
+        if device is not None and getattr(X, "device", device) != device:
+            X = X.to(device)
+        return server.submit(name, X, alpha, keep_result)
+
+    def start(self) -> "ShardedServer":
+        for s in self.servers:
+            s.start()
+        return self
+
+    def stop(self) -> None:
+        for s in self.servers:
+            s.stop()
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
