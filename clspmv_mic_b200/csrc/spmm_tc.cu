@@ -45,6 +45,7 @@
 // ends the kernel cleanly, tensor memory released, and is counted in a device
 // word that clspmv_tensor_timeouts reads.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include "clspmv_b200.h"
@@ -215,7 +216,7 @@ __device__ __forceinline__ void load_step(StepLoads<KC>& f, int col_lane, int gw
         const float* xp = X + (size_t)(4 * c4) * ldx + j;
 #pragma unroll
         for (int c = 0; c < 4; c++)
-            f.x[4 * i + c] = (ok && 4 * c4 + c < width) ? ld_x(xp + (size_t)c * ldx, pl) : 0.f;
+            f.x[4 * i + c] = (ok && (unsigned)(4 * c4 + c) < (unsigned)width) ? ld_x(xp + (size_t)c * ldx, pl) : 0.f;
     }
     f.v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (lane < 16 && gw + (lane >> 2) < b1)
@@ -416,9 +417,17 @@ int launch_tc(const clspmv_b4csr_f32& m, const float* X, int ldx, float* Y, int 
               cudaStream_t st)
 {
     using S = TcSmem<KC>;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_b4csr_spmm_tc<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kLaunch);
-    if (attr != cudaSuccess) return CLSPMV_ERR_CUDA;
+    // the shared-memory limit is a per-device attribute of the function: set once per device
+    static std::atomic<unsigned long long> attr_set{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CLSPMV_ERR_CUDA;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
+        if (cudaFuncSetAttribute(k_b4csr_spmm_tc<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kLaunch) !=
+            cudaSuccess)
+            return CLSPMV_ERR_CUDA;
+        attr_set.fetch_or(bit);
+    }
     const int ntiles = (m.b4csr_row_num + kTcTileRows - 1) / kTcTileRows;
     const int grid = std::max(1, std::min(ntiles, sm_count() * S::kPerSm));
     k_b4csr_spmm_tc<KC><<<grid, kTcThreads, S::kLaunch, st>>>(m.b4csr_row_num, m.matinfo.height, m.matinfo.width,
