@@ -116,12 +116,25 @@ int clspmv_pad_csr_f32(const clspmv_csr_f32* src, clspmv_csr_f32* dst, int align
     });
 }
 
+// The reference's coo2dia (include/matrix_storage.h:936-1014) sizes every
+// diagonal at aligned(min(w, h)) and writes the value of row r at index r,
+// so a taller-than-wide matrix with an entry at or below that row would
+// write past its arrays; such input is rejected (CLSPMV_ERR_ARG). Taller
+// matrices whose entries all sit above it convert exactly as there.
+static bool rows_fit_diagonals(const clspmv_coo_f32* src, int alignment)
+{
+    const int w = src->matinfo.width, h = src->matinfo.height;
+    if (h <= w) return true;
+    const long long len = aligned_length<long long>(w, alignment);
+    for (int i = 0; i < src->matinfo.nnz; i++)
+        if (src->coo_row_id[i] >= len) return false;
+    return true;
+}
+
 int clspmv_coo2dia_f32(const clspmv_coo_f32* src, clspmv_dia_f32* dst, int alignment)
 {
     if (!coo_ok(src) || !dst || alignment <= 0 || !coo_in_range(src)) return CLSPMV_ERR_ARG;
-    // The reference writes dia_data[row] with row < aligned(min(w, h)); a
-    // taller-than-wide matrix would overflow it, so it is rejected here.
-    if (src->matinfo.height > src->matinfo.width) return CLSPMV_ERR_ARG;
+    if (!rows_fit_diagonals(src, alignment)) return CLSPMV_ERR_ARG;
     return guarded([&] {
         bool ok = coo2dia<int, int, float>(const_cast<coo_t*>(as_tmpl<coo_t>(src)), as_tmpl<dia_t>(dst), alignment);
         return ok ? (int)CLSPMV_OK : (int)CLSPMV_ERR_REFUSED;
@@ -131,7 +144,7 @@ int clspmv_coo2dia_f32(const clspmv_coo_f32* src, clspmv_dia_f32* dst, int align
 int clspmv_coo2bdia_f32(const clspmv_coo_f32* src, clspmv_bdia_f32* dst, int alignment)
 {
     if (!coo_ok(src) || !dst || alignment <= 0 || !coo_in_range(src)) return CLSPMV_ERR_ARG;
-    if (src->matinfo.height > src->matinfo.width) return CLSPMV_ERR_ARG;
+    if (!rows_fit_diagonals(src, alignment)) return CLSPMV_ERR_ARG;
     return guarded([&] {
         bool ok = coo2bdia<int, int, float>(const_cast<coo_t*>(as_tmpl<coo_t>(src)), as_tmpl<bdia_t>(dst), alignment);
         return ok ? (int)CLSPMV_OK : (int)CLSPMV_ERR_REFUSED;
