@@ -198,3 +198,48 @@ def test_part_layout_change_keeps_nonzeros(table_dirs):
                         np.testing.assert_array_equal(alt.part(p).array(field), arr)
             done += 1
     assert done >= 1
+
+
+def _random_matrix(rng, n):
+    """A square matrix of 1-3 overlaid structures (band, 4x4 blocks, scattered
+    with empty rows, power-law rows) drawn from `rng`."""
+    parts = []
+    for kind in rng.choice(["band", "blocks", "random", "power"], size=int(rng.integers(1, 4)), replace=False):
+        s = int(rng.integers(0, 10 ** 6))
+        if kind == "band":
+            parts.append(synth.banded(n, int(rng.integers(1, 12)), seed=s))
+        elif kind == "blocks":
+            b = synth.block_rows(max(1, n // 4 - 1), int(rng.integers(1, 9)), 4, 4, seed=s)
+            parts.append((n, n, b[2], b[3], b[4]))
+        elif kind == "random":
+            parts.append(synth.random_coo(n, n, float(rng.uniform(0.0005, 0.01)), seed=s,
+                                          empty_row_frac=float(rng.uniform(0, 0.5))))
+        else:
+            parts.append(synth.powerlaw(n, maxlen=max(2, n // 3), seed=s))
+    clipped = []
+    for p in parts:
+        r, c, v = np.asarray(p[2]), np.asarray(p[3]), np.asarray(p[4])
+        keep = (r < n) & (c < n)
+        clipped.append((n, n, r[keep], c[keep], v[keep]))
+    return F.coo_matrix(*_union(*clipped))
+
+
+def test_random_matrices_and_tables_identical(tmp_path):
+    """Seeded random matrices (64-3000 rows, overlaid structures), random
+    table sets and all four analyzer modes: byte-identical partitions."""
+    ref_or_skip()
+    rng = np.random.default_rng(2024)
+    dirs = []
+    for i in range(4):
+        d = tmp_path / f"t{i}"
+        d.mkdir()
+        sc = {k: float(np.exp(rng.uniform(np.log(0.1), np.log(6)))) for k in tables.IMP}
+        tables.model_tables(d, seed=i + 3, scale=sc, launch_us=float(rng.choice([0.05, 0.5, 4.0])),
+                            gather_per_s=float(rng.choice([5e11, 2e12, 1e13])))
+        dirs.append(d)
+    for it in range(60):
+        coo = _random_matrix(rng, int(rng.integers(64, 3000)))
+        mode = _ALL_MODES[it % 4]
+        d = dirs[it % len(dirs)]
+        diffs = compare_cocktails(CK.analyze(coo, d, *mode), ref_analyze(coo, d, *mode))
+        assert not diffs, f"case {it} mode={mode}: {diffs[:5]}"
