@@ -195,3 +195,26 @@ def test_cpp_compat_serial_templates_match_reference(tmp_path, name):
         np.testing.assert_array_equal(got[fmt], y[:h], err_msg=fmt)
         checked.append(fmt)
     assert {"coo", "csr", "sell", "bcsr"} <= set(checked)
+
+
+def test_read_mmf_random_files_match_reference(tmp_path):
+    """Seeded random MatrixMarket files (general and symmetric, real and
+    pattern, shuffled entry order, values at several magnitudes and printed
+    precisions, 0-2 comment lines): identical COO to the reference's ReadMMF."""
+    ref_or_skip()
+    for it in range(60):
+        rng = np.random.default_rng(it)
+        h, w = int(rng.integers(1, 40)), int(rng.integers(1, 40))
+        sym = bool(rng.random() < 0.4)
+        if sym:
+            w = h
+        mask = rng.random((h, w)) < rng.uniform(0, 0.3)
+        if sym:
+            mask = np.tril(mask)
+        r, c = np.nonzero(mask)
+        v = np.round(rng.standard_normal(r.size) * 10.0 ** int(rng.integers(-3, 4)), int(rng.integers(0, 6)))
+        field = "pattern" if rng.random() < 0.25 else "real"
+        p = tmp_path / f"m{it}.mtx"
+        write_mtx(p, h, w, r, c, v, field=field, symmetry="symmetric" if sym else "general",
+                  order=rng.permutation(r.size), comments=tuple(["c"] * int(rng.integers(0, 3))))
+        assert_same_coo(read_mmf(p), ref_read(p))
