@@ -165,3 +165,36 @@ def test_inverse_converters_match_reference(coo):
             assert n <= theirs.nnz and np.all(mine.array("coo_col_id") < h)
         else:
             assert mine.scalars() == theirs.scalars(), (fmt, args)
+
+
+@SETTINGS
+@given(h=st.integers(1, 60), w=st.integers(1, 60), n=st.integers(0, 400), seed=st.integers(0, 10 ** 6))
+def test_sort_coo_matches_reference_without_duplicates(h, w, n, seed):
+    """sort_coo on shuffled duplicate-free input: the same arrays as the
+    reference's quicksort (any order of distinct keys sorts to one result)."""
+    L = ref_or_skip()
+    import ctypes as C
+    rng = np.random.default_rng(seed)
+    keys = rng.permutation(np.unique(rng.integers(0, h * w, n)))
+    r, c = keys // w, keys % w
+    v = rng.standard_normal(keys.size).astype(np.float32)
+    a = F.coo_matrix(h, w, r, c, v)
+    b = a.copy()
+    F.sort_coo(a)
+    assert L.ref_sort_coo(C.byref(b.struct)) == 1
+    for f in ("coo_row_id", "coo_col_id", "coo_data"):
+        assert np.array_equal(a.array(f).view(np.uint32), b.array(f).view(np.uint32))
+
+
+def test_sort_coo_is_stable_on_repeated_keys():
+    """Repeated (row, col) keys, outside the COO contract of both libraries,
+    keep their input order here (the device sort does the same); the
+    reference's quicksort leaves them in an order set by its pivoting."""
+    rng = np.random.default_rng(5)
+    r = rng.integers(0, 6, 200)
+    c = rng.integers(0, 5, 200)
+    v = np.arange(1, 201, dtype=np.float32)   # input position, to check the order of equal keys
+    order = np.lexsort((np.arange(200), c, r))   # by key, then by input position
+    a = F.coo_matrix(6, 5, r.copy(), c.copy(), v.copy())   # sorted in place
+    F.sort_coo(a)
+    assert np.array_equal(a.array("coo_data"), v[order])
