@@ -346,6 +346,15 @@ bool coo2dia(coo_matrix<dimType, dataType>* source, dia_matrix<dimType, offsetTy
     const dimType nnz = source->matinfo.nnz;
     dest->dia_offsets = NULL;
     dest->dia_data = NULL;
+    /* The reference stores row r of every diagonal at index r of a len-long
+     * array, so a taller-than-wide matrix with an entry at row >= len would
+     * be written past it (undefined there): refused here instead. */
+    for (dimType i = 0; i < nnz; i++)
+        if (source->coo_row_id[i] >= len) {
+            dest->dia_num = 0;
+            dest->dia_length_aligned = len;
+            return false;
+        }
     /* slot[offset + (h - 1)] = discovery index + 1 */
     std::vector<int32_t> slot((size_t)w + (size_t)h, 0);
     std::vector<offsetType> found;

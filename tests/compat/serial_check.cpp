@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "fileio.h"
@@ -55,7 +56,7 @@ int main(int argc, char** argv)
     if (!f) return 4;
 
     std::vector<float> y(h + 4096, 0.0f);
-    auto reset = [&](size_t n) { y.assign(n + 64, 0.0f); };
+    auto reset = [&](size_t n) { y.assign(std::max(n, (size_t)h) + 64, 0.0f); };
 
     reset(h);
     coo_spmv<int, float>(&coo, x.data(), y.data(), w);
