@@ -14,6 +14,11 @@
 // uninitialised (sbell column ids of padding block rows, bell column ids
 // past the block-row count) are zero here.
 #include <algorithm>
+#include <atomic>
+#include <climits>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include <cstddef>
 #include <cstdio>
 #include <new>
@@ -639,6 +644,35 @@ struct BlockCount {
     int partial_block_num = 0, partial_nnz = 0, full_block_num = 0, full_nnz = 0;
 };
 
+// Runs f(0) .. f(n - 1) on up to n host threads; an exception thrown by any
+// of them is rethrown here once all have finished.
+template <class F>
+void for_each_parallel(int n, F f)
+{
+    const int nt = std::min<int>(n, (int)std::max(1u, std::thread::hardware_concurrency()));
+    if (nt < 2) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::exception_ptr err;
+    std::mutex err_lock;
+    vector<std::thread> threads;
+    for (int t = 0; t < nt; t++)
+        threads.emplace_back([&] {
+            for (int i; (i = next++) < n;) {
+                try {
+                    f(i);
+                } catch (...) {
+                    std::lock_guard<std::mutex> g(err_lock);
+                    if (!err) err = std::current_exception();
+                }
+            }
+        });
+    for (std::thread& th : threads) th.join();
+    if (err) std::rethrow_exception(err);
+}
+
 vector<int> row_pointer(const Coo& a)
 {
     vector<int> rp((size_t)a.height + 1, 0);
@@ -665,14 +699,25 @@ BlockSplit split_blocks(const Coo& a, const vector<int>& rp, int bw, int bh, Kee
     const int bs = bw * bh;
     out.rowptr.assign((size_t)nbr + 1, 0);
     vector<int> idx;
+    int head[8], stop[8];
     for (int br = 0; br < nbr; br++) {
         const int r0 = br * bh;
         const int s = rp[r0], e = r0 + bh <= a.height ? rp[r0 + bh] : rp[a.height];
         idx.resize((size_t)std::max(0, e - s));
-        for (int k = s; k < e; k++) idx[(size_t)(k - s)] = k;
-        std::stable_sort(idx.begin(), idx.end(), [&](int p, int q) {
-            return a.c[p] != a.c[q] ? a.c[p] < a.c[q] : a.r[p] < a.r[q];
-        });
+        // (column, row) order of the block row's entries, as a stable sort by
+        // that key would leave them: each row is already in column order, so
+        // merge the rows, the lower row first on equal columns
+        const int nr = std::min(bh, a.height - r0);
+        for (int t = 0; t < nr; t++) {
+            head[t] = rp[r0 + t];
+            stop[t] = rp[r0 + t + 1];
+        }
+        for (size_t k = 0; k < idx.size(); k++) {
+            int best = -1;
+            for (int t = 0; t < nr; t++)
+                if (head[t] < stop[t] && (best < 0 || a.c[head[t]] < a.c[head[best]])) best = t;
+            idx[k] = head[best]++;
+        }
         int kept = 0;
         size_t k = 0;
         while (k < idx.size()) {
@@ -704,13 +749,28 @@ BlockSplit split_blocks(const Coo& a, const vector<int>& rp, int bw, int bh, Kee
     return out;
 }
 
+// Stable sort by (row, column): a stable counting sort by row, then a
+// stable sort by column of each row whose entries are not already in
+// column order (the leftovers of a block split arrive row by row in column
+// order, so usually none).
 void sort_rest(Coo& rest)
 {
-    vector<size_t> p(rest.r.size());
-    for (size_t i = 0; i < p.size(); i++) p[i] = i;
-    std::stable_sort(p.begin(), p.end(), [&](size_t x, size_t y) {
-        return rest.r[x] != rest.r[y] ? rest.r[x] < rest.r[y] : rest.c[x] < rest.c[y];
-    });
+    const size_t n = rest.r.size();
+    vector<size_t> start((size_t)rest.height + 1, 0);
+    for (size_t i = 0; i < n; i++) start[(size_t)rest.r[i] + 1]++;
+    for (int h = 0; h < rest.height; h++) start[(size_t)h + 1] += start[(size_t)h];
+    vector<size_t> p(n), fill(start.begin(), start.end() - 1);
+    for (size_t i = 0; i < n; i++) p[fill[(size_t)rest.r[i]]++] = i;
+    for (int h = 0; h < rest.height; h++) {
+        auto b = p.begin() + (long)start[(size_t)h], e = p.begin() + (long)start[(size_t)h + 1];
+        bool ordered = true;
+        for (auto it = b; it + 1 < e; ++it)
+            if (rest.c[*(it + 1)] < rest.c[*it]) {
+                ordered = false;
+                break;
+            }
+        if (!ordered) std::stable_sort(b, e, [&](size_t x, size_t y) { return rest.c[x] < rest.c[y]; });
+    }
     Coo s;
     s.width = rest.width;
     s.height = rest.height;
@@ -968,34 +1028,43 @@ bool Partitioner::extract_block(const Coo& a, Coo& rest, bool flat_partial, bool
         if (threshold[i] > kBH[i] * kBW[i] - 1) threshold[i] = kBH[i] * kBW[i] - 1;
     }
 
-    // per shape and block row: blocks and nonzeros, all / denser than the threshold
+    // per shape and block row: blocks and nonzeros, all / denser than the
+    // threshold. Each row's columns are sorted, so merging the rows of a
+    // block row yields its block columns in order without sorting; the
+    // eight shapes are counted side by side.
     vector<vector<BlockCount> > bc(8);
-    vector<int> keys;
-    for (int s = 0; s < 8; s++) {
+    for_each_parallel(8, [&](int s) {
         const int bh = kBH[s], bw = kBW[s];
         const int nbr = a.height / bh + (a.height % bh ? 1 : 0);
         bc[s].assign((size_t)nbr, BlockCount());
+        int head[8], stop[8];
         for (int br = 0; br < nbr; br++) {
-            const int r0 = br * bh;
-            const int st = rp[r0], en = rp[std::min(r0 + bh, a.height)];
-            keys.assign(a.c.begin() + st, a.c.begin() + en);
-            for (int& k : keys) k /= bw;
-            std::sort(keys.begin(), keys.end());
+            const int r0 = br * bh, nr = std::min(bh, a.height - r0);
+            for (int t = 0; t < nr; t++) {
+                head[t] = rp[r0 + t];
+                stop[t] = rp[r0 + t + 1];
+            }
             BlockCount& c = bc[s][br];
-            for (size_t i = 0; i < keys.size();) {
-                size_t j = i;
-                while (j < keys.size() && keys[j] == keys[i]) j++;
-                const int n = (int)(j - i);
+            for (;;) {
+                int key = INT_MAX;
+                for (int t = 0; t < nr; t++)
+                    if (head[t] < stop[t]) key = std::min(key, a.c[head[t]] / bw);
+                if (key == INT_MAX) break;
+                int n = 0;
+                for (int t = 0; t < nr; t++)
+                    while (head[t] < stop[t] && a.c[head[t]] / bw == key) {
+                        head[t]++;
+                        n++;
+                    }
                 c.full_block_num++;
                 c.full_nnz += n;
                 if (n > threshold[s]) {
                     c.partial_block_num++;
                     c.partial_nnz += n;
                 }
-                i = j;
             }
         }
-    }
+    });
 
     double block_ovh[8];
     for (int i = 0; i < 8; i++) block_ovh[i] = overhead(a.height / (kBH[i] * SELL_GROUP_SIZE), SELL_GROUP_SIZE) / 1000.0;
@@ -1215,8 +1284,10 @@ static SellEllPlan plan_sell_ell(const vector<int>& rownnz, int nnz, const maxfl
     p.part_w.assign((size_t)ns, 0);
     p.part_nnz = 0;
     p.full_nnz = nnz;
+    vector<int> sw;
+    sw.reserve((size_t)sh);
     for (int i = 0; i < ns; i++) {
-        vector<int> sw;
+        sw.clear();
         for (int j = i * sh; j < (i + 1) * sh && j < (int)rownnz.size(); j++) sw.push_back(rownnz[j]);
         std::sort(sw.begin(), sw.end());
         p.full_w[i] = sw[sw.size() - 1];
