@@ -691,16 +691,16 @@ struct BlockSplit {
     int kept_nnz = 0;
 };
 
+// Block rows [b0, b1) into `out` (rowptr relative to b0) and `rest`.
 template <class Keep>
-BlockSplit split_blocks(const Coo& a, const vector<int>& rp, int bw, int bh, Keep keep, Coo& rest)
+void split_block_rows(const Coo& a, const vector<int>& rp, int bw, int bh, Keep& keep, int b0, int b1, BlockSplit& out,
+                      Coo& rest)
 {
-    BlockSplit out;
-    const int nbr = a.height / bh + (a.height % bh ? 1 : 0);
     const int bs = bw * bh;
-    out.rowptr.assign((size_t)nbr + 1, 0);
+    out.rowptr.assign((size_t)(b1 - b0) + 1, 0);
     vector<int> idx;
     int head[8], stop[8];
-    for (int br = 0; br < nbr; br++) {
+    for (int br = b0; br < b1; br++) {
         const int r0 = br * bh;
         const int s = rp[r0], e = r0 + bh <= a.height ? rp[r0 + bh] : rp[a.height];
         idx.resize((size_t)std::max(0, e - s));
@@ -744,7 +744,57 @@ BlockSplit split_blocks(const Coo& a, const vector<int>& rp, int bw, int bh, Kee
             }
             k = k1;
         }
-        out.rowptr[br + 1] = out.rowptr[br] + kept;
+        out.rowptr[br - b0 + 1] = out.rowptr[br - b0] + kept;
+    }
+}
+
+// Block rows are independent: ranges of about equal nonzeros are split on
+// separate host threads and joined in order, which gives the same arrays
+// (and the same order of leftovers) as one pass. `keep` must only read.
+template <class Keep>
+BlockSplit split_blocks(const Coo& a, const vector<int>& rp, int bw, int bh, Keep keep, Coo& rest)
+{
+    const int nbr = a.height / bh + (a.height % bh ? 1 : 0);
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min(hw, std::min(nbr, a.nnz() / (1 << 16) + 1)));
+    vector<int> cut((size_t)nt + 1, nbr);
+    cut[0] = 0;
+    for (int t = 1; t < nt; t++) {
+        const long long target = (long long)a.nnz() * t / nt;
+        int lo = cut[t - 1], hi = nbr;   // first block row starting at or past target
+        while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (rp[std::min(mid * bh, a.height)] >= target) hi = mid;
+            else lo = mid + 1;
+        }
+        cut[t] = lo;
+    }
+    vector<BlockSplit> part((size_t)nt);
+    vector<Coo> left((size_t)nt);
+    for_each_parallel(nt, [&](int t) { split_block_rows(a, rp, bw, bh, keep, cut[t], cut[t + 1], part[t], left[t]); });
+    BlockSplit out;
+    out.rowptr.assign((size_t)nbr + 1, 0);
+    size_t nblocks = 0, nleft = 0;
+    for (int t = 0; t < nt; t++) {
+        nblocks += part[t].colid.size();
+        nleft += left[t].r.size();
+    }
+    out.colid.reserve(nblocks);
+    out.data.reserve(nblocks * (size_t)(bw * bh));
+    rest.r.reserve(rest.r.size() + nleft);
+    rest.c.reserve(rest.c.size() + nleft);
+    rest.v.reserve(rest.v.size() + nleft);
+    for (int t = 0; t < nt; t++) {
+        for (int br = cut[t]; br < cut[t + 1]; br++)
+            out.rowptr[br + 1] = out.rowptr[br] + (part[t].rowptr[br - cut[t] + 1] - part[t].rowptr[br - cut[t]]);
+        out.colid.insert(out.colid.end(), part[t].colid.begin(), part[t].colid.end());
+        out.data.insert(out.data.end(), part[t].data.begin(), part[t].data.end());
+        out.kept_nnz += part[t].kept_nnz;
+        vector<int>().swap(part[t].colid);
+        vector<float>().swap(part[t].data);
+        rest.r.insert(rest.r.end(), left[t].r.begin(), left[t].r.end());
+        rest.c.insert(rest.c.end(), left[t].c.begin(), left[t].c.end());
+        rest.v.insert(rest.v.end(), left[t].v.begin(), left[t].v.end());
     }
     return out;
 }
