@@ -18,6 +18,7 @@
 #include <climits>
 #include <exception>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <cstddef>
 #include <cstdio>
@@ -644,31 +645,32 @@ struct BlockCount {
     int partial_block_num = 0, partial_nnz = 0, full_block_num = 0, full_nnz = 0;
 };
 
-// Runs f(0) .. f(n - 1) on up to n host threads; an exception thrown by any
-// of them is rethrown here once all have finished.
+// Runs f(0) .. f(n - 1) on the calling thread and up to n - 1 more host
+// threads (fewer if they cannot be started); an exception thrown by any call
+// is rethrown here once all have finished.
 template <class F>
 void for_each_parallel(int n, F f)
 {
     const int nt = std::min<int>(n, (int)std::max(1u, std::thread::hardware_concurrency()));
-    if (nt < 2) {
-        for (int i = 0; i < n; i++) f(i);
-        return;
-    }
     std::atomic<int> next{0};
     std::exception_ptr err;
     std::mutex err_lock;
-    vector<std::thread> threads;
-    for (int t = 0; t < nt; t++)
-        threads.emplace_back([&] {
-            for (int i; (i = next++) < n;) {
-                try {
-                    f(i);
-                } catch (...) {
-                    std::lock_guard<std::mutex> g(err_lock);
-                    if (!err) err = std::current_exception();
-                }
+    auto work = [&] {
+        for (int i; (i = next++) < n;) {
+            try {
+                f(i);
+            } catch (...) {
+                std::lock_guard<std::mutex> g(err_lock);
+                if (!err) err = std::current_exception();
             }
-        });
+        }
+    };
+    vector<std::thread> threads;
+    try {
+        for (int t = 1; t < nt; t++) threads.emplace_back(work);
+    } catch (const std::system_error&) {   // no more threads: the ones running and this one finish the work
+    }
+    work();
     for (std::thread& th : threads) th.join();
     if (err) std::rethrow_exception(err);
 }
@@ -1755,6 +1757,9 @@ extern "C" int clspmv_analyze_matrix_f32(const clspmv_coo_f32* coo, clspmv_cockt
         analyze_matrix_tables(bench, *reinterpret_cast<coo_matrix<int, float>*>(const_cast<clspmv_coo_f32*>(coo)), *mat,
                               dia_priority_multiplier, estimate_flat_partial != 0, estimate_flat_full != 0);
     } catch (const std::bad_alloc&) {
+        free_cocktail(*mat);
+        return CLSPMV_ERR_ALLOC;
+    } catch (...) {   // any other resource failure (e.g. host threads): nothing kept
         free_cocktail(*mat);
         return CLSPMV_ERR_ALLOC;
     }
