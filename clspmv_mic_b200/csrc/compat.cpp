@@ -12,8 +12,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cerrno>
 #include <cstring>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "clspmv_b200.h"
@@ -55,6 +58,140 @@ std::string lower(const char* s)
     return t;
 }
 
+// The entry lines of a MatrixMarket file as whitespace-separated tokens,
+// `per` of them per entry (row, column[, value]), parsed on several host
+// threads: the text is cut into ranges at whitespace, each range's tokens are
+// counted, and each range then converts its tokens knowing their global
+// index. Integers go through strtoll and values through strtod, the
+// conversions fscanf's %lld / %lf make, so every entry is the one fscanf
+// would read. Tokens past nnz entries are ignored, as by fscanf.
+int parse_entries(const std::vector<char>& text, long long nnz, int per, long long height, long long width,
+                  std::vector<int>& r, std::vector<int>& c, std::vector<float>& v)
+{
+    const size_t n = text.size() - 1;   // text ends with '\0'
+    auto space = [&](size_t i) { return i >= n || std::isspace((unsigned char)text[i]); };
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)hw, n / (1u << 20) + 1));
+    std::vector<size_t> cut((size_t)nt + 1, n);
+    cut[0] = 0;
+    for (int t = 1; t < nt; t++) {
+        size_t b = std::max(cut[t - 1], n / nt * (size_t)t);
+        while (!space(b)) b++;   // never inside a token
+        cut[t] = b;
+    }
+    std::vector<long long> count((size_t)nt, 0), first((size_t)nt + 1, 0);
+    std::vector<int> bad((size_t)nt, 0);
+    auto run = [&](auto body) {
+        std::vector<std::thread> th;
+        try {
+            for (int t = 1; t < nt; t++) th.emplace_back(body, t);
+        } catch (const std::system_error&) {
+            for (int t = (int)th.size() + 1; t < nt; t++) body(t);   // no more threads: the rest here
+        }
+        body(0);
+        for (std::thread& x : th) x.join();
+    };
+    run([&](int t) {
+        long long k = 0;
+        for (size_t i = cut[t]; i < cut[t + 1]; i++)
+            if (!space(i) && (i == cut[t] || space(i - 1))) k++;
+        count[t] = k;
+    });
+    for (int t = 0; t < nt; t++) first[t + 1] = first[t] + count[t];
+    if (first[nt] < nnz * per) return CLSPMV_ERR_ARG;   // the file ends before nnz entries
+    run([&](int t) {
+        long long tok = first[t];
+        size_t i = cut[t];
+        while (i < cut[t + 1] && tok < nnz * per) {
+            while (i < cut[t + 1] && space(i)) i++;
+            if (i >= cut[t + 1]) break;
+            const char* s = text.data() + i;
+            char* end = nullptr;
+            const long long e = tok / per;
+            const int field = (int)(tok % per);
+            if (field < 2) {
+                errno = 0;
+                const long long x = std::strtoll(s, &end, 10);
+                if (end == s || errno || (field == 0 ? (x < 1 || x > height) : (x < 1 || x > width))) bad[t] = 1;
+                else (field == 0 ? r : c)[(size_t)e] = (int)(x - 1);
+            } else {
+                const double d = std::strtod(s, &end);
+                if (end == s) bad[t] = 1;
+                else v[(size_t)e] = (float)d;
+            }
+            if (bad[t]) return;
+            if (!space((size_t)(end - text.data()))) {   // a token with trailing characters
+                bad[t] = 1;
+                return;
+            }
+            i = (size_t)(end - text.data());
+            tok++;
+        }
+    });
+    for (int t = 0; t < nt; t++)
+        if (bad[t]) return CLSPMV_ERR_ARG;
+    return CLSPMV_OK;
+}
+
+// Stable sort of (row, column) pairs with their values, as std::stable_sort
+// by (row, column) would leave them: a stable counting sort by row, then a
+// stable sort by column of each row not already in column order (files
+// written column by column come out of the first step sorted).
+void sort_entries(int* r, int* c, float* v, size_t n, int height)
+{
+    std::vector<size_t> start((size_t)height + 1, 0);
+    for (size_t i = 0; i < n; i++) start[(size_t)r[i] + 1]++;
+    for (int h = 0; h < height; h++) start[(size_t)h + 1] += start[(size_t)h];
+    std::vector<unsigned> perm(n);
+    {
+        std::vector<size_t> fill(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < n; i++) perm[fill[(size_t)r[i]]++] = (unsigned)i;
+    }
+    // rows are independent: ranges of rows on separate host threads; short
+    // rows by insertion (stable), long ones by std::stable_sort
+    auto sort_rows = [&](int h0, int h1) {
+        for (int h = h0; h < h1; h++) {
+            unsigned* b = perm.data() + start[(size_t)h];
+            const size_t len = start[(size_t)h + 1] - start[(size_t)h];
+            bool ordered = true;
+            for (size_t k = 1; k < len && ordered; k++) ordered = c[b[k - 1]] <= c[b[k]];
+            if (ordered) continue;
+            if (len <= 32) {
+                for (size_t k = 1; k < len; k++) {
+                    const unsigned x = b[k];
+                    size_t j = k;
+                    for (; j > 0 && c[b[j - 1]] > c[x]; j--) b[j] = b[j - 1];
+                    b[j] = x;
+                }
+            } else {
+                std::stable_sort(b, b + len, [&](unsigned x, unsigned y) { return c[x] < c[y]; });
+            }
+        }
+    };
+    const int nt = (int)std::max<size_t>(1, std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                                              n / (1u << 16) + 1));
+    std::vector<int> cut((size_t)nt + 1, height);
+    cut[0] = 0;
+    for (int t = 1; t < nt; t++)   // about n / nt entries per range
+        cut[t] = (int)(std::lower_bound(start.begin(), start.end(), n / nt * (size_t)t) - start.begin());
+    for (int t = 1; t <= nt; t++) cut[t] = std::max(cut[t], cut[t - 1]);
+    std::vector<std::thread> th;
+    try {
+        for (int t = 1; t < nt; t++) th.emplace_back(sort_rows, cut[t], cut[t + 1]);
+    } catch (const std::system_error&) {
+        for (int t = (int)th.size() + 1; t < nt; t++) sort_rows(cut[t], cut[t + 1]);
+    }
+    sort_rows(cut[0], cut[1]);
+    for (std::thread& x : th) x.join();
+    std::vector<int> tr(r, r + n), tc(c, c + n);
+    std::vector<float> tv(v, v + n);
+    for (size_t i = 0; i < n; i++) {
+        r[i] = tr[perm[i]];
+        c[i] = tc[perm[i]];
+        v[i] = tv[perm[i]];
+    }
+}
+
 int read_mmf(const char* filename, coo_matrix<int, float>* mat)
 {
     init_coo_matrix(*mat);
@@ -83,25 +220,30 @@ int read_mmf(const char* filename, coo_matrix<int, float>* mat)
         fclose(f);
         return CLSPMV_ERR_ARG;
     }
-    std::vector<int> r((size_t)nnz), c((size_t)nnz);
-    std::vector<float> v((size_t)nnz, 1.0f);
-    long long diag = 0;
-    for (long long i = 0; i < nnz; i++) {
-        long long ri, ci;
-        if (fscanf(f, "%lld %lld", &ri, &ci) != 2 || ri < 1 || ri > height || ci < 1 || ci > width) {
-            fclose(f);
-            return CLSPMV_ERR_ARG;
+    // the entry lines, whole, into memory
+    std::vector<char> text;
+    {
+        const long here = ftell(f);
+        size_t guess = 0;
+        if (here >= 0 && fseek(f, 0, SEEK_END) == 0) {
+            const long endpos = ftell(f);
+            if (endpos > here) guess = (size_t)(endpos - here);
+            fseek(f, here, SEEK_SET);
         }
-        if (has_value) {
-            double d = 0.0;
-            if (fscanf(f, "%lf", &d) != 1) { fclose(f); return CLSPMV_ERR_ARG; }
-            v[i] = (float)d;
-        }
-        r[i] = (int)(ri - 1);
-        c[i] = (int)(ci - 1);
-        if (r[i] == c[i]) diag++;
+        text.reserve(guess + 1);
+        char chunk[1 << 16];
+        size_t got;
+        while ((got = fread(chunk, 1, sizeof(chunk), f)) > 0) text.insert(text.end(), chunk, chunk + got);
+        text.push_back('\0');
     }
     fclose(f);
+    std::vector<int> r((size_t)nnz), c((size_t)nnz);
+    std::vector<float> v((size_t)nnz, 1.0f);
+    const int rc = parse_entries(text, nnz, has_value ? 3 : 2, height, width, r, c, v);
+    if (rc) return rc;
+    std::vector<char>().swap(text);
+    long long diag = 0;
+    for (long long i = 0; i < nnz; i++) diag += r[(size_t)i] == c[(size_t)i];
     const size_t total = symmetric ? (size_t)(2 * nnz - diag) : (size_t)nnz;
     mat->matinfo.height = (int)height;
     mat->matinfo.width = (int)width;
@@ -125,7 +267,7 @@ int read_mmf(const char* filename, coo_matrix<int, float>* mat)
             mat->coo_data[k++] = v[i];
         }
     }
-    if (!if_sorted_coo(mat)) sort_coo(mat);
+    if (!if_sorted_coo(mat)) sort_entries(mat->coo_row_id, mat->coo_col_id, mat->coo_data, total, (int)height);
     return CLSPMV_OK;
 }
 

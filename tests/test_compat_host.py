@@ -239,3 +239,35 @@ def test_read_mmf_random_files_match_reference(tmp_path):
         write_mtx(p, h, w, r, c, v, field=field, symmetry="symmetric" if sym else "general",
                   order=rng.permutation(r.size), comments=tuple(["c"] * int(rng.integers(0, 3))))
         assert_same_coo(read_mmf(p), ref_read(p))
+
+
+@pytest.mark.parametrize("field,symmetry", [("real", "general"), ("pattern", "general"), ("real", "symmetric")])
+def test_read_mmf_large_files_match_reference(tmp_path, field, symmetry):
+    """Files of several MB, so the entry text is cut into ranges parsed on
+    separate threads, with irregular whitespace (tabs, runs of blanks, CRLF
+    line ends, entries split over lines) and shuffled entries: the same COO
+    as the reference's ReadMMF."""
+    ref_or_skip()
+    rng = np.random.default_rng(7)
+    n = 3000
+    m = 250_000
+    r = rng.integers(0, n, m)
+    c = rng.integers(0, n, m)
+    if symmetry == "symmetric":
+        r, c = np.maximum(r, c), np.minimum(r, c)
+    key = np.unique(r.astype(np.int64) * n + c)
+    key = key[rng.permutation(key.size)]
+    r, c = key // n, key % n
+    v = rng.standard_normal(key.size) * 10.0 ** rng.integers(-4, 5, key.size)
+    seps = [" ", "\t", "   ", " \t "]
+    ends = ["\n", "\r\n", "\n\n"]
+    parts = [f"%%MatrixMarket matrix coordinate {field} {symmetry}\n% generated\n{n} {n} {key.size}\n"]
+    for i in range(key.size):
+        s1, s2 = seps[i % 4], seps[(i // 4) % 4]
+        tail = "" if field == "pattern" else f"{s2}{v[i]:.8g}"
+        split = "\n" if i % 997 == 0 else s1   # now and then an entry over two lines
+        parts.append(f"{r[i] + 1}{split}{c[i] + 1}{tail}{ends[i % 3]}")
+    p = tmp_path / "big.mtx"
+    p.write_bytes("".join(parts).encode())
+    assert p.stat().st_size > 2_500_000   # at least three 1 MB ranges
+    assert_same_coo(read_mmf(p), ref_read(p))
