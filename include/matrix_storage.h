@@ -217,18 +217,51 @@ bool if_sorted_coo(coo_matrix<dimType, dataType>* mat)
     return true;
 }
 
-/* sort_coo: include/matrix_storage.h:744-815. Stable (row, col) order. */
+/* sort_coo: include/matrix_storage.h:744-815. Stable (row, col) order: a
+ * stable counting sort on rows, then a stable sort of each row that is not
+ * already in column order (insertion for short rows); input with a row id
+ * outside [0, height) takes one comparison sort of the whole array. */
 template <class dimType, class dataType>
 bool sort_coo(coo_matrix<dimType, dataType>* mat)
 {
     const size_t n = (size_t)mat->matinfo.nnz;
-    std::vector<size_t> perm(n);
-    std::iota(perm.begin(), perm.end(), (size_t)0);
     const dimType* r = mat->coo_row_id;
     const dimType* c = mat->coo_col_id;
-    std::stable_sort(perm.begin(), perm.end(), [r, c](size_t a, size_t b) {
-        return r[a] != r[b] ? r[a] < r[b] : c[a] < c[b];
-    });
+    const long long height = (long long)mat->matinfo.height;
+    bool rows_ok = height >= 0;
+    for (size_t i = 0; i < n && rows_ok; i++) rows_ok = r[i] >= 0 && (long long)r[i] < height;
+    std::vector<size_t> perm(n);
+    if (rows_ok) {
+        std::vector<size_t> start((size_t)height + 1, 0);
+        for (size_t i = 0; i < n; i++) start[(size_t)r[i] + 1]++;
+        for (long long h = 0; h < height; h++) start[(size_t)h + 1] += start[(size_t)h];
+        {
+            std::vector<size_t> fill(start.begin(), start.end() - 1);
+            for (size_t i = 0; i < n; i++) perm[fill[(size_t)r[i]]++] = i;
+        }
+        for (long long h = 0; h < height; h++) {
+            size_t* b = perm.data() + start[(size_t)h];
+            const size_t len = start[(size_t)h + 1] - start[(size_t)h];
+            bool ordered = true;
+            for (size_t k = 1; k < len && ordered; k++) ordered = !(c[b[k]] < c[b[k - 1]]);
+            if (ordered) continue;
+            if (len <= 32) {
+                for (size_t k = 1; k < len; k++) {
+                    const size_t x = b[k];
+                    size_t j = k;
+                    for (; j > 0 && c[x] < c[b[j - 1]]; j--) b[j] = b[j - 1];
+                    b[j] = x;
+                }
+            } else {
+                std::stable_sort(b, b + len, [c](size_t x, size_t y) { return c[x] < c[y]; });
+            }
+        }
+    } else {
+        std::iota(perm.begin(), perm.end(), (size_t)0);
+        std::stable_sort(perm.begin(), perm.end(), [r, c](size_t a, size_t b) {
+            return r[a] != r[b] ? r[a] < r[b] : c[a] < c[b];
+        });
+    }
     std::vector<dimType> tr(n), tc(n);
     std::vector<dataType> td(n);
     for (size_t i = 0; i < n; i++) { tr[i] = r[perm[i]]; tc[i] = c[perm[i]]; td[i] = mat->coo_data[perm[i]]; }
