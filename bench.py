@@ -8,20 +8,30 @@ with the format's best kernel (the reference's drivers likewise report the
 best variant per format, e.g. src/spmv_csr_vector.cpp:649-656):
 
   stencil27   3D 27-point stencil 128^3 (2,097,152 rows, 55,742,968 nnz):  DIA, BDIA
-  powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR (merge-path kernel),
+  powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR (nonzero-chunk kernel),
               COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32
   blocks4x4   500,000 block rows x 8 dense 4x4 blocks (2,000,000 rows, 64M nnz):  BELL, SBELL, BCSR
 
-The CSR-vector and CSR-scalar kernels (the reference's two CSR drivers) are
-timed separately and reported under "variants".
+The merge-path, CSR-vector and CSR-scalar kernels (the last two are the
+reference's CSR drivers' mappings) and SELL read through its length plan
+are timed separately and reported under "variants".
 
 value = sum of useful flops (2 nnz per SpMV) / sum of kernel times, GFLOP/s.
 Kernel times are CUDA events on the launching stream; every matrix is larger
 than the 126 MB L2 and the formats run back to back, so no explicit flush.
 
+After timing, every format's y is computed once more at full size and
+compared per row with the reference's csr_spmv (|y - y_ref| <= 1e-5
+sum|a x|, the check the reference prints after each variant's first launch,
+src/util.cpp:93-131) and with the FP64 oracle ("parity" in the line).
+
+Output: one JSON line per detail block ("detail": ...), then the headline
+line last (compact, parsed by callers from the last line of stdout).
+
 --impl reference: the reference's own serial csr_spmv (include/spmv_serial.h
 :198-217, compiled from its sources into oracle/_ref; the C restatement in
-oracle/ where that build is absent), single thread, on the same matrices.
+oracle/ where that build is absent) on all host threads over row blocks, on
+the same matrices; this arm never loads libclspmv_b200.so.
 """
 from __future__ import annotations
 
@@ -42,6 +52,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "SpMV GFLOP/s (per-format FP32 sweep)"
 UNIT = "GFLOP/s"
 FALLBACK_HBM_GBS = 6650.0
+RTOL = 1e-5   # per-row bound: |y - y_ref| <= RTOL * sum_j |a_ij x_j|
 
 
 def parse_args():
@@ -56,6 +67,8 @@ def parse_args():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the several-right-hand-side, batched and serving measurements")
     p.add_argument("--serving-requests", type=int, default=1000)
+    p.add_argument("--detail-file", default="",
+                   help="also write every measurement (per format, variants, parity, extras) to this JSON file")
     return p.parse_args()
 
 
@@ -91,17 +104,11 @@ def build_workload(small: bool, only=None):
     """Host matrices of the sweep; `only` restricts it to some format keys
     (and builds only the matrices they need)."""
     from clspmv_mic_b200 import formats as F
-    from clspmv_mic_b200 import synth
 
     want = set(only) if only else {k for ks in FORMAT_KEYS.values() for k in ks}
     if "ell" in want or "ell_tail_coo" in want:
         want |= {"ell", "ell_tail_coo"}
-    gens = {
-        "stencil27": (lambda: synth.stencil_27pt(32)) if small else (lambda: synth.stencil_27pt(128)),
-        "powerlaw": (lambda: synth.powerlaw(1 << 15, maxlen=2000)) if small else (lambda: synth.powerlaw(1 << 20)),
-        "blocks4x4": (lambda: synth.block_rows(8000, 8)) if small else (lambda: synth.block_rows(500_000, 8)),
-    }
-    mats = {name: gen() for name, gen in gens.items() if want & set(FORMAT_KEYS[name])}
+    mats = {name: arrs for name, arrs in sweep_matrices(small, [n for n in FORMAT_KEYS if want & set(FORMAT_KEYS[n])]).items()}
     items = []
     meta = {"ell_width": None}
 
@@ -249,33 +256,136 @@ def ncu_traffic():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's serial csr_spmv
+# CPU leg: the reference's serial csr_spmv, timed as the baseline and used
+# as the checker of every format's y
 # ---------------------------------------------------------------------------
-def cpu_csr_seconds(mats, budget_s: float = 15.0):
-    """Best-of-k single-thread csr_spmv per matrix (compiled reference when
-    available). Returns (sum of best times, flops, kind, sample text)."""
+def host_threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
+
+
+def ref_csr(arrs):
+    """Host CSR of a generated COO built by the reference's own coo2csr
+    (include/matrix_storage.h:1268-1307, compiled into oracle/_ref); the C
+    restatement's arrays where that build is absent. Touches nothing of
+    libclspmv_b200.so."""
     from clspmv_mic_b200 import formats as F
-    from clspmv_mic_b200 import synth
     from oracle import oracle as O
-    use_ref = O.ref() is not None
-    kind = "reference" if use_ref else "port"
+    coo = F.coo_matrix(*arrs)
+    if O.ref() is not None:
+        ok, csr = O.ref_convert("csr", coo)
+        assert ok
+        return csr
+    h, w, r, c, v = arrs
+    rp = np.zeros(h + 1, np.int64)
+    np.add.at(rp, r.astype(np.int64) + 1, 1)
+    return F.from_arrays("csr", dict(width=w, height=h, nnz=r.size),
+                         dict(csr_row_ptr=np.cumsum(rp).astype(np.int32), csr_col_id=c, csr_data=v))
+
+
+def row_blocks(csr, parts: int):
+    """(r0, r1, slab) row blocks of a host CSR matrix with about nnz / parts
+    nonzeros each; each slab is a CSR view of rows [r0, r1) (its row
+    pointer rebased, col_id / data sliced), for the host threads."""
+    from clspmv_mic_b200 import formats as F
+    rp, col, val = csr.array("csr_row_ptr"), csr.array("csr_col_id"), csr.array("csr_data")
+    h, w = csr.shape
+    cuts = [0] + [int(np.searchsorted(rp, csr.nnz * t / parts)) for t in range(1, parts)] + [h]
+    out = []
+    for t in range(parts):
+        r0, r1 = cuts[t], max(cuts[t], cuts[t + 1])
+        if r1 <= r0:
+            continue
+        lo, hi = int(rp[r0]), int(rp[r1])
+        out.append((r0, r1, F.from_arrays("csr", dict(width=w, height=r1 - r0, nnz=hi - lo),
+                                          dict(csr_row_ptr=(rp[r0:r1 + 1] - lo).astype(np.int32),
+                                               csr_col_id=col[lo:hi], csr_data=val[lo:hi]))))
+    return out
+
+
+def csr_spmv_call():
+    """(call(csr, x, y), kind): the reference's csr_spmv compiled from its
+    sources, else the C restatement."""
+    import ctypes as C
+    from oracle import oracle as O
+    if O.ref() is not None:
+        return (lambda m, x, y: O.ref().ref_csr_spmv(C.byref(m.struct), x.ctypes.data, y.ctypes.data, x.size)), \
+            "reference"
+    return (lambda m, x, y: O.port().orc_csr_spmv_f32(C.byref(m.struct), x.ctypes.data, y.ctypes.data)), "port"
+
+
+class Oracle:
+    """y = A x of one matrix by the reference's csr_spmv (FP32, each row
+    summed left to right as written) and by the FP64 oracle with the row
+    scale sum_j |a_ij x_j|, each on all host threads over row blocks (rows
+    are independent, so the blocks give the one-thread result bit for bit)."""
+
+    def __init__(self, csr, x, pool, threads):
+        import ctypes as C
+        from oracle import oracle as O
+        h = csr.shape[0]
+        call, _ = csr_spmv_call()
+        self.y32 = np.zeros(h, np.float32)
+        self.y64 = np.zeros(h, np.float64)
+        self.scale = np.zeros(h, np.float64)
+        blocks = row_blocks(csr, threads)
+        L = O.port()
+
+        def one(b):
+            r0, r1, slab = b
+            call(slab, x, self.y32[r0:r1])
+            L.orc_csr_spmv_f64(C.byref(slab.struct), x.ctypes.data, self.y64[r0:r1].ctypes.data,
+                               self.scale[r0:r1].ctypes.data)
+        list(pool.map(one, blocks))
+
+    def check(self, y):
+        """rows over the bound |y - y_ref| <= 1e-5 sum|a x|, and the largest
+        |y - y64| / sum|a x|."""
+        y = y.astype(np.float64)
+        err = np.abs(y - self.y32.astype(np.float64))
+        over = int(np.count_nonzero(err > RTOL * self.scale + 1e-30))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            e64 = np.abs(y - self.y64) / np.where(self.scale > 0, self.scale, 1.0)
+        return over, float(e64.max()) if e64.size else 0.0
+
+    def ref_err64(self):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            e = np.abs(self.y32.astype(np.float64) - self.y64) / np.where(self.scale > 0, self.scale, 1.0)
+        return float(e.max()) if e.size else 0.0
+
+
+def cpu_csr_seconds(csrs, xs, budget_s: float = 15.0):
+    """Best-of-k one-thread csr_spmv per matrix (the reference's serial path
+    as written). Returns (sum of best times, flops, kind, sample text)."""
+    call, kind = csr_spmv_call()
     total_t, total_f, desc = 0.0, 0, []
-    per = budget_s / len(mats)
-    for name, arrs in mats.items():
-        coo = F.coo_matrix(*arrs)
-        csr = F.coo2csr(coo)
-        x = synth.x_vector(arrs[1])
+    per = budget_s / len(csrs)
+    for name, csr in csrs.items():
+        x = xs[name]
         best, n, t_start = float("inf"), 0, time.perf_counter()
         while n < 3 or (time.perf_counter() - t_start < per and n < 50):
-            y = np.zeros(arrs[0], np.float32)
+            y = np.zeros(csr.shape[0], np.float32)
             t0 = time.perf_counter()
-            (O.spmv_ref if use_ref else O.spmv_port)(csr, x, y)
+            call(csr, x, y)
             best = min(best, time.perf_counter() - t0)
             n += 1
         total_t += best
         total_f += 2 * csr.nnz
         desc.append(f"{name} best of {n}")
     return total_t, total_f, kind, "csr_spmv on " + ", ".join(desc) + ", 1 thread"
+
+
+def loaded_native_libs():
+    """Shared objects of this repository mapped into the process (from
+    /proc/self/maps): the reference arm must map oracle/ libraries only."""
+    out = set()
+    try:
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            t = line.split()
+            if len(t) >= 6 and t[-1].endswith(".so") and t[-1].startswith(str(ROOT)):
+                out.add(os.path.relpath(t[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 # ---------------------------------------------------------------------------
@@ -318,55 +428,41 @@ def job_value(flops_per_replica_step: float, world: int, ms_per_step: float) -> 
     return flops_per_replica_step * world / (ms_per_step * 1e-3) / 1e9
 
 
-def row_blocks(csr, parts: int):
-    """(r0, r1, slab) row blocks of a host CSR matrix with about nnz / parts
-    nonzeros each; each slab is a CSR view of rows [r0, r1) (its row
-    pointer rebased, col_id / data sliced), for the threads of the
-    reference arm."""
-    from clspmv_mic_b200 import formats as F
-    rp, col, val = csr.array("csr_row_ptr"), csr.array("csr_col_id"), csr.array("csr_data")
-    h, w = csr.shape
-    cuts = [0] + [int(np.searchsorted(rp, csr.nnz * t / parts)) for t in range(1, parts)] + [h]
-    out = []
-    for t in range(parts):
-        r0, r1 = cuts[t], max(cuts[t], cuts[t + 1])
-        if r1 <= r0:
-            continue
-        lo, hi = int(rp[r0]), int(rp[r1])
-        out.append((r0, r1, F.from_arrays("csr", dict(width=w, height=r1 - r0, nnz=hi - lo),
-                                          dict(csr_row_ptr=(rp[r0:r1 + 1] - lo).astype(np.int32),
-                                               csr_col_id=col[lo:hi], csr_data=val[lo:hi]))))
-    return out
+def sweep_matrices(small: bool, names=None):
+    """The sweep's three matrices (row-sorted COO tuples from the numpy
+    generators), or the named ones."""
+    from clspmv_mic_b200 import synth
+    gens = {
+        "stencil27": (lambda: synth.stencil_27pt(32)) if small else (lambda: synth.stencil_27pt(128)),
+        "powerlaw": (lambda: synth.powerlaw(1 << 15, maxlen=2000)) if small else (lambda: synth.powerlaw(1 << 20)),
+        "blocks4x4": (lambda: synth.block_rows(8000, 8)) if small else (lambda: synth.block_rows(500_000, 8)),
+    }
+    return {n: g() for n, g in gens.items() if names is None or n in names}
+
+
+WORKLOAD = ("nine-format FP32 sweep: stencil27 128^3 -> DIA,BDIA; powerlaw 2^20 Zipf(2.0) mean 16 -> "
+            "CSR,COO,ELL(K)+COO tail,SELL-32; 4x4 blocks 500k x 8 -> BELL,SBELL,BCSR")
 
 
 def run_reference(args):
+    """The reference's serial csr_spmv (its own code, compiled from its
+    sources into oracle/_ref) on every host thread: each thread runs it on a
+    block of rows holding about nnz / threads nonzeros (ctypes releases the
+    GIL during the call). Matrices come from the numpy generators and their
+    CSR from the reference's coo2csr; libclspmv_b200.so is never loaded."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from clspmv_mic_b200 import synth  # noqa: F401
-    mats = {}
-    if args.small:
-        from clspmv_mic_b200 import synth as S
-        mats = {"stencil27": S.stencil_27pt(32), "powerlaw": S.powerlaw(1 << 15, maxlen=2000),
-                "blocks4x4": S.block_rows(8000, 8)}
-    else:
-        from clspmv_mic_b200 import synth as S
-        mats = {"stencil27": S.stencil_27pt(128), "powerlaw": S.powerlaw(1 << 20), "blocks4x4": S.block_rows(500_000, 8)}
-    import ctypes as C
     from concurrent.futures import ThreadPoolExecutor
-    from clspmv_mic_b200 import formats as F
-    from oracle import oracle as O
-    use_ref = O.ref() is not None
-    # the reference's serial csr_spmv (its own code, compiled from its sources)
-    # on every host thread: each thread runs it on a block of rows holding
-    # about nnz / threads nonzeros (ctypes releases the GIL during the call)
-    call = (lambda m, x, y: O.ref().ref_csr_spmv(C.byref(m.struct), x.ctypes.data, y.ctypes.data, x.size)) if use_ref \
-        else (lambda m, x, y: O.port().orc_csr_spmv_f32(C.byref(m.struct), x.ctypes.data, y.ctypes.data))
-    threads = max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1))
+
+    from clspmv_mic_b200 import synth
+    mats = sweep_matrices(args.small)
+    call, kind = csr_spmv_call()
+    threads = host_threads()
     prepared, keep = [], []
     for name, arrs in mats.items():
-        csr = F.coo2csr(F.coo_matrix(*arrs))
+        csr = ref_csr(arrs)
         keep.append(csr)
         h, w = csr.shape
         x = synth.x_vector(arrs[1])
@@ -381,32 +477,59 @@ def run_reference(args):
             y.fill(0.0)
         list(pool.map(lambda t: call(*t), prepared))
 
-    for _ in range(args.warmup):
+    for _ in range(max(3, args.warmup)):
         step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step()
     dt = (time.perf_counter() - t0) / args.steps
+    pool.shutdown()
     value = flops / dt / 1e9
+    native = loaded_native_libs()
+    if any("clspmv_mic_b200" in n for n in native):
+        raise RuntimeError(f"the reference arm mapped this library: {native}")
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(dt * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "csr_spmv (the reference's serial CPU path) over stencil27 128^3, powerlaw 2^20, "
                                "blocks4x4 500k x 8" + (" (small)" if args.small else ""),
                    "parallelism": f"{threads} host threads, each running csr_spmv on a block of rows with "
                                   "nnz / threads nonzeros"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference" if use_ref else "port",
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{args.steps} steps of csr_spmv over the three matrices"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "native_libs": native,
     }
-    pool.shutdown()
     print(json.dumps(line), flush=True)
     return 0
 
 
+def headline(*, value, world, steps, warmup, ms_per_step, small, roofline, e2e, launches, clocks, cpu_baseline,
+             parity, fracs, ell_width, gather_peak):
+    """The line the driver parses: compact (well under 2 KB), printed last."""
+    return {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": WORKLOAD + (" (SMALL)" if small else ""), "global_batch": 1,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "no flush: every matrix > 126 MB L2", "ell_width": ell_width},
+        "roofline": roofline,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": {k: clocks.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "cpu_baseline": cpu_baseline,
+        "parity": parity,
+        "format_frac": fracs,
+        "gather_peak_g_per_s": gather_peak,
+    }
+
+
 def run_ours(args):
     import torch
+    from concurrent.futures import ThreadPoolExecutor
+
     from clspmv_mic_b200 import formats as F
     from clspmv_mic_b200 import synth
 
@@ -451,7 +574,8 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()          # sampling starts before the warm-up so it covers the timed region
     t_warm = time.perf_counter()
-    for _ in range(max(3, args.warmup)):
+    warmup = max(3, args.warmup)
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     while time.perf_counter() - t_warm < 0.5:   # keep the GPU busy while nvidia-smi spins up
@@ -526,6 +650,7 @@ def run_ours(args):
     e2e_ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
         e2e_ms = max_over_ranks(e2e_ms, dev)
+    del hx, hy, dx
 
     # the ELL part and its COO tail together carry the matrix's flops once
     flops_step = sum(format_flops(it) for it in items if it["part_of"] is None) + \
@@ -550,12 +675,13 @@ def run_ours(args):
         formats[it["key"]] = {
             "matrix": it["matrix"], "ms": round(float(med[j]), 5), "gflops": round(format_flops(it) / (med[j] * 1e-3) / 1e9, 2),
             "gbs": round(ab / (med[j] * 1e-3) / 1e9, 1), "frac": round(ab / (med[j] * 1e-3) / 1e9 / peak, 3),
+            "frac_useful": round(useful / (med[j] * 1e-3) / 1e9 / peak, 3),
             "alg_bytes": ab, "useful_bytes": useful, "nnz": it["nnz"], "rows": it["rows"],
         }
         if gather_peak and it["matrix"] == "powerlaw":
             g = it["nnz"] / (med[j] * 1e-3)
             formats[it["key"]].update(gathers_per_s=round(g / 1e9, 1), gather_frac=round(g / gather_peak, 3))
-    # the CSR-vector / CSR-scalar variants, outside the timed step
+    # the CSR-vector / CSR-scalar / merge-path / planned-SELL variants, outside the timed step
     variant_stats = {}
     for it in variants:
         with torch.cuda.stream(stream):
@@ -583,43 +709,84 @@ def run_ours(args):
     dom_it = items[dom]
     ab = algorithmic_bytes(dom_it)
     achieved = ab / (mean[dom] * 1e-3) / 1e9
-    traffic = ncu_traffic().get(dom_it["key"])
-    line = {
-        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-        "config": {
-            "workload": "per-format FP32 sweep: stencil27 128^3 -> DIA,BDIA; powerlaw 2^20 Zipf(2.0) mean 16 "
-                        "-> CSR(merge,vector,scalar),COO,ELL(K)+COO tail,SELL-32; 4x4 blocks 500k x 8 -> "
-                        "BELL,SBELL,BCSR" + (" (SMALL)" if args.small else ""),
-            "global_batch": 1, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-            "l2": "no flush: every matrix exceeds the 126 MB L2 and the formats run back to back",
-            "ell_width": meta["ell_width"],
-        },
-        "roofline": {"bound": "hbm", "kernel": dom_it["key"], "achieved": round(achieved, 1), "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
-                     "traffic": traffic, "alg_bytes_per_launch": ab},
-        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": round(e2e_ms, 4)},
-        "gather_peak_per_s": None if gather_peak is None else round(gather_peak / 1e9, 1),
-        "gpu_launches": int(launches),
-        "clocks": clk,
-        "formats": formats,
-        "variants": variant_stats,
-    }
-    if not args.no_extras and not args.only and world == 1:
-        line["extras"] = run_extras(args, items, mats, peak)
-        line["extras"]["cocktail_c3"] = run_cocktail_c3(args, peak)
-        line["extras"]["iterate_c1"] = run_iterate_c1()
+    useful_dom = 12 * dom_it["nnz"] + 4 * dom_it["cols"] + 8 * dom_it["rows"]
+    fr = {k: v["frac"] for k, v in formats.items()}
+    min_key = min(fr, key=fr.get)
+    roofline = {"bound": "hbm", "kernel": dom_it["key"], "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                "frac_useful": round(useful_dom / (mean[dom] * 1e-3) / 1e9 / peak, 3),
+                "min_frac": fr[min_key], "min_frac_kernel": min_key,
+                "traffic": ncu_traffic().get(dom_it["key"]), "alg_bytes_per_launch": ab,
+                "share_of_step": round(float(mean[dom] / mean.sum()), 3)}
+    e2e = {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "ms_per_step": round(e2e_ms, 4)}
+
+    # CPU leg (rank 0 at N=1): the reference's csr_spmv as the baseline,
+    # and every format's y at full size against it and the FP64 oracle
+    cpu_baseline = None
+    parity = None
+    detail = {"formats": formats, "variants": variant_stats}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t_cpu, f_cpu, kind, sample = cpu_csr_seconds(mats)
-        line["cpu_baseline"] = {"value": round(f_cpu / t_cpu / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
-                                "sample": sample}
+        csrs = {name: ref_csr(arrs) for name, arrs in mats.items()}
+        xh = {name: synth.x_vector(arrs[1]) for name, arrs in mats.items()}
+        t_cpu, f_cpu, kind, sample = cpu_csr_seconds(csrs, xh)
+        cpu_baseline = {"value": round(f_cpu / t_cpu / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
+                        "sample": sample}
+        threads = host_threads()
+        with ThreadPoolExecutor(threads) as pool:
+            oracles = {name: Oracle(csrs[name], xh[name], pool, threads) for name in mats}
+        parity, detail["parity"] = check_parity(items + variants, xs, oracles, stream)
+        del csrs, oracles
+
+    if not args.no_extras and not args.only and world == 1:
+        for name, fn in (("extras", lambda: run_extras(args, items, mats, peak)),
+                         ("cocktail_c3", lambda: run_cocktail_c3(args, peak)),
+                         ("iterate_c1", run_iterate_c1)):
+            detail[name] = fn()
+            if rank == 0:
+                print(json.dumps({"detail": name, **detail[name]}), flush=True)
+    line = headline(value=value, world=world, steps=args.steps, warmup=warmup, ms_per_step=ms_per_step,
+                    small=args.small, roofline=roofline, e2e=e2e, launches=launches, clocks=clk,
+                    cpu_baseline=cpu_baseline, parity=parity, fracs=fr, ell_width=meta["ell_width"],
+                    gather_peak=None if gather_peak is None else round(gather_peak / 1e9, 1))
     if rank == 0:
+        print(json.dumps({"detail": "formats", "formats": formats, "variants": variant_stats,
+                          "parity": detail.get("parity"), "clocks": clk}), flush=True)
+        if args.detail_file:
+            Path(args.detail_file).parent.mkdir(parents=True, exist_ok=True)
+            Path(args.detail_file).write_text(json.dumps({"headline": line, **detail}, indent=1))
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def check_parity(items, xs, oracles, stream):
+    """Every format's y = A x at full size (beta = 0; the ELL part and its
+    COO tail accumulate into one y) against the reference's csr_spmv within
+    the per-row bound 1e-5 sum|a x|, and its error against the FP64 oracle.
+    Returns (summary for the headline, per-format detail)."""
+    import torch
+    per = {}
+    groups = {}
+    for it in items:
+        groups.setdefault(it["part_of"] or it["key"], []).append(it)
+    for key, parts in groups.items():
+        m = parts[0]["matrix"]
+        y = torch.zeros(parts[0]["rows"], dtype=torch.float32, device=xs[m].device)
+        with torch.cuda.stream(stream):
+            for j, it in enumerate(parts):
+                it["dev"].spmv(xs[m], y, 1.0, 0.0 if j == 0 else 1.0, stream=stream, **it["kw"])
+        torch.cuda.synchronize()
+        over, e64 = oracles[m].check(y.cpu().numpy())
+        per[key] = {"matrix": m, "rows_over_bound": over, "max_err_fp64": e64}
+    summary = {"checked": sorted(per), "rows_over_bound": int(sum(v["rows_over_bound"] for v in per.values())),
+               "max_err_fp64": max((v["max_err_fp64"] for v in per.values()), default=0.0),
+               "ref_err_fp64": max(o.ref_err64() for o in oracles.values()),
+               "bound": "per row |y-y_ref| <= 1e-5 sum|a x|, full size"}
+    summary["max_err_fp64"] = float(f"{summary['max_err_fp64']:.3g}")
+    summary["ref_err_fp64"] = float(f"{summary['ref_err_fp64']:.3g}")
+    return summary, per
 
 
 def run_device_convert(items):

@@ -267,7 +267,16 @@ int read_mmf(const char* filename, coo_matrix<int, float>* mat)
             mat->coo_data[k++] = v[i];
         }
     }
-    if (!if_sorted_coo(mat)) sort_entries(mat->coo_row_id, mat->coo_col_id, mat->coo_data, total, (int)height);
+    if (!if_sorted_coo(mat)) {
+        // sort_entries counts rows in [0, height); a mirrored entry of a
+        // non-square symmetric file has row = its column, which can reach
+        // width - 1 >= height: such input takes sort_coo, which compares keys
+        // and indexes nothing by row (the reference sorts it the same way)
+        bool rows_in_range = true;
+        for (size_t i = 0; i < total && rows_in_range; i++) rows_in_range = mat->coo_row_id[i] < height;
+        if (rows_in_range) sort_entries(mat->coo_row_id, mat->coo_col_id, mat->coo_data, total, (int)height);
+        else sort_coo(mat);
+    }
     return CLSPMV_OK;
 }
 

@@ -41,7 +41,10 @@ static __device__ __align__(256) int g_noalloc_plan[2 * (kNoallocMaxTiles + 1)];
 std::mutex g_noalloc_mu;
 int* g_noalloc_ptr[kNoallocMaxDevices] = {};
 
-// Device address of g_noalloc_plan on the current device, looked up once.
+// Device address of g_noalloc_plan on the current device, looked up once per
+// device and kept for the life of the process; a cudaDeviceReset destroys
+// the device's copy of the array, so the cached address is not valid after
+// one (documented at the entry point's declaration).
 int noalloc_plan(int** out)
 {
     int dev = 0;

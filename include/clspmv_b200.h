@@ -367,6 +367,9 @@ int clspmv_csr_chunk_spmv_f32(const clspmv_csr_f32* dev, const int* chunk_row, c
  *    is launched;
  *  - the first call on each device (with that device current) looks the
  *    array up; make it before starting any stream capture on that device;
+ *  - the looked-up address is kept for the life of the process: after
+ *    cudaDeviceReset on a device (which destroys its copy of the array),
+ *    do not call this entry point on that device again;
  *  - nothing needs to start at zero: each call writes the whole plan it
  *    reads, in `stream`, before its SpMV kernel;
  *  - there is one array per device, so calls on one device must not

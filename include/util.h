@@ -1,6 +1,6 @@
 /*
  * util.h — host helpers, source-compatible with include/util.h of clSpMV
- * (src/util.cpp). Implemented in libclspmv_b200 (csrc/host_util.cpp).
+ * (src/util.cpp). Implemented in libclspmv_b200 (clspmv_mic_b200/csrc/compat.cpp).
  */
 #ifndef CLSPMV_UTIL_H
 #define CLSPMV_UTIL_H

@@ -12,6 +12,7 @@ this module.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -23,7 +24,9 @@ from clspmv_mic_b200.formats import HostMatrix
 HERE = Path(__file__).resolve().parent
 PORT_LIB = HERE / "libclspmv_oracle.so"
 REF_LIB = HERE / "_ref" / "libclspmv_ref.so"
-REFERENCE_TREE = Path("/root/reference")
+# the reference checkout the recipe compiles from (absent on machines that
+# only run the prebuilt oracle/_ref library); CLSPMV_REFERENCE overrides it
+REFERENCE_TREE = Path(os.environ.get("CLSPMV_REFERENCE", "/root/reference"))
 
 _port = None
 _ref = None
@@ -131,15 +134,26 @@ def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def _x_padded(x):
+    """x followed by 64 zeros. The reference's serial block products
+    (bell_spmv, include/spmv_serial.h:251-279) read x up to a block's width
+    past the last block column without a bound check, so every oracle call
+    gets a buffer with zero padding; the logical length stays x.size."""
+    x = _f32(x)
+    xp = np.zeros(x.size + 64, dtype=np.float32)
+    xp[:x.size] = x
+    return xp, x.size
+
+
 def spmv_port(m: HostMatrix, x: np.ndarray, y: np.ndarray | None = None, out_len: int | None = None) -> np.ndarray:
     """result += A x with the C restatement; returns the result array."""
     L = port()
-    x = _f32(x)
+    x, nx = _x_padded(x)
     n = out_len if out_len is not None else m.shape[0]
     res = np.zeros(n, dtype=np.float32) if y is None else _f32(y).copy()
     fn = getattr(L, f"orc_{m.fmt}_spmv_f32")
     if m.fmt in ("dia", "bdia", "bcsr"):
-        fn(C.byref(m.struct), x.ctypes.data, res.ctypes.data, x.size)
+        fn(C.byref(m.struct), x.ctypes.data, res.ctypes.data, nx)
     else:
         fn(C.byref(m.struct), x.ctypes.data, res.ctypes.data)
     return res
@@ -148,10 +162,10 @@ def spmv_port(m: HostMatrix, x: np.ndarray, y: np.ndarray | None = None, out_len
 def spmv_ref(m: HostMatrix, x: np.ndarray, y: np.ndarray | None = None, out_len: int | None = None) -> np.ndarray:
     """result += A x with the reference's own <fmt>_spmv."""
     L = ref()
-    x = _f32(x)
+    x, nx = _x_padded(x)
     n = out_len if out_len is not None else m.shape[0]
     res = np.zeros(n, dtype=np.float32) if y is None else _f32(y).copy()
-    getattr(L, f"ref_{m.fmt}_spmv")(C.byref(m.struct), x.ctypes.data, res.ctypes.data, x.size)
+    getattr(L, f"ref_{m.fmt}_spmv")(C.byref(m.struct), x.ctypes.data, res.ctypes.data, nx)
     return res
 
 

@@ -50,7 +50,10 @@ int main(int argc, char** argv)
     if (coo.matinfo.nnz == 0) return 3;
     printMatInfo(&coo);
     const int h = coo.matinfo.height, w = coo.matinfo.width;
-    std::vector<float> x(w);
+    // the block formats' serial products read x up to the last block's
+    // width past the last block column (the reference's bell_spmv does not
+    // check), so x carries zero padding beyond its w entries
+    std::vector<float> x((size_t)w + 64, 0.0f);
     for (int i = 0; i < w; i++) x[i] = (float)(((i * 7) % 13) - 6) * 0.375f;
     FILE* f = fopen(argv[2], "wb");
     if (!f) return 4;

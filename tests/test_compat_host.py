@@ -241,6 +241,26 @@ def test_read_mmf_random_files_match_reference(tmp_path):
         assert_same_coo(read_mmf(p), ref_read(p))
 
 
+@pytest.mark.parametrize("h,w", [(7, 19), (19, 7), (1, 40)])
+def test_read_mmf_nonsquare_symmetric_matches_reference(tmp_path, h, w):
+    """A 'symmetric' file that is not square, with entries above the
+    diagonal: each mirrored entry takes its column as its row, which reaches
+    past the declared height when width > height. Read without writing out
+    of bounds, and sorted into the same COO as the reference's ReadMMF."""
+    ref_or_skip()
+    rng = np.random.default_rng(h * 100 + w)
+    mask = np.triu(rng.random((h, w)) < 0.4, k=1)      # strictly above the diagonal: no mirrored duplicates
+    d = np.arange(0, min(h, w), 3)
+    mask[d, d] = True                                  # some diagonal entries (not mirrored)
+    r, c = np.nonzero(mask)
+    v = np.round(rng.standard_normal(r.size), 3)
+    p = tmp_path / "nonsquare_sym.mtx"
+    write_mtx(p, h, w, r, c, v, symmetry="symmetric", order=rng.permutation(r.size))
+    ours = read_mmf(p)
+    assert ours.nnz == r.size + int((r != c).sum())
+    assert_same_coo(ours, ref_read(p))
+
+
 @pytest.mark.parametrize("field,symmetry", [("real", "general"), ("pattern", "general"), ("real", "symmetric")])
 def test_read_mmf_large_files_match_reference(tmp_path, field, symmetry):
     """Files of several MB, so the entry text is cut into ranges parsed on
