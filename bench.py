@@ -165,8 +165,9 @@ def build_workload(small: bool, only=None):
 def algorithmic_bytes(it) -> int:
     """Arrays the kernel must stream (values, indices, pointers, padding),
     plus x read once and y read and written once. SELL with its length plan
-    reads each row only up to its last real entry: those entries, the row
-    lengths, the tail items and the slice pointers."""
+    reads, of each slice column, only the 32-byte sectors holding real
+    entries: those sectors of col and data, the row lengths and the slice
+    pointers."""
     if it.get("needed") is not None:
         return int(it["needed"] + 4 * it["cols"] + 8 * it["rows"])
     return int(it["stored"] + 4 * it["cols"] + 8 * it["rows"])
@@ -550,10 +551,9 @@ def run_ours(args):
         if it["host"].fmt == "csr" and it["kw"].get("variant") == "chunk":
             it["dev"].chunk_plan(stream)
         if it["host"].fmt == "sell" and it["kw"].get("variant") == "planned":
+            # the sectors holding real entries, the row lengths and the slice pointers
             d = it["dev"]
-            n_items = int(F.lib().clspmv_sell_plan_items(d.sell_plan()))
-            it["needed"] = (8 * d.sell_plan_entries() + 4 * it["rows"] + 8 * n_items
-                            + 4 * (it["host"].struct.sell_slice_num + 1))
+            it["needed"] = d.sell_plan_sector_bytes() + 4 * it["rows"] + 4 * (it["host"].struct.sell_slice_num + 1)
         it.pop("host")
     torch.cuda.synchronize()
 
@@ -1033,21 +1033,28 @@ def run_cocktail_c3(args, peak):
     ref = W.Fp64Rows(csr, rows=1 << 15, starts=(0, band, band + block))
     out["err_fp64"] = ref.error(x[:, None], y[:, None])
     del csr, ref
-    for _ in range(5):
-        dev.spmv(x, y, 1.0, 1.0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 20
-    e0.record()
-    for _ in range(reps):
-        dev.spmv(x, y, 1.0, 1.0)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+    def timed(schedule, reps=20):
+        dev.set_schedule(schedule)
+        for _ in range(5):
+            dev.spmv(x, y, 1.0, 1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            dev.spmv(x, y, 1.0, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_fused = timed("fused") if dev.fused_items > 0 else None
+    ms = timed("auto")
     stored = sum(p.stored_bytes() for p in mat.parts().values())
     ab = stored + 4 * w + 8 * h
     out.update(rows=h, nnz=int(coo.nnz), ms=round(ms, 4), gflops=round(2 * coo.nnz / (ms * 1e-3) / 1e9, 1),
                alg_bytes=int(ab), gbs=round(ab / (ms * 1e-3) / 1e9, 1), frac=round(ab / (ms * 1e-3) / 1e9 / peak, 3),
-               note="alg bytes = every part's stored arrays + x once + y read and written once")
+               fused_items=dev.fused_items, ms_fused=None if ms_fused is None else round(ms_fused, 4),
+               note="alg bytes = every part's stored arrays + x once + y read and written once; ms = the runtime's "
+                    "default schedule (one launch per part), ms_fused = one persistent launch over all parts "
+                    "from an interleaved work list")
     dev.close()
     return out
 

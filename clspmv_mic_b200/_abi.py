@@ -223,6 +223,9 @@ def _declare(lib):
         "clspmv_coo_spmv_f32": (I32, [S["coo"], VP, VP, f32, f32, VP]),
         "clspmv_dia_spmv_f32": (I32, [S["dia"], VP, VP, f32, f32, VP]),
         "clspmv_bdia_spmv_f32": (I32, [S["bdia"], VP, VP, f32, f32, VP]),
+        "clspmv_dia_bulk_spmv_f32": (I32, [S["dia"], VP, VP, f32, f32, VP]),
+        "clspmv_bdia_bulk_spmv_f32": (I32, [S["bdia"], VP, VP, f32, f32, VP]),
+        "clspmv_pipeline_timeouts": (I32, [C.POINTER(C.c_uint)]),
         "clspmv_ell_spmv_f32": (I32, [S["ell"], VP, VP, f32, f32, VP]),
         "clspmv_sell_spmv_f32": (I32, [S["sell"], VP, VP, f32, f32, VP]),
         "clspmv_b4ell_spmv_f32": (I32, [S["b4ell"], VP, VP, f32, f32, VP]),
@@ -234,6 +237,8 @@ def _declare(lib):
         "clspmv_cocktail_spmv_f32": (I32, [VP, VP, VP, f32, f32, VP]),
         "clspmv_cocktail_device_view": (I32, [VP, P(Cocktail)]),
         "clspmv_cocktail_iterate_f32": (I32, [VP, VP, VP, f32, f32, I32, VP]),
+        "clspmv_cocktail_set_schedule": (I32, [VP, I32]),
+        "clspmv_cocktail_fused_items": (I32, [VP]),
         "clspmv_cocktail_free": (I32, [VP]),
         "clspmv_run_method_f32": (I32, [S["coo"], I32, I32, I32, P(BenchResult)]),
         "clspmv_bandwidth_test": (I32, [C.c_size_t, I32, I32, P(C.c_double), P(C.c_double)]),
@@ -250,6 +255,7 @@ def _declare(lib):
         "clspmv_sell_plan_spmv_f32": (I32, [S["sell"], VP, VP, VP, f32, f32, VP]),
         "clspmv_sell_plan_entries": (C.c_longlong, [VP]),
         "clspmv_sell_plan_items": (C.c_longlong, [VP]),
+        "clspmv_sell_plan_sector_bytes": (C.c_longlong, [VP]),
         "clspmv_sell_plan_free": (I32, [VP]),
         "clspmv_pack_values": (I32, [I32, VP, I32, VP, VP, VP]),
         "clspmv_batch_create": (I32, [I32, P(VP)]),

@@ -125,6 +125,19 @@ class DeviceCocktail:
         self.parts = [p for p, _ in COCKTAIL_PARTS if host.uses(p)]
         self.stored_bytes = sum(m.stored_bytes() for m in host.parts().values())
 
+    SCHEDULES = {"auto": 0, "fused": 1, "per_part": 2}
+
+    def set_schedule(self, schedule: str) -> None:
+        """"auto" (= "per_part": one launch per part on forked streams) or
+        "fused" (one persistent launch over all parts from an interleaved
+        work list; refused where a part is not covered)."""
+        check(lib().clspmv_cocktail_set_schedule(self.handle, self.SCHEDULES[schedule]), "cocktail_set_schedule")
+
+    @property
+    def fused_items(self) -> int:
+        """Work-list entries of the fused schedule (0: the handle has none)."""
+        return int(lib().clspmv_cocktail_fused_items(self.handle))
+
     def spmv(self, x, y, alpha: float = 1.0, beta: float = 1.0, stream=None) -> None:
         """y <- alpha * A x + beta * y, asynchronous on `stream`."""
         from .formats import _stream_handle

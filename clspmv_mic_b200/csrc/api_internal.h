@@ -30,4 +30,21 @@ int launch_sbell(const clspmv_sbell_f32* m, const float* x, float* y, float alph
 int launch_packed(int format, const void* dev, int value_type, const void* values, const float* scale, const int* tc,
                   const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_b4csr(const clspmv_b4csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+
+// DIA / BDIA with the diagonals staged in shared memory by bulk copies
+// (diag_bulk.cu); BDIA passes its bptr (the diagonal count is read on the
+// device), DIA bptr = nullptr and its ndiag.
+bool diag_bulk_supported(int len, const void* data);
+int launch_diag_bulk(int rows, int cols, int ndiag, int len, const int* offsets, const int* bptr, int nband,
+                     const float* data, const float* x, float* y, float alpha, float beta, cudaStream_t st);
+
+// Fused Cocktail SpMV (cocktail_fused.cu): the parts of a partitioned matrix
+// (device struct) cut into tiles, interleaved into one work list and run by
+// one persistent launch. fused_plan_create returns CLSPMV_ERR_UNSUPPORTED
+// when a part's layout is outside what the fused kernel covers.
+struct FusedPlan;
+int fused_plan_create(const clspmv_cocktail_f32* dev, const int* chunk_plan, FusedPlan** out);
+int fused_spmv(const FusedPlan* plan, const float* x, float* y, float alpha, float beta, cudaStream_t st);
+void fused_plan_free(FusedPlan* plan);
+int fused_plan_items(const FusedPlan* plan);
 }  // namespace clspmv

@@ -13,6 +13,7 @@
 // without host round trips (the reference's A^k x loop, src/eval.cpp:19-72,
 // synchronises after every step).
 #include <cstddef>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -25,6 +26,8 @@ struct clspmv_cocktail_handle {
     clspmv_cocktail_f32 dev;          // part structs with device pointers
     int* chunk_plan = nullptr;        // first row of every nonzero chunk of the CSR part
     int nparts = 0;
+    FusedPlan* fused = nullptr;       // one persistent launch over all parts (two or more parts)
+    int schedule = CLSPMV_SCHEDULE_AUTO;
     cudaStream_t streams[9] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[9] = {};
@@ -93,6 +96,7 @@ void release(clspmv_cocktail_handle* h)
         if (h->join[i]) cudaEventDestroy(h->join[i]);
     }
     if (h->fork) cudaEventDestroy(h->fork);
+    if (h->fused) fused_plan_free(h->fused);
     if (h->iter_exec) cudaGraphExecDestroy(h->iter_exec);
     if (h->cap) cudaStreamDestroy(h->cap);
 }
@@ -191,6 +195,11 @@ int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_
         if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->join[p], cudaEventDisableTiming));
     }
     if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+    if (!rc && h->nparts >= 2) {
+        // a part layout the fused kernel does not cover keeps the per-part launches
+        const int frc = fused_plan_create(&h->dev, h->chunk_plan, &h->fused);
+        if (frc != CLSPMV_ERR_UNSUPPORTED) rc = frc;
+    }
     if (rc) {
         release(h);
         delete h;
@@ -210,6 +219,10 @@ int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y
     if (h->nparts == 1) {
         for (int p = 0; p < P_COUNT; p++)
             if (uses(h->dev, p)) return launch_part(h, p, x, y, alpha, beta, st, false);
+    }
+    if (h->schedule == CLSPMV_SCHEDULE_FUSED) {
+        if (!h->fused) return CLSPMV_ERR_UNSUPPORTED;
+        if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) return fused_spmv(h->fused, x, y, alpha, beta, st);
     }
     int rc = launch_prescale(y, rows, beta, st);
     if (rc) return rc;
@@ -240,6 +253,20 @@ int clspmv_cocktail_iterate_f32(clspmv_cocktail_handle* h, float* x, float* y, f
     if (!rc) rc = iterate_steps(h, x, y, alpha, beta, rest, st);
     return rc;
 }
+
+int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule)
+{
+    if (!h || schedule < CLSPMV_SCHEDULE_AUTO || schedule > CLSPMV_SCHEDULE_PER_PART) return CLSPMV_ERR_ARG;
+    if (schedule == CLSPMV_SCHEDULE_FUSED && !h->fused) return CLSPMV_ERR_UNSUPPORTED;
+    h->schedule = schedule;
+    if (h->iter_exec) {   // the cached iteration graph was captured under the old schedule
+        cudaGraphExecDestroy(h->iter_exec);
+        h->iter_exec = nullptr;
+    }
+    return CLSPMV_OK;
+}
+
+int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h) { return h ? fused_plan_items(h->fused) : -1; }
 
 int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail_f32* out)
 {

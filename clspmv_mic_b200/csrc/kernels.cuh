@@ -469,6 +469,87 @@ __device__ __forceinline__ void sell_tail_cta(const SellArgs& a, const int* __re
     }
 }
 
+// SELL with the padding skipped, on the column-balanced mapping of sell_cta:
+// the Q lanes of a column each own 4 rows of the slice, and a lane issues its
+// 128-bit loads only for the columns before the longest real length of its 4
+// rows (rlen, from the plan). A slice padded to the width of one long row then
+// reads, in its tail columns, the 32-byte sectors of that row only (the
+// padded read takes the whole 128-byte line of 32 rows per column and
+// array), while the warp still walks the slot space in equal runs of columns.
+// Requires slice_height = 4 Q, 16-byte aligned arrays and beta already
+// applied.
+template <int Q, bool ATOMIC_ALL>
+__device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __restrict__ rlen, int cta, int ncta)
+{
+    constexpr int G = 32 / Q;             // columns per warp step
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    const int sh = Q * 4;
+    const long long total_cols = (long long)a.slice_ptr[a.nslice] / sh;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / Q, q = lane % Q;
+    const long long nwarps_total = (long long)ncta * (kBlock / 32);
+    const long long wid = (long long)cta * (kBlock / 32) + (threadIdx.x >> 5);
+    for (long long c0 = wid * kSellWarpCols; c0 < total_cols; c0 += nwarps_total * kSellWarpCols) {
+        const long long c1 = min(c0 + kSellWarpCols, total_cols);
+        int lo = 0, hi = a.nslice - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((long long)a.slice_ptr[mid + 1] <= c0 * sh) lo = mid + 1;
+            else hi = mid;
+        }
+        int s = lo;
+        long long c = c0;
+        while (c < c1) {
+            const long long sb = a.slice_ptr[s] / sh, se = a.slice_ptr[s + 1] / sh;
+            if (se <= c) {
+                s++;
+                continue;
+            }
+            const long long ce = min(c1, se);
+            const long long row0 = (long long)s * sh + 4 * q;
+            int live = 0;                 // columns sb .. sb + live - 1 hold real entries of this lane's rows
+            if (row0 + 3 < a.rows) {
+                const int4 l = __ldg(reinterpret_cast<const int4*>(rlen + row0));
+                live = max(max(l.x, l.y), max(l.z, l.w));
+            } else {
+                for (int i = 0; i < 4; i++)
+                    if (row0 + i < a.rows) live = max(live, __ldg(rlen + row0 + i));
+            }
+            const long long klim = sb + live;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+            for (long long cc = c + g; cc < ce; cc += G) {
+                if (cc < klim) {
+                    const size_t base = (size_t)cc * sh + 4 * q;
+                    const int4 cv = ld_stream_i4(a.col + base, pe);
+                    const float4 v = ld_stream_f4(a.data + base, pe);
+                    acc[0] = fmaf(v.x, ld_x(a.x + cv.x, pl), acc[0]);
+                    acc[1] = fmaf(v.y, ld_x(a.x + cv.y, pl), acc[1]);
+                    acc[2] = fmaf(v.z, ld_x(a.x + cv.z, pl), acc[2]);
+                    acc[3] = fmaf(v.w, ld_x(a.x + cv.w, pl), acc[3]);
+                }
+            }
+#pragma unroll
+            for (int off = Q; off < 32; off <<= 1) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(kFull, acc[i], off);
+            }
+            if (g == 0) {
+                const bool whole = sb >= c0 && se <= c1;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (row0 + i < a.rows) {
+                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += a.alpha * acc[i];
+                        else atomicAdd(a.y + row0 + i, a.alpha * acc[i]);
+                    }
+                }
+            }
+            c = ce;
+            s++;
+        }
+    }
+}
+
 // Other slice heights: one row per thread, slice by slice.
 template <bool ATOMIC, class V>
 __device__ __forceinline__ void sell_rows_cta(const SellArgsT<V>& a, int cta, int ncta, char*)

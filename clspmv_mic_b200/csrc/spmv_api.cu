@@ -76,10 +76,12 @@ __global__ void __launch_bounds__(kBlock, 5) k_bdia_occ(BdiaArgsT<V> a) { bdia_c
 
 // Kernel form of the diagonal formats: 0 scalar x loads, 1 aligned x
 // windows, 2 aligned x windows with the register cap, 3 (DIA) one aligned
-// window per lane completed by shuffles. Measured on B200 (stencil27 128^3):
+// window per lane completed by shuffles, 4 diagonals staged in shared memory
+// by bulk copies (diag_bulk.cu; FP32 values, own rows only). Measured on B200 (stencil27 128^3):
 // DIA is fastest with form 0 (74.6 % of peak vs 60 / 72 / 53), BDIA with
 // form 1 (78 % vs 69 / 75). CLSPMV_DIA_FORM overrides both (for
 // measurements).
+constexpr int kDiaDefaultForm = 0, kBdiaDefaultForm = 1;
 int dia_form(int dflt)
 {
     static int forced = [] {
@@ -108,6 +110,11 @@ __global__ void __launch_bounds__(kBlock) k_sell_rlen(const int* __restrict__ sl
         rlen[r] = sell_row_length(slice_ptr, col, data, sh, r);
 }
 
+template <int Q, bool A>
+__global__ void __launch_bounds__(kBlock) k_sell_masked(SellArgs a, const int* __restrict__ rlen)
+{
+    sell_masked_cta<Q, A>(a, rlen, blockIdx.x, gridDim.x);
+}
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_sell_head(SellArgs a, const int* __restrict__ rlen)
 {
@@ -274,7 +281,12 @@ int launch_dia_v(const clspmv_dia_f32* m, const V* data, const float* scale, con
     if (m->dia_num > 0 && (!m->dia_offsets || !data)) return CLSPMV_ERR_ARG;
     if ((m->dia_length_aligned & 3) || !aligned_v4(data) || rows > m->dia_length_aligned) return CLSPMV_ERR_ALIGN;
     DiaArgsT<V> a{rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, data, x, y, alpha, beta, scale};
-    const int form = aligned16(x) ? dia_form(0) : 0;
+    const int form = aligned16(x) ? dia_form(kDiaDefaultForm) : 0;
+    if constexpr (std::is_same<V, float>::value) {
+        if (form == 4 && !atomic && m->dia_num > 0 && diag_bulk_supported(m->dia_length_aligned, data))
+            return launch_diag_bulk(rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, nullptr, 0,
+                                    data, x, y, alpha, beta, st);
+    }
     auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a); };
     if (atomic) {
         if (form == 3) go(k_dia<true, V, 3>);
@@ -305,7 +317,12 @@ int launch_bdia_v(const clspmv_bdia_f32* m, const V* data, const float* scale, c
     if (m->bdia_band_num > 0 && (!m->bdia_offsets || !m->bdia_bptr || !data)) return CLSPMV_ERR_ARG;
     if ((m->bdia_length_aligned & 3) || !aligned_v4(data) || rows > m->bdia_length_aligned) return CLSPMV_ERR_ALIGN;
     BdiaArgsT<V> a{rows, m->matinfo.width, m->bdia_band_num, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr, data, x, y, alpha, beta, scale};
-    const int form = aligned16(x) ? dia_form(1) : 0;
+    const int form = aligned16(x) ? dia_form(kBdiaDefaultForm) : 0;
+    if constexpr (std::is_same<V, float>::value) {
+        if (form == 4 && !atomic && m->bdia_band_num > 0 && diag_bulk_supported(m->bdia_length_aligned, data))
+            return launch_diag_bulk(rows, m->matinfo.width, 0, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr,
+                                    m->bdia_band_num, data, x, y, alpha, beta, st);
+    }
     auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a); };
     if (atomic) {
         if (form == 2) go(k_bdia_occ<true, V, true>);
@@ -397,6 +414,22 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
     if (m->sell_slice_height == 0) return CLSPMV_ERR_ARG;
     SellArgs a{rows, (int)m->sell_slice_height, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, m->sell_data,
                x, y, alpha, beta, nullptr};
+    const int sh = (int)m->sell_slice_height;
+    if (aligned16(m->sell_col_id) && aligned16(m->sell_data) && aligned16(rlen) &&
+        (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
+        // column-balanced walk with each lane's loads cut at its rows' real length
+        if (!atomic) {
+            int rc = prescale(y, rows, beta, st);
+            if (rc) return rc;
+        }
+        a.beta = 1.0f;
+        return dispatch_lanes(sh / 4, [&](auto q) {
+            constexpr int Q = decltype(q)::value;
+            if (atomic) k_sell_masked<Q, true><<<persistent_grid(k_sell_masked<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen);
+            else k_sell_masked<Q, false><<<persistent_grid(k_sell_masked<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen);
+            return after_launch(1);
+        });
+    }
     if (atomic) k_sell_head<true><<<persistent_grid(k_sell_head<true>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
     else k_sell_head<false><<<persistent_grid(k_sell_head<false>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
     int rc = after_launch(1);
@@ -712,6 +745,28 @@ int clspmv_csr_chunk_spmv_f32(const clspmv_csr_f32* m, const int* chunk_row, con
 
 int clspmv_dia_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_dia(m, x, y, alpha, beta, S(s), false); }
+int clspmv_dia_bulk_spmv_f32(const clspmv_dia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    if (m->matinfo.height <= 0) return CLSPMV_OK;
+    if (m->dia_num <= 0) return launch_dia(m, x, y, alpha, beta, S(s), false);
+    if (!m->dia_offsets || !m->dia_data) return CLSPMV_ERR_ARG;
+    if (m->matinfo.height > m->dia_length_aligned || !diag_bulk_supported(m->dia_length_aligned, m->dia_data))
+        return CLSPMV_ERR_ALIGN;
+    return launch_diag_bulk(m->matinfo.height, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, nullptr,
+                            0, m->dia_data, x, y, alpha, beta, S(s));
+}
+int clspmv_bdia_bulk_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{
+    if (!m || !x || !y) return CLSPMV_ERR_ARG;
+    if (m->matinfo.height <= 0) return CLSPMV_OK;
+    if (m->bdia_band_num <= 0) return launch_bdia(m, x, y, alpha, beta, S(s), false);
+    if (!m->bdia_offsets || !m->bdia_bptr || !m->bdia_data) return CLSPMV_ERR_ARG;
+    if (m->matinfo.height > m->bdia_length_aligned || !diag_bulk_supported(m->bdia_length_aligned, m->bdia_data))
+        return CLSPMV_ERR_ALIGN;
+    return launch_diag_bulk(m->matinfo.height, m->matinfo.width, 0, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr,
+                            m->bdia_band_num, m->bdia_data, x, y, alpha, beta, S(s));
+}
 int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
 { return launch_bdia(m, x, y, alpha, beta, S(s), false); }
 int clspmv_ell_spmv_f32(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
@@ -722,6 +777,7 @@ struct clspmv_sell_plan {
     int* rlen = nullptr;       // device: stored length of every row (padding excluded)
     int2* items = nullptr;     // device: (row, first entry) of each tail item
     long long rows = 0, nitems = 0, entries = 0;
+    long long sector_bytes = 0;   // col + data bytes of the 32-byte sectors holding real entries
 };
 
 int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
@@ -746,6 +802,15 @@ int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
             p->entries += rlen[r];
             for (int k = kSellHead; k < rlen[r]; k += kSellTailCols) items.push_back(make_int2((int)r, k));
         }
+        // a 32-byte sector of one slice column holds 8 consecutive rows (slice
+        // starts are multiples of the slice height): per group of 8 rows, the
+        // longest real length counts sectors in each of col and data
+        const long long sh = (long long)m->sell_slice_height;
+        for (long long r0 = 0; r0 < rows; r0 += 8) {
+            int mx = 0;
+            for (long long r = r0; r < std::min(rows, r0 + 8) && (r / sh) == (r0 / sh); r++) mx = std::max(mx, rlen[r]);
+            p->sector_bytes += 2LL * 32 * mx;
+        }
         p->nitems = (long long)items.size();
         rc = cuda_status(cudaMalloc(&p->items, sizeof(int2) * std::max<size_t>(1, items.size())));
         if (!rc && !items.empty())
@@ -768,6 +833,7 @@ int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* 
 
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* p) { return p ? p->entries : -1; }
 long long clspmv_sell_plan_items(const clspmv_sell_plan* p) { return p ? p->nitems : -1; }
+long long clspmv_sell_plan_sector_bytes(const clspmv_sell_plan* p) { return p ? p->sector_bytes : -1; }
 
 int clspmv_sell_plan_free(clspmv_sell_plan* p)
 {

@@ -285,6 +285,11 @@ class DeviceMatrix:
         """Stored entries the padding-free SELL SpMV reads."""
         return int(lib().clspmv_sell_plan_entries(self.sell_plan()))
 
+    def sell_plan_sector_bytes(self) -> int:
+        """col + data bytes of the 32-byte sectors holding real entries (what
+        the padding-free SELL SpMV must move from the matrix arrays)."""
+        return int(lib().clspmv_sell_plan_sector_bytes(self.sell_plan()))
+
     def __del__(self):
         p = getattr(self, "_sell_plan", None)
         if p:
@@ -319,7 +324,8 @@ class DeviceMatrix:
         """y <- alpha * A x + beta * y on the device (asynchronous on `stream`);
         with `packed`, from the 16-bit values of self.pack(). `variant`: CSR
         "chunk" (default; "merge" when col_id / data are not 16-byte aligned),
-        "merge", "vector" or "scalar"; SELL "planned" reads only each
+        "merge", "vector" or "scalar"; DIA / BDIA "bulk" stages the diagonals
+        in shared memory by bulk copies; SELL "planned" reads only each
         row's real entries (its length plan), which on B200 is slower than the
         padded read for power-law slices: the tails of long rows are strided
         column-major reads."""
@@ -361,6 +367,10 @@ class DeviceMatrix:
         if self.fmt == "sell" and variant == "planned":
             check(L.clspmv_sell_plan_spmv_f32(C.byref(self.struct), self.sell_plan(), x.data_ptr(), y.data_ptr(),
                                               alpha, beta, s), "sell_plan_spmv")
+            return
+        if self.fmt in ("dia", "bdia") and variant == "bulk":
+            name = f"clspmv_{self.fmt}_bulk_spmv_f32"
+            check(getattr(L, name)(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s), name)
             return
         name = _SPMV[self.fmt]
         check(getattr(L, name)(C.byref(self.struct), x.data_ptr(), y.data_ptr(), alpha, beta, s), name)
@@ -544,6 +554,13 @@ def device_spmm_tc(m: "DeviceMatrix", X, Y, alpha: float = 1.0, beta: float = 0.
         raise ValueError("shape mismatch")
     check(lib().clspmv_b4csr_spmm_tc_f32(C.byref(m.struct), k, X.data_ptr(), X.stride(0), Y.data_ptr(), Y.stride(0),
                                          alpha, beta, _stream_handle(stream)), "spmm_tc")
+
+
+def pipeline_timeouts() -> int:
+    """Bounded waits of the bulk-copy pipeline kernels that ran out since the last call (synchronous; resets)."""
+    n = C.c_uint(0)
+    check(lib().clspmv_pipeline_timeouts(C.byref(n)), "pipeline_timeouts")
+    return int(n.value)
 
 
 def tensor_timeouts() -> int:

@@ -391,6 +391,25 @@ int clspmv_coo_spmv_f32(const clspmv_coo_f32* dev, const float* x, float* y,
 int clspmv_dia_spmv_f32(const clspmv_dia_f32* dev, const float* x, float* y,
                         float alpha, float beta, clspmv_stream_t stream);
 
+/* DIA and BDIA with the diagonals staged in shared memory by bulk copies:
+ * per CTA one producer warp streams tiles of 1024 rows, 9 diagonals at a
+ * time, into a ring of three shared-memory stages (cp.async.bulk, mbarrier
+ * handoff with bounded waits) and eight consumer warps compute four rows per
+ * thread from shared memory, x gathered through L1; two CTAs per SM, each
+ * over an equal range of rows. The bytes in flight no longer depend on
+ * registers. Requires dia_length_aligned (bdia_length_aligned) a multiple
+ * of 32 and a 16-byte aligned data array (CLSPMV_ERR_ALIGN otherwise). Same
+ * y as clspmv_dia_spmv_f32 / clspmv_bdia_spmv_f32 up to summation order. A
+ * wait that runs out (about 2 s; none expected) ends the kernel and is
+ * counted for clspmv_pipeline_timeouts. No counterpart in the reference. */
+int clspmv_dia_bulk_spmv_f32(const clspmv_dia_f32* dev, const float* x, float* y,
+                             float alpha, float beta, clspmv_stream_t stream);
+int clspmv_bdia_bulk_spmv_f32(const clspmv_bdia_f32* dev, const float* x, float* y,
+                              float alpha, float beta, clspmv_stream_t stream);
+/* Reads and resets the number of bounded waits of the bulk-copy pipelines
+ * that ran out since the last call (0 in normal operation). */
+int clspmv_pipeline_timeouts(unsigned int* count);
+
 /* BDIA with a shared-memory x window per band. Replaces gpu_bdia* variants
  * (kernels/spmv_bdia.cl:4-283), driver src/spmv_bdia.cpp:413-441. */
 int clspmv_bdia_spmv_f32(const clspmv_bdia_f32* dev, const float* x, float* y,
@@ -411,18 +430,17 @@ int clspmv_sell_spmv_f32(const clspmv_sell_f32* dev, const float* x, float* y,
  * (include/matrix_storage.h:1466-1491), so a slot equal to its predecessor's
  * column with value 0 adds nothing and a row's trailing run of such slots is
  * padding. clspmv_sell_plan_create finds where every row's real entries end
- * and lists the long rows' tails (synchronous, once per matrix; it allocates
- * device memory, released with clspmv_sell_plan_free). The planned SpMV sums
- * each row's first 32 entries with a thread per row and the tails of longer
- * rows with a warp per 256 entries, so a slice as wide as one power-law row
- * costs that row's entries, not slice_height times them. Any slice height.
- * Measured on B200 it is slower than clspmv_sell_spmv_f32 for power-law
- * slices (a long row's tail is a strided, column-major read: one 32-byte
- * sector per 4-byte entry in each array), so the padded read stays the
- * default everywhere in this library.
- * Same y as clspmv_sell_spmv_f32 up to summation order, except where x
- * holds Inf or NaN at a skipped padding column. No counterpart in the
- * reference. */
+ * (synchronous, once per matrix; it allocates device memory, released with
+ * clspmv_sell_plan_free). For slice heights 4..128 (powers of two) with
+ * 16-byte aligned arrays the planned SpMV walks the slot space like
+ * clspmv_sell_spmv_f32 (equal runs of slice columns per warp, 4 rows per
+ * lane) but each lane loads a column only while one of its 4 rows still has
+ * real entries, so the tail columns of a slice padded to one long row fetch
+ * that row's 32-byte sectors only; other slice heights sum each row's first
+ * 32 entries with a thread per row and longer rows' tails with a warp per
+ * 256 entries. Same y as clspmv_sell_spmv_f32 up to summation order, except
+ * where x holds Inf or NaN at a skipped padding column. No counterpart in
+ * the reference. */
 typedef struct clspmv_sell_plan clspmv_sell_plan;
 int clspmv_sell_plan_create(const clspmv_sell_f32* dev, clspmv_sell_plan** out);
 int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* dev, const clspmv_sell_plan* plan, const float* x, float* y,
@@ -430,6 +448,9 @@ int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* dev, const clspmv_sell_plan
 /* stored entries the plan reads (real entries and explicit zeros before them), and its tail items */
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* plan);
 long long clspmv_sell_plan_items(const clspmv_sell_plan* plan);
+/* bytes of col and data in the 32-byte sectors that hold real entries: what
+ * the planned SpMV must move from the matrix arrays */
+long long clspmv_sell_plan_sector_bytes(const clspmv_sell_plan* plan);
 int clspmv_sell_plan_free(clspmv_sell_plan* plan);
 
 /* BELL = b4ell, block shapes {1,2,4,8} x {4,8}. Replaces the 32 kernels of
@@ -592,12 +613,39 @@ typedef struct clspmv_cocktail_handle clspmv_cocktail_handle;
  * src/spmv_cocktail.cpp:304-1009, 1590-1611). Synchronous. */
 int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_handle** out);
 /* y <- alpha*A*x + beta*y over all parts (replaces do_spmv,
- * src/spmv_cocktail.cpp:1088-1132). Parts run concurrently on internal
- * streams forked from and joined into `stream`; safe to capture in a CUDA
- * graph. The parts' additions to y are atomic, so the summation order (and
- * the last bits of y) may differ from run to run within the 1e-5 bound. */
+ * src/spmv_cocktail.cpp:1088-1132, which runs one kernel per part in
+ * sequence). Two schedules (clspmv_cocktail_set_schedule):
+ *  - PER_PART (the default, AUTO): one launch per part on internal streams
+ *    forked from and joined into `stream`;
+ *  - FUSED: ONE persistent launch. Every part is cut into tiles, the tiles of
+ *    all parts are interleaved into one work list in proportion to each
+ *    part's estimated time, and the CTAs take list entries from a device
+ *    counter, so all parts run side by side on every SM (a small kernel
+ *    before it applies beta and resets the counter). Measured on B200 it
+ *    ties the per-part launches on the Cocktail benchmark matrix (4M rows,
+ *    SBELL 4x4 + COO parts: 0.165 against 0.166 ms): the HBM-streaming and
+ *    the x-gathering part share the L2, so overlapping them gains nothing
+ *    there, and AUTO keeps the per-part launches. An x that is not 16-byte
+ *    aligned takes the per-part launches.
+ * Either way it is stream ordered and safe to capture in a CUDA graph; calls
+ * on one handle must not overlap on the GPU (the work counter and the
+ * streams belong to the handle). The parts' additions to y are atomic, so
+ * the summation order (and the last bits of y) may differ from run to run
+ * within the 1e-5 bound. */
 int clspmv_cocktail_spmv_f32(clspmv_cocktail_handle* h, const float* x, float* y, float alpha, float beta,
                              clspmv_stream_t stream);
+/* Schedule of a handle's SpMV: AUTO (the per-part launches), FUSED (one
+ * persistent launch; refused with CLSPMV_ERR_UNSUPPORTED when the handle has
+ * fewer than two parts or a part layout the fused kernel does not cover:
+ * block shapes taller than 4, or 8 wide and taller than 2) or PER_PART. No
+ * counterpart in the reference. */
+#define CLSPMV_SCHEDULE_AUTO 0
+#define CLSPMV_SCHEDULE_FUSED 1
+#define CLSPMV_SCHEDULE_PER_PART 2
+int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule);
+/* Work-list entries of the fused schedule, 0 when the handle has none (one
+ * part, or a part the fused kernel does not cover). */
+int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h);
 /* The reference's A^k x loop (src/eval.cpp:19-72) kept on the device:
  * `iterations` times y <- alpha*A*x + beta*y, then the first mat_height
  * entries of x <- y (cpy_vector_from_gpu, src/spmv_cocktail.cpp:1510-1556).

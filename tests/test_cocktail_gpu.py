@@ -43,10 +43,16 @@ def setup(tmp_path_factory):
 
 @pytest.mark.parametrize("cfg,mname,mode", CASES)
 @pytest.mark.parametrize("alpha,beta", [(1.0, 1.0), (2.0, -0.5), (1.0, 0.0)])
-def test_cocktail_spmv(setup, cfg, mname, mode, alpha, beta):
+@pytest.mark.parametrize("schedule", ["auto", "fused"])
+def test_cocktail_spmv(setup, cfg, mname, mode, alpha, beta, schedule):
+    """Both schedules: one launch per part (auto) and the fused persistent
+    launch over all parts (partitions of two or more parts)."""
     import torch
     coo, ck = setup[(cfg, mname)]
     dev = ck.to_device()
+    if schedule == "fused" and len(dev.parts) < 2:
+        pytest.skip("one part: nothing to fuse")
+    dev.set_schedule(schedule)
     x = synth.x_vector(coo.shape[1])
     y0 = np.random.default_rng(3).standard_normal(coo.shape[0]).astype(np.float32)
     xd = torch.from_numpy(x).cuda()
@@ -55,6 +61,149 @@ def test_cocktail_spmv(setup, cfg, mname, mode, alpha, beta):
     torch.cuda.synchronize()
     y_ref, _, bound = reference_y(coo, x, y0, alpha, beta)
     assert_close(yd.cpu().numpy(), y_ref, bound, f"cocktail {cfg}/{mname} parts={dev.parts}")
+
+
+def test_cocktail_fused_covers_multi_part_cases(setup):
+    """Every multi-part partition of the test configurations gets a fused
+    work list (their block shapes are among those the fused kernel covers),
+    and "fused" can be required; a single part keeps its own launch."""
+    seen = 0
+    for (cfg, mname), (coo, ck) in setup.items():
+        dev = ck.to_device()
+        if len(dev.parts) >= 2:
+            assert dev.fused_items >= len(dev.parts), (cfg, mname, dev.parts)
+            dev.set_schedule("fused")
+            seen += 1
+        else:
+            assert dev.fused_items == 0
+    assert seen >= 3
+
+
+def test_cocktail_fused_graph_replay_and_repeat(setup):
+    """The fused schedule replayed from a captured graph and called back to
+    back (the work counter is reset by the launch before it each time): y =
+    y0 + k A x."""
+    import torch
+    coo, ck = setup[("block_partial", "mixed")]
+    dev = ck.to_device()
+    assert dev.fused_items > 0, dev.parts
+    dev.set_schedule("fused")
+    x = synth.x_vector(coo.shape[1])
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros(coo.shape[0], dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        dev.spmv(xd, yd, 1.0, 1.0, stream=s)
+    torch.cuda.synchronize()
+    yd.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        dev.spmv(xd, yd, 1.0, 1.0, stream=s)
+    yd.zero_()
+    for _ in range(3):
+        g.replay()
+    for _ in range(2):
+        dev.spmv(xd, yd, 1.0, 1.0)
+    torch.cuda.synchronize()
+    y_ref, _, bound = reference_y(coo, x)
+    assert_close(yd.cpu().numpy() / 5, y_ref, bound, "fused replay")
+
+
+def hand_partition(layout, seed=3, scatter=30000):
+    """A matrix of n rows (tridiagonal band + 4x4 blocks + scattered
+    entries) split by hand into the Cocktail slots of `layout`
+    ({slot: converter}), every entry in exactly one slot: the band to the
+    first slot, the blocks to the second, the scattered entries dealt out by
+    row to the rest. Returns (COO of the whole matrix, CocktailMatrix)."""
+    from clspmv_mic_b200 import _abi
+    rng = np.random.default_rng(seed)
+    n = 4096
+    r = np.arange(n)
+    band = [(r, r, np.full(n, 2.0))] + [(r[1:], r[1:] - 1, -np.ones(n - 1)), (r[:-1], r[:-1] + 1, -np.ones(n - 1))]
+    br = rng.choice(n // 4, 600, replace=False)
+    bc = rng.integers(0, n // 4, 600)
+    bi, bj = np.meshgrid(np.arange(4), np.arange(4), indexing="ij")
+    blk_r = (br[:, None] * 4 + bi.ravel()[None, :]).ravel()
+    blk_c = (bc[:, None] * 4 + bj.ravel()[None, :]).ravel()
+    sr = rng.integers(0, n, scatter)
+    sc = rng.integers(0, n, scatter)
+    groups = {"band": (np.concatenate([b[0] for b in band]), np.concatenate([b[1] for b in band])),
+              "blocks": (blk_r, blk_c), "scatter": (sr, sc)}
+    # distinct (row, col): an entry keeps the first group that claims it
+    taken = set()
+    split = {}
+    for g, (gr, gc) in groups.items():
+        keys = gr.astype(np.int64) * n + gc
+        keys = np.unique(keys)
+        keys = np.array([k for k in keys if k not in taken], dtype=np.int64)
+        taken.update(keys.tolist())
+        split[g] = keys
+    slots = list(layout)
+    pieces = {slots[0]: split["band"], slots[1]: split["blocks"]}
+    rest = slots[2:]
+    srow = split["scatter"] // n
+    for i, sl in enumerate(rest):
+        pieces[sl] = split["scatter"][srow % len(rest) == i]
+    st = _abi.Cocktail()
+    st.mat_width = st.mat_height = n
+    keep = []
+    allk = []
+    for sl, keys in pieces.items():
+        keys = np.sort(keys)
+        allk.append(keys)
+        vals = rng.standard_normal(keys.size).astype(np.float32)
+        part_coo = F.coo_matrix(n, n, keys // n, keys % n, vals)
+        host = layout[sl](part_coo)
+        keep.append((part_coo, host))
+        setattr(st, f"ifuse{sl}", True)
+        setattr(st, sl, type(getattr(st, sl)).from_buffer_copy(host.struct))
+    st.mat_nnz = int(sum(k.size for k in allk))
+    ck = CK.CocktailMatrix(st, owner=None)
+    ck._keep = keep
+    # the whole matrix: every slot's entries, with the values each slot holds
+    rows = np.concatenate([pc.array("coo_row_id") for pc, _ in keep])
+    cols = np.concatenate([pc.array("coo_col_id") for pc, _ in keep])
+    vals = np.concatenate([pc.array("coo_data") for pc, _ in keep])
+    o = np.lexsort((cols, rows))
+    return F.coo_matrix(n, n, rows[o], cols[o], vals[o]), ck
+
+
+HAND_LAYOUTS = {
+    "dia_sbell_ell_sell_csr_coo": {"dia": F.coo2dia, "sbell": lambda c: F.coo2sbell(c, 4, 4, 32),
+                                   "ell": lambda c: F.coo2ell(c), "sell": lambda c: F.coo2sell(c, 32),
+                                   "csr": F.coo2csr, "coo": lambda c: c},
+    "bdia_bell_bcsr_sell8_coo": {"bdia": F.coo2bdia, "bell": lambda c: F.coo2b4ell(c, 4, 2),
+                                 "bcsr": lambda c: F.coo2b4csr(c, 8, 1), "sell": lambda c: F.coo2sell(c, 8),
+                                 "coo": lambda c: c},
+    "dia_bcsr_sell20": {"dia": F.coo2dia, "bcsr": lambda c: F.coo2b4csr(c, 4, 4), "sell": lambda c: F.coo2sell(c, 20)},
+    # dense scattered part: SELL by slice columns; slice height 7: SELL row by row
+    "dia_bcsr_sell32_dense": {"dia": F.coo2dia, "bcsr": lambda c: F.coo2b4csr(c, 4, 4), "sell": lambda c: F.coo2sell(c, 32)},
+    "bdia_sbell82_sell7": {"bdia": F.coo2bdia, "sbell": lambda c: F.coo2sbell(c, 8, 2, 32), "sell": lambda c: F.coo2sell(c, 7)},
+}
+HAND_SCATTER = {"dia_bcsr_sell32_dense": 90000}
+
+
+@pytest.mark.parametrize("layout", sorted(HAND_LAYOUTS))
+@pytest.mark.parametrize("schedule", ["fused", "per_part"])
+def test_cocktail_hand_partitions(layout, schedule):
+    """Hand-made partitions using all nine slots between them (several flat
+    parts at once, every fused kernel kind: DIA, BDIA, SBELL, BELL, BCSR with
+    8-wide blocks, SELL by columns and by rows, ELL, CSR, COO): the fused
+    launch and the per-part launches against the oracle."""
+    import torch
+    coo, ck = hand_partition(HAND_LAYOUTS[layout], scatter=HAND_SCATTER.get(layout, 30000))
+    dev = ck.to_device()
+    assert dev.fused_items >= len(dev.parts)
+    dev.set_schedule(schedule)
+    x = synth.x_vector(coo.shape[1])
+    y0 = np.random.default_rng(2).standard_normal(coo.shape[0]).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (1.5, -0.5)]:
+        xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+        dev.spmv(xd, yd, alpha, beta)
+        torch.cuda.synchronize()
+        y_ref, _, bound = reference_y(coo, x, y0, alpha, beta)
+        assert_close(yd.cpu().numpy(), y_ref, bound, f"{layout} {schedule} parts={dev.parts}")
 
 
 def test_cocktail_graph_replay(setup):
