@@ -559,6 +559,8 @@ def run_ours(args):
 
     variants = [it for it in items if it["key"] in VARIANT_KEYS]
     items = [it for it in items if it["key"] not in VARIANT_KEYS]
+    if not items:   # --only named variants alone: they form the step
+        items, variants = variants, []
     K = len(items)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(K + 1)] for _ in range(args.steps)]
 

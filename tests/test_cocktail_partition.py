@@ -243,3 +243,20 @@ def test_random_matrices_and_tables_identical(tmp_path):
         d = dirs[it % len(dirs)]
         diffs = compare_cocktails(CK.analyze(coo, d, *mode), ref_analyze(coo, d, *mode))
         assert not diffs, f"case {it} mode={mode}: {diffs[:5]}"
+
+
+@pytest.mark.slow
+def test_partition_at_c3_size_matches_reference(tmp_path):
+    """The Cocktail benchmark matrix at full size (4M rows, 66.2M nonzeros:
+    7-diagonal band, 4x4 blocks, power-law rows) partitioned by both
+    analyzers with the same tables and knobs into BDIA + BCSR + COO: the
+    cocktail<> results are byte-identical. (The reference takes about a
+    minute here.)"""
+    ref_or_skip()
+    cfg = dict(_table_configs())["block_partial"]
+    tables.model_tables(tmp_path, **cfg)
+    coo = F.coo_matrix(*synth.cocktail_mixed())
+    mine = CK.analyze(coo, tmp_path, 1.0, False, False)
+    assert {p for p in ("bdia", "bcsr", "coo") if mine.uses(p)} == {"bdia", "bcsr", "coo"}, mine.summary()
+    theirs = ref_analyze(coo, tmp_path, 1.0, False, False)
+    assert compare_cocktails(mine, theirs) == []
