@@ -740,6 +740,11 @@ def run_ours(args):
         parity, detail["parity"] = check_parity(items + variants, xs, oracles, stream)
         del csrs, oracles
 
+    if not args.no_extras and not args.only:
+        # every rank takes part (one all-gather per step)
+        detail["sharded_akx"] = run_sharded_akx(world, dev)
+        if rank == 0:
+            print(json.dumps({"detail": "sharded_akx", **detail["sharded_akx"]}), flush=True)
     if not args.no_extras and not args.only and world == 1:
         for name, fn in (("extras", lambda: run_extras(args, items, mats, peak)),
                          ("cocktail_c3", lambda: run_cocktail_c3(args, peak)),
@@ -789,6 +794,43 @@ def check_parity(items, xs, oracles, stream):
     summary["max_err_fp64"] = float(f"{summary['max_err_fp64']:.3g}")
     summary["ref_err_fp64"] = float(f"{summary['ref_err_fp64']:.3g}")
     return summary, per
+
+
+def run_sharded_akx(world: int, dev, n: int = 128, steps: int = 40):
+    """The reference's A^k x loop (src/eval.cpp:19-72) on the 27-point
+    stencil 128^3 with its rows split evenly over the ranks: each rank builds
+    its own rows only, and a step is the rank's SpMV (CSR by nonzero chunks)
+    plus one all-gather of every rank's y block into x (NCCL over NVLink /
+    NVSwitch; a device copy at one rank). Time per step: CUDA events around
+    `steps` steps, the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    from clspmv_mic_b200 import sharded as S
+    from clspmv_mic_b200 import synth
+    m = n ** 3
+    s = S.ShardedCsr(None, device=dev, n=m, make_rows=lambda r0, r1: synth.stencil_27pt_rows(n, r0, r1))
+    rng = np.random.default_rng(5)
+    s.load(rng.uniform(-1, 1, m).astype(np.float32), np.zeros(m, np.float32))
+    alpha = 1.0 / 32.0   # |row sums| <= 27: x stays bounded over the steps
+    nnz = torch.tensor([s.nnz], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(nnz)
+    s.iterate(3, alpha, 0.0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    s.iterate(steps, alpha, 0.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, dev)
+    total = float(nnz.item())
+    finite = bool(torch.isfinite(s.x).all().item())
+    return {"matrix": f"stencil27 {n}^3", "rows": m, "nnz": int(total), "world": world, "steps": steps,
+            "ms_per_step": round(ms, 4), "gflops": round(2 * total / (ms * 1e-3) / 1e9, 1),
+            "gather_bytes_per_step": 4 * s.block * world, "x_finite": finite,
+            "note": "rows split evenly, each rank's slab built from its own rows; one all_gather_into_tensor per step"}
 
 
 def run_device_convert(items):

@@ -113,6 +113,22 @@ __device__ __forceinline__ float4 ld_x4(const float* p, uint64_t pol)
     return v;
 }
 
+// x gathers at scattered columns (COO, CSR by chunks): GX = 0 allocates the
+// line in L1 like ld_x; GX = 1 does not (with uniformly scattered columns
+// almost no gather hits L1, and the line fill costs L1 bandwidth).
+__device__ __forceinline__ float ld_x_na(const float* p, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+template <int GX>
+__device__ __forceinline__ float ld_gx(const float* p, uint64_t pol)
+{
+    if constexpr (GX == 1) return ld_x_na(p, pol);
+    else return ld_x(p, pol);
+}
+
 // Matrix values stored as FP32, BF16 or FP16, read as float: ldv4 loads 4
 // consecutive values (16 bytes, or 8 for 16-bit storage; 4-value aligned),
 // ldv one. Streamed like the other matrix arrays.

@@ -9,6 +9,7 @@
 // Cocktail evaluate() (src/spmv_cocktail.cpp:1431-1455).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include "clspmv_b200.h"
@@ -30,7 +31,9 @@ __global__ void k_copy4(const float4* __restrict__ a, float4* __restrict__ b, si
 __global__ void k_nothing() {}
 
 // Random gathers x[idx[i]] with the SpMV kernels' load forms: indices
-// streamed with 128-bit loads, x read through L1 with an L2 keep policy.
+// streamed with 128-bit loads, x read with an L2 keep policy, through L1
+// with allocation (GX = 0) or without (GX = 1), as ld_gx.
+template <int GX>
 __global__ void __launch_bounds__(kBlock) k_gather(const int* __restrict__ idx, const float* __restrict__ x,
                                                    float* __restrict__ out, long long n4)
 {
@@ -38,7 +41,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(const int* __restrict__ idx, 
     float acc = 0.0f;
     for (long long i = blockIdx.x * (long long)kBlock + threadIdx.x; i < n4; i += (long long)gridDim.x * kBlock) {
         const int4 c = ld_stream_i4(idx + 4 * i, pol_s);
-        acc += ld_x(x + c.x, pol_x) + ld_x(x + c.y, pol_x) + ld_x(x + c.z, pol_x) + ld_x(x + c.w, pol_x);
+        acc += ld_gx<GX>(x + c.x, pol_x) + ld_gx<GX>(x + c.y, pol_x) + ld_gx<GX>(x + c.z, pol_x) + ld_gx<GX>(x + c.w, pol_x);
     }
     out[blockIdx.x * (long long)kBlock + threadIdx.x] = acc;
 }
@@ -459,15 +462,16 @@ int clspmv_gather_test(int x_len, long long count, int ntimes, int verbose, doub
         k_fill_random<<<grid, kBlock, 0, st>>>(idx, 4 * n4, x_len, 12345u);
         rc = after_launch(1);
     }
-    for (int i = 0; !rc && i < 3; i++) {
-        k_gather<<<grid, kBlock, 0, st>>>(idx, x, out, n4);
-        rc = after_launch(1);
-    }
+    // the load form the SpMV kernels use (CLSPMV_GATHER_FORM as in spmv_api.cu)
+    const char* gf = getenv("CLSPMV_GATHER_FORM");
+    auto gather = [&]() {
+        if (gf && atoi(gf) == 1) k_gather<1><<<grid, kBlock, 0, st>>>(idx, x, out, n4);
+        else k_gather<0><<<grid, kBlock, 0, st>>>(idx, x, out, n4);
+        return after_launch(1);
+    };
+    for (int i = 0; !rc && i < 3; i++) rc = gather();
     if (!rc) rc = cuda_status(cudaEventRecord(e0, st));
-    for (int i = 0; !rc && i < ntimes; i++) {
-        k_gather<<<grid, kBlock, 0, st>>>(idx, x, out, n4);
-        rc = after_launch(1);
-    }
+    for (int i = 0; !rc && i < ntimes; i++) rc = gather();
     if (!rc) rc = cuda_status(cudaEventRecord(e1, st));
     if (!rc) rc = cuda_status(cudaEventSynchronize(e1));
     float ms = 0.0f;

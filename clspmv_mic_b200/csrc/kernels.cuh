@@ -264,7 +264,7 @@ __device__ __forceinline__ void bdia_cta(const BdiaArgsT<V>& a, int cta, int nct
 // ---------------------------------------------------------------------------
 constexpr int kEllRowsPerPass = kBlock * 4;
 
-template <bool ATOMIC, class V>
+template <bool ATOMIC, class V, int GX = 0>
 __device__ __forceinline__ void ell_cta(const EllArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
@@ -278,10 +278,10 @@ __device__ __forceinline__ void ell_cta(const EllArgsT<V>& a, int cta, int ncta,
         for (int k = 0; k < a.ell_num; k++) {
             const int4 c = ld_stream_i4(cp + (size_t)k * a.len, pe);
             const float4 v = ldv4(dp + (size_t)k * a.len, pe);
-            acc[0] = fmaf(v.x, ld_x(a.x + c.x, pl), acc[0]);
-            acc[1] = fmaf(v.y, ld_x(a.x + c.y, pl), acc[1]);
-            acc[2] = fmaf(v.z, ld_x(a.x + c.z, pl), acc[2]);
-            acc[3] = fmaf(v.w, ld_x(a.x + c.w, pl), acc[3]);
+            acc[0] = fmaf(v.x, ld_gx<GX>(a.x + c.x, pl), acc[0]);
+            acc[1] = fmaf(v.y, ld_gx<GX>(a.x + c.y, pl), acc[1]);
+            acc[2] = fmaf(v.z, ld_gx<GX>(a.x + c.z, pl), acc[2]);
+            acc[3] = fmaf(v.w, ld_gx<GX>(a.x + c.w, pl), acc[3]);
         }
         y_put4<ATOMIC>(acc, row0, e, a.y, a.alpha, a.beta, scl(a));
     }
@@ -478,13 +478,21 @@ __device__ __forceinline__ void sell_tail_cta(const SellArgs& a, const int* __re
 // array), while the warp still walks the slot space in equal runs of columns.
 // Requires slice_height = 4 Q, 16-byte aligned arrays and beta already
 // applied.
+//
+// With `head` (a prefix table of per-slice head widths, nslice + 1 entries),
+// only the first head[s+1] - head[s] columns of slice s are walked: the
+// columns up to its second-longest row, the rest of its longest row being
+// left to sell_tail_cta.
 template <int Q, bool ATOMIC_ALL>
-__device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __restrict__ rlen, int cta, int ncta)
+__device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __restrict__ rlen, int cta, int ncta,
+                                                const int* __restrict__ head = nullptr)
 {
     constexpr int G = 32 / Q;             // columns per warp step
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     const int sh = Q * 4;
-    const long long total_cols = (long long)a.slice_ptr[a.nslice] / sh;
+    const int* __restrict__ cptr = head ? head : a.slice_ptr;   // column-space prefix (slots / sh without head)
+    const long long cdiv = head ? 1 : sh;
+    const long long total_cols = (long long)cptr[a.nslice] / cdiv;
     const int lane = threadIdx.x & 31;
     const int g = lane / Q, q = lane % Q;
     const long long nwarps_total = (long long)ncta * (kBlock / 32);
@@ -494,18 +502,20 @@ __device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __
         int lo = 0, hi = a.nslice - 1;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if ((long long)a.slice_ptr[mid + 1] <= c0 * sh) lo = mid + 1;
+            if ((long long)cptr[mid + 1] <= c0 * cdiv) lo = mid + 1;
             else hi = mid;
         }
         int s = lo;
         long long c = c0;
         while (c < c1) {
-            const long long sb = a.slice_ptr[s] / sh, se = a.slice_ptr[s + 1] / sh;
+            const long long sb = cptr[s] / cdiv, se = cptr[s + 1] / cdiv;
             if (se <= c) {
                 s++;
                 continue;
             }
             const long long ce = min(c1, se);
+            // slot of column cc of this slice: (cc - sb) * sh + slice start
+            const long long sbase = (long long)a.slice_ptr[s] - sb * sh;
             const long long row0 = (long long)s * sh + 4 * q;
             int live = 0;                 // columns sb .. sb + live - 1 hold real entries of this lane's rows
             if (row0 + 3 < a.rows) {
@@ -520,7 +530,7 @@ __device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __
 #pragma unroll 4
             for (long long cc = c + g; cc < ce; cc += G) {
                 if (cc < klim) {
-                    const size_t base = (size_t)cc * sh + 4 * q;
+                    const size_t base = (size_t)(sbase + cc * sh) + 4 * q;
                     const int4 cv = ld_stream_i4(a.col + base, pe);
                     const float4 v = ld_stream_f4(a.data + base, pe);
                     acc[0] = fmaf(v.x, ld_x(a.x + cv.x, pl), acc[0]);
@@ -778,7 +788,7 @@ __device__ __forceinline__ void coo_red(const ArgsT<V>& a, int row, float v)
 template <template <class> class ArgsT, class V>
 __device__ __forceinline__ void warp_segments(const ArgsT<V>& a, const int (&r)[kCooSteps][4], const float (&p)[kCooSteps][4]);
 
-template <class V>
+template <class V, int GX = 0>
 __device__ __forceinline__ void coo_warp_chunk(const CooArgsT<V>& a, long long base, uint64_t pe, uint64_t pl)
 {
     const int lane = threadIdx.x & 31;
@@ -810,7 +820,7 @@ __device__ __forceinline__ void coo_warp_chunk(const CooArgsT<V>& a, long long b
         for (int s = 0; s < kCooSteps; s++)
 #pragma unroll
             for (int j = 0; j < 4; j++)
-                if (r[s][j] != kCooNoRow) p[s][j] *= ld_x(a.x + c[s][j], pl);
+                if (r[s][j] != kCooNoRow) p[s][j] *= ld_gx<GX>(a.x + c[s][j], pl);
     }
     warp_segments(a, r, p);
 }
@@ -891,14 +901,14 @@ __device__ __forceinline__ void warp_segments(const ArgsT<V>& a, const int (&r)[
     if (carry_row >= 0 && lane == 0) coo_red(a, carry_row, carry);
 }
 
-template <class V>
+template <class V, int GX = 0>
 __device__ __forceinline__ void coo_cta(const CooArgsT<V>& a, int cta, int ncta, char*)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     const long long nchunks = ((long long)a.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
     long long b, e;
     cta_share(nchunks, 1, cta, ncta, b, e);
-    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) coo_warp_chunk(a, ch * kCooWarpNnz, pe, pl);
+    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) coo_warp_chunk<V, GX>(a, ch * kCooWarpNnz, pe, pl);
 }
 
 // ---------------------------------------------------------------------------
@@ -913,7 +923,7 @@ __device__ __forceinline__ void coo_cta(const CooArgsT<V>& a, int cta, int ncta,
 // Matrix bytes are CSR's 8 nnz + 4 (m + 1) instead of COO's 12 nnz.
 // beta must already be applied; col_id and data 16-byte aligned.
 // ---------------------------------------------------------------------------
-template <class V>
+template <class V, int GX = 0>
 __device__ __forceinline__ void csr_chunk_warp(const CsrArgsT<V>& a, const int* __restrict__ chunk_row, long long ch,
                                                uint64_t pe, uint64_t pl)
 {
@@ -944,7 +954,7 @@ __device__ __forceinline__ void csr_chunk_warp(const CsrArgsT<V>& a, const int* 
         for (int s = 0; s < kCooSteps; s++)
 #pragma unroll
             for (int j = 0; j < 4; j++)
-                if (base + s * 128 + lane * 4 + j < a.nnz) p[s][j] *= ld_x(a.x + c[s][j], pl);
+                if (base + s * 128 + lane * 4 + j < a.nnz) p[s][j] *= ld_gx<GX>(a.x + c[s][j], pl);
     }
     const int ra = __ldg(chunk_row + ch), rb = __ldg(chunk_row + ch + 1);
 #pragma unroll
@@ -978,14 +988,14 @@ __device__ __forceinline__ void csr_chunk_warp(const CsrArgsT<V>& a, const int* 
     warp_segments(a, r, p);
 }
 
-template <class V>
+template <class V, int GX = 0>
 __device__ __forceinline__ void csr_chunk_cta(const CsrArgsT<V>& a, const int* __restrict__ chunk_row, int cta, int ncta)
 {
     const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
     const long long nchunks = ((long long)a.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
     long long b, e;
     cta_share(nchunks, 1, cta, ncta, b, e);
-    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) csr_chunk_warp(a, chunk_row, ch, pe, pl);
+    for (long long ch = b + (threadIdx.x >> 5); ch < e; ch += kBlock / 32) csr_chunk_warp<V, GX>(a, chunk_row, ch, pe, pl);
 }
 
 // chunk_row[c] = row of nonzero c * kCooWarpNnz (the largest row whose start

@@ -91,8 +91,8 @@ int dia_form(int dflt)
     return forced >= 0 ? forced : dflt;
 }
 
-template <bool A, class V>
-__global__ void __launch_bounds__(kBlock) k_ell(EllArgsT<V> a) { ell_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
+template <bool A, class V, int GX = 0>
+__global__ void __launch_bounds__(kBlock) k_ell(EllArgsT<V> a) { ell_cta<A, V, GX>(a, blockIdx.x, gridDim.x, nullptr); }
 
 template <int Q, bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_sell(SellArgsT<V> a) { sell_cta<Q, A>(a, blockIdx.x, gridDim.x, nullptr); }
@@ -111,9 +111,9 @@ __global__ void __launch_bounds__(kBlock) k_sell_rlen(const int* __restrict__ sl
 }
 
 template <int Q, bool A>
-__global__ void __launch_bounds__(kBlock) k_sell_masked(SellArgs a, const int* __restrict__ rlen)
+__global__ void __launch_bounds__(kBlock) k_sell_masked(SellArgs a, const int* __restrict__ rlen, const int* __restrict__ head)
 {
-    sell_masked_cta<Q, A>(a, rlen, blockIdx.x, gridDim.x);
+    sell_masked_cta<Q, A>(a, rlen, blockIdx.x, gridDim.x, head);
 }
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_sell_head(SellArgs a, const int* __restrict__ rlen)
@@ -147,13 +147,25 @@ __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, co
     csr_merge_search(rows, nnz, row_ptr, (long long)t * kMergeTile, tc + 2 * t);
 }
 
-template <class V>
-__global__ void __launch_bounds__(kBlock) k_coo(CooArgsT<V> a) { coo_cta(a, blockIdx.x, gridDim.x, nullptr); }
+template <class V, int GX = 0>
+__global__ void __launch_bounds__(kBlock) k_coo(CooArgsT<V> a) { coo_cta<V, GX>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <class V>
+template <class V, int GX = 0>
 __global__ void __launch_bounds__(kBlock) k_csr_chunk(CsrArgsT<V> a, const int* __restrict__ chunk_row)
 {
-    csr_chunk_cta(a, chunk_row, blockIdx.x, gridDim.x);
+    csr_chunk_cta<V, GX>(a, chunk_row, blockIdx.x, gridDim.x);
+}
+
+// Form of the scattered x gathers of COO and CSR by chunks (ld_gx): 0 through
+// L1 with allocation, 1 without. CLSPMV_GATHER_FORM overrides (measurements).
+constexpr int kGatherDefaultForm = 0;
+int gather_form()
+{
+    static int f = [] {
+        const char* e = getenv("CLSPMV_GATHER_FORM");
+        return e ? atoi(e) : kGatherDefaultForm;
+    }();
+    return f;
 }
 
 __global__ void __launch_bounds__(kBlock) k_csr_chunk_plan(const int* __restrict__ row_ptr, int rows, long long nchunks,
@@ -352,8 +364,14 @@ int launch_ell_v(const clspmv_ell_f32* m, const V* data, const float* scale, con
     if ((m->ell_height_aligned & 3) || !aligned16(m->ell_col_id) || !aligned_v4(data) || rows > m->ell_height_aligned)
         return CLSPMV_ERR_ALIGN;
     EllArgsT<V> a{rows, m->ell_num, m->ell_height_aligned, m->ell_col_id, data, x, y, alpha, beta, scale};
-    if (atomic) k_ell<true, V><<<persistent_grid(k_ell<true, V>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
-    else k_ell<false, V><<<persistent_grid(k_ell<false, V>, rows, kEllRowsPerPass), kBlock, 0, st>>>(a);
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kEllRowsPerPass), kBlock, 0, st>>>(a); };
+    if (gather_form() == 1) {
+        if (atomic) go(k_ell<true, V, 1>);
+        else go(k_ell<false, V, 1>);
+    } else {
+        if (atomic) go(k_ell<true, V, 0>);
+        else go(k_ell<false, V, 0>);
+    }
     return after_launch(1);
 }
 
@@ -404,9 +422,16 @@ int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha,
     return launch_sell_v<float>(m, m ? m->sell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
 }
 
-// Padding-free SELL: heads (plain y update, or atomic), then the long rows' tails (atomic).
-int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* items, long long nitems, const float* x,
-                        float* y, float alpha, float beta, cudaStream_t st, bool atomic)
+// Padding-free SELL. Power-of-two slice heights with 16-byte aligned arrays:
+// the column-balanced walk with each lane's loads cut at its rows' real
+// length, either over every column of every slice (head == nullptr), or over
+// each slice's columns up to its second-longest row (head: prefix table of
+// those widths) followed by the longest rows' tails, a warp per item of up to
+// kSellTailCols entries (split_items). Other slice heights: each row's first
+// kSellHead entries with a thread per row, then the tails (items).
+int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* items, long long nitems, const int* head,
+                        const int2* split_items, long long nsplit, const float* x, float* y, float alpha, float beta,
+                        cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y || !m->sell_slice_ptr || !rlen || (nitems > 0 && !items)) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
@@ -417,18 +442,20 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
     const int sh = (int)m->sell_slice_height;
     if (aligned16(m->sell_col_id) && aligned16(m->sell_data) && aligned16(rlen) &&
         (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)) {
-        // column-balanced walk with each lane's loads cut at its rows' real length
         if (!atomic) {
             int rc = prescale(y, rows, beta, st);
             if (rc) return rc;
         }
         a.beta = 1.0f;
-        return dispatch_lanes(sh / 4, [&](auto q) {
+        int rc = dispatch_lanes(sh / 4, [&](auto q) {
             constexpr int Q = decltype(q)::value;
-            if (atomic) k_sell_masked<Q, true><<<persistent_grid(k_sell_masked<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen);
-            else k_sell_masked<Q, false><<<persistent_grid(k_sell_masked<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen);
+            if (atomic) k_sell_masked<Q, true><<<persistent_grid(k_sell_masked<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen, head);
+            else k_sell_masked<Q, false><<<persistent_grid(k_sell_masked<Q, false>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen, head);
             return after_launch(1);
         });
+        if (rc || !head || nsplit == 0) return rc;
+        k_sell_tail<<<persistent_grid(k_sell_tail, nsplit, kBlock / 32), kBlock, 0, st>>>(a, rlen, split_items, nsplit);
+        return after_launch(1);
     }
     if (atomic) k_sell_head<true><<<persistent_grid(k_sell_head<true>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
     else k_sell_head<false><<<persistent_grid(k_sell_head<false>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
@@ -506,7 +533,10 @@ int launch_csr_chunk_v(const clspmv_csr_f32* m, const V* data, const float* scal
     if (!aligned16(m->csr_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
     CsrArgsT<V> a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, data, x, y, alpha, 1.0f, scale};
     const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
-    k_csr_chunk<V><<<persistent_grid(k_csr_chunk<V>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
+    if (gather_form() == 1)
+        k_csr_chunk<V, 1><<<persistent_grid(k_csr_chunk<V, 1>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
+    else
+        k_csr_chunk<V, 0><<<persistent_grid(k_csr_chunk<V, 0>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
     return after_launch(1);
 }
 
@@ -539,7 +569,9 @@ int launch_coo_v(const clspmv_coo_f32* m, const V* data, const float* scale, con
     if (!m->coo_row_id || !m->coo_col_id || !data) return CLSPMV_ERR_ARG;
     if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
     CooArgsT<V> a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, data, x, y, alpha, scale};
-    k_coo<V><<<persistent_grid(k_coo<V>, ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz, kBlock / 32), kBlock, 0, st>>>(a);
+    const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
+    if (gather_form() == 1) k_coo<V, 1><<<persistent_grid(k_coo<V, 1>, nchunks, kBlock / 32), kBlock, 0, st>>>(a);
+    else k_coo<V, 0><<<persistent_grid(k_coo<V, 0>, nchunks, kBlock / 32), kBlock, 0, st>>>(a);
     return after_launch(1);
 }
 
@@ -775,9 +807,12 @@ int clspmv_sell_spmv_f32(const clspmv_sell_f32* m, const float* x, float* y, flo
 { return launch_sell(m, x, y, alpha, beta, S(s), false); }
 struct clspmv_sell_plan {
     int* rlen = nullptr;       // device: stored length of every row (padding excluded)
-    int2* items = nullptr;     // device: (row, first entry) of each tail item
-    long long rows = 0, nitems = 0, entries = 0;
+    int2* items = nullptr;     // device: (row, first entry) of each tail item past the first kSellHead entries
+    int* head = nullptr;       // device: prefix of per-slice widths up to the second-longest row
+    int2* split_items = nullptr;   // device: (longest row, first entry) of each tail item past its slice's head
+    long long rows = 0, nitems = 0, nsplit = 0, entries = 0;
     long long sector_bytes = 0;   // col + data bytes of the 32-byte sectors holding real entries
+    bool split = true;         // walk the heads and the tails apart (power-of-two slice heights)
 };
 
 int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
@@ -802,6 +837,33 @@ int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
             p->entries += rlen[r];
             for (int k = kSellHead; k < rlen[r]; k += kSellTailCols) items.push_back(make_int2((int)r, k));
         }
+        // heads and tails: per slice the width up to its second-longest row,
+        // and the longest row's entries past it in items of kSellTailCols
+        const long long shs = (long long)m->sell_slice_height, ns = m->sell_slice_num;
+        std::vector<int> head((size_t)ns + 1, 0);
+        std::vector<int2> split;
+        for (long long sl = 0; sl < ns; sl++) {
+            int l1 = 0, l2 = 0;
+            long long arg = -1;
+            for (long long r = sl * shs; r < std::min(rows, (sl + 1) * shs); r++) {
+                const int l = rlen[(size_t)r];
+                if (l > l1) { l2 = l1; l1 = l; arg = r; }
+                else if (l > l2) l2 = l;
+            }
+            head[(size_t)sl + 1] = head[(size_t)sl] + l2;
+            for (int k = l2; arg >= 0 && k < l1; k += kSellTailCols) split.push_back(make_int2((int)arg, k));
+        }
+        p->nsplit = (long long)split.size();
+        rc = cuda_status(cudaMalloc(&p->head, sizeof(int) * head.size()));
+        if (!rc) rc = cuda_status(cudaMemcpy(p->head, head.data(), sizeof(int) * head.size(), cudaMemcpyHostToDevice));
+        if (!rc) rc = cuda_status(cudaMalloc(&p->split_items, sizeof(int2) * std::max<size_t>(1, split.size())));
+        if (!rc && !split.empty())
+            rc = cuda_status(cudaMemcpy(p->split_items, split.data(), sizeof(int2) * split.size(), cudaMemcpyHostToDevice));
+        // CLSPMV_SELL_SPLIT=0 walks every column instead (for measurements)
+        const char* e = getenv("CLSPMV_SELL_SPLIT");
+        p->split = !(e && atoi(e) == 0);
+    }
+    if (!rc) {
         // a 32-byte sector of one slice column holds 8 consecutive rows (slice
         // starts are multiples of the slice height): per group of 8 rows, the
         // longest real length counts sectors in each of col and data
@@ -828,7 +890,8 @@ int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* 
                               float beta, clspmv_stream_t s)
 {
     if (!p) return CLSPMV_ERR_ARG;
-    return launch_sell_planned(m, p->rlen, p->items, p->nitems, x, y, alpha, beta, S(s), false);
+    return launch_sell_planned(m, p->rlen, p->items, p->nitems, p->split ? p->head : nullptr, p->split_items, p->nsplit, x, y,
+                               alpha, beta, S(s), false);
 }
 
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* p) { return p ? p->entries : -1; }
@@ -840,6 +903,8 @@ int clspmv_sell_plan_free(clspmv_sell_plan* p)
     if (!p) return CLSPMV_ERR_ARG;
     if (p->rlen) cudaFree(p->rlen);
     if (p->items) cudaFree(p->items);
+    if (p->head) cudaFree(p->head);
+    if (p->split_items) cudaFree(p->split_items);
     delete p;
     return CLSPMV_OK;
 }

@@ -60,6 +60,29 @@ def slab(csr: F.HostMatrix, bounds: list, rank: int) -> F.HostMatrix:
                               csr_data=np.array(val[lo:hi], dtype=np.float32)))
 
 
+def split_rows_even(m: int, world: int) -> list:
+    """Contiguous row ranges with m / world rows each (for matrices whose
+    rows hold about the same number of nonzeros, such as stencils, where no
+    rank needs the whole row-pointer array to balance the split)."""
+    cuts = [m * q // world for q in range(world + 1)]
+    return [(cuts[q], cuts[q + 1]) for q in range(world)]
+
+
+def slab_from_rows(row_ptr, col, val, bounds: list, rank: int) -> F.HostMatrix:
+    """This rank's slab in the padded layout from its own rows only:
+    row_ptr (rebased to 0) / col (global ids) / val of rows bounds[rank]."""
+    r0, r1 = bounds[rank]
+    block = max(1, max(b1 - b0 for b0, b1 in bounds))
+    row_ptr = np.asarray(row_ptr, dtype=np.int64)
+    if row_ptr.size != r1 - r0 + 1 or row_ptr[0] != 0:
+        raise ValueError("row_ptr must hold the rank's rows, starting at 0")
+    nnz = int(row_ptr[-1])
+    return F.from_arrays("csr", dict(width=len(bounds) * block, height=r1 - r0, nnz=nnz),
+                         dict(csr_row_ptr=row_ptr.astype(np.int32),
+                              csr_col_id=padded_columns(np.asarray(col)[:nnz], bounds, block),
+                              csr_data=np.asarray(val, dtype=np.float32)[:nnz]))
+
+
 class ShardedCsr:
     """This rank's slab of a square CSR matrix and the buffers of the loop.
 
@@ -68,20 +91,35 @@ class ShardedCsr:
     replaces the device SpMV (the CPU tests pass the oracle); by default the
     slab is uploaded and run by DeviceMatrix.spmv."""
 
-    def __init__(self, csr: F.HostMatrix, group=None, device="cuda",
-                 local_spmv: Optional[Callable] = None):
+    def __init__(self, csr: Optional[F.HostMatrix], group=None, device="cuda",
+                 local_spmv: Optional[Callable] = None, *, n: Optional[int] = None,
+                 make_rows: Optional[Callable] = None):
+        """From the whole host matrix `csr` (every rank holds it; rows split
+        by nonzeros), or, with `n` and `make_rows(r0, r1) -> (row_ptr, col,
+        val)` (the rows [r0, r1) with row_ptr rebased to 0 and global column
+        ids), from this rank's rows alone (rows split evenly): no rank then
+        holds more of A than its slab."""
         import torch
         import torch.distributed as dist
-        h, w = csr.shape
-        if h != w:
-            raise ValueError("x <- y needs a square matrix")
         self.group = group
         self.world = dist.get_world_size(group) if dist.is_initialized() else 1
         self.rank = dist.get_rank(group) if dist.is_initialized() else 0
-        self.bounds = split_rows(csr.array("csr_row_ptr"), self.world)
+        if csr is not None:
+            h, w = csr.shape
+            if h != w:
+                raise ValueError("x <- y needs a square matrix")
+            self.bounds = split_rows(csr.array("csr_row_ptr"), self.world)
+        else:
+            if n is None or make_rows is None:
+                raise ValueError("give the matrix, or its size and a row generator")
+            self.bounds = split_rows_even(int(n), self.world)
         self.block = max(1, max(b1 - b0 for b0, b1 in self.bounds))
         self.rows = self.bounds[self.rank][1] - self.bounds[self.rank][0]
-        self.host = slab(csr, self.bounds, self.rank)
+        if csr is not None:
+            self.host = slab(csr, self.bounds, self.rank)
+        else:
+            r0, r1 = self.bounds[self.rank]
+            self.host = slab_from_rows(*make_rows(r0, r1), self.bounds, self.rank)
         self.nnz = self.host.nnz
         self.device = torch.device(device)
         self.x = torch.zeros(self.world * self.block, dtype=torch.float32, device=self.device)

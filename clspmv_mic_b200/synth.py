@@ -76,6 +76,29 @@ def stencil_27pt(n: int = 128, seed: int = SEED):
     return _finish(m, m, rows, cols, vals)
 
 
+def stencil_27pt_rows(n: int, r0: int, r1: int, seed: int = SEED):
+    """Rows [r0, r1) of the 27-point stencil on an n^3 grid as CSR arrays
+    (row_ptr rebased to 0, global column ids ascending in each row, values
+    uniform in [-1, 1) from a generator seeded by (seed, r0)): one rank's
+    slab, made without the rest of the matrix."""
+    r = np.arange(r0, r1, dtype=np.int64)
+    k, j, i = r // (n * n), (r // n) % n, r % n
+    d = np.array([-1, 0, 1])
+    dk, dj, di = [a.ravel() for a in np.meshgrid(d, d, d, indexing="ij")]
+    offs = dk * n * n + dj * n + di
+    order = np.argsort(offs, kind="stable")
+    dk, dj, di, offs = dk[order], dj[order], di[order], offs[order]
+    valid = np.ones((r.size, 27), dtype=bool)
+    for t in range(27):
+        valid[:, t] = ((k + dk[t]) >= 0) & ((k + dk[t]) < n) & ((j + dj[t]) >= 0) & ((j + dj[t]) < n) & \
+                      ((i + di[t]) >= 0) & ((i + di[t]) < n)
+    cols = (r[:, None] + offs[None, :])[valid]
+    row_ptr = np.zeros(r.size + 1, dtype=np.int64)
+    np.cumsum(valid.sum(axis=1), out=row_ptr[1:])
+    vals = np.random.default_rng([seed, int(r0)]).uniform(-1.0, 1.0, size=cols.size).astype(np.float32)
+    return row_ptr, cols.astype(np.int32), vals
+
+
 def zipf_lengths(m: int, s: float, mean: float, maxlen: int, rng) -> np.ndarray:
     """Row lengths: k ~ Zipf(s) truncated to [1, maxlen], scaled by
     mean / E[k] and rounded, clipped to [1, maxlen]."""

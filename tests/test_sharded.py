@@ -140,3 +140,64 @@ def test_device_world_of_one_matches_device_loop():
     # both run the chunked CSR kernel, whose cut rows add atomically: equal
     # within summation-order noise
     assert np.abs(got - want).max() <= 1e-5 * (np.abs(want).max() + 1e-30)
+
+
+def _rows_worker(rank, world, port, q, n, k):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from clspmv_mic_b200 import synth
+    from oracle import oracle as O
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        holder = {}
+
+        def local(x, y, a, b):
+            ax = O.spmv_port(holder["s"].host, x.numpy())
+            y.copy_(torch.from_numpy((np.float32(a) * ax + np.float32(b) * y.numpy()).astype(np.float32)))
+
+        # this rank generates its own rows only
+        s = S.ShardedCsr(None, device="cpu", local_spmv=local, n=n ** 3,
+                         make_rows=lambda r0, r1: synth.stencil_27pt_rows(n, r0, r1))
+        holder["s"] = s
+        x0, y0 = _vectors(n ** 3)
+        s.load(x0, y0)
+        s.iterate(k, 0.05, 0.5)
+        q.put((rank, s.global_x(), s.bounds, s.host.nnz))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_from_own_rows_match_one_process(world):
+    """Each rank builds its slab from its own rows of the 27-point stencil
+    (no rank holds the whole matrix; rows split evenly): x after k steps
+    equals the one-process loop on the whole matrix assembled from the same
+    row generator, bit for bit."""
+    from clspmv_mic_b200 import synth
+    n, k = 9, 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rows_worker, args=(r, world, port, q, n, k)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=180) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    m = n ** 3
+    bounds = S.split_rows_even(m, world)
+    parts = [synth.stencil_27pt_rows(n, r0, r1) for r0, r1 in bounds]
+    rp = np.concatenate([[0]] + [p[0][1:] + sum(int(q[0][-1]) for q in parts[:i]) for i, p in enumerate(parts)])
+    csr = F.from_arrays("csr", dict(width=m, height=m, nnz=int(rp[-1])),
+                        dict(csr_row_ptr=rp.astype(np.int32), csr_col_id=np.concatenate([p[1] for p in parts]),
+                             csr_data=np.concatenate([p[2] for p in parts])))
+    x0, y0 = _vectors(m)
+    ref = _loop_reference(csr, x0, y0, k, 0.05, 0.5)
+    assert sum(t[3] for t in out) == csr.nnz
+    for rank, x, b, _ in out:
+        assert b == bounds
+        assert np.array_equal(x.view(np.uint32), ref.view(np.uint32)), rank
