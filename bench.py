@@ -66,7 +66,7 @@ def parse_args():
     p.add_argument("--only", default="", help="comma list of format keys to run (debugging)")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the several-right-hand-side, batched and serving measurements")
-    p.add_argument("--serving-requests", type=int, default=1000)
+    p.add_argument("--serving-requests", type=int, default=4000)
     p.add_argument("--detail-file", default="",
                    help="also write every measurement (per format, variants, parity, extras) to this JSON file")
     return p.parse_args()
@@ -937,29 +937,33 @@ def run_extras(args, items, mats, peak):
     out["spmm"]["seconds"] = round(time.perf_counter() - t0, 1)
 
     t0 = time.perf_counter()
-    mats256 = W.uneven_matrices(256)
-    out["batched"] = {"config": "256 CSR matrices, rows log-uniform [1k, 500k], 5-64 nnz/row, banded/blocked/random "
-                                "(generated on the device); one persistent launch replayed from a CUDA graph vs one "
-                                "plain launch per matrix",
-                      "nnz_total": int(sum(m.nnz for _, m in mats256)),
+    mats256 = W.uneven_matrices(256, tuned=True, check=8)
+    out["batched"] = {"config": "256 matrices, rows log-uniform [1k, 500k], 5-64 nnz/row, banded/blocked/random "
+                                "(generated on the device), each stored in the fastest layout for its structure "
+                                "(banded: DIA/ELL/CSR, blocked: SBELL/BCSR/BELL 4x4/CSR, random: CSR; converted on "
+                                "the device); one persistent launch replayed from a CUDA graph vs one plain launch "
+                                "per matrix; err_fp64 over every row of the first 8 matrices",
+                      "nnz_total": int(sum(e[1].nnz for e in mats256)),
+                      "layouts": W.layout_counts(mats256),
                       "results": W.batched(mats256)}
     del mats256
     torch.cuda.empty_cache()
     out["batched"]["seconds"] = round(time.perf_counter() - t0, 1)
 
     t0 = time.perf_counter()
-    smats = W.serving_matrices(64)
+    smats = W.serving_matrices(64, tuned=True)
     nnz = int(sum(m.nnz for m in smats))
     budget = 120 * 10 ** 9
-    out["serving"] = {"config": f"64 resident CSR matrices (rows 10k-4M, 20M-200M nnz, {nnz} nnz in all), "
-                                f"120 GB budget, Poisson arrivals, sequential = one plain launch + sync per request",
-                      "mixed_k": W.serve(smats, budget, args.serving_requests, rate=20_000.0, k_lo=1, k_hi=32),
-                      "k1": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1),
-                      "k1_bf16": W.serve(smats, budget, 2 * args.serving_requests, rate=50_000.0, k_lo=1, k_hi=1,
-                                         value_type="bf16"),
+    n = args.serving_requests
+    out["serving"] = {"config": f"64 resident matrices (rows 10k-4M, 20M-200M nnz, {nnz} nnz in all), each in the "
+                                f"fastest layout for its structure, 120 GB budget, Poisson arrivals, sequential = one "
+                                f"plain launch + sync per request; long enough streams for tens of batches",
+                      "layouts": W.layout_counts([(getattr(m, "structure", "?"), m) for m in smats]),
+                      "mixed_k": W.serve(smats, budget, n, rate=20_000.0, k_lo=1, k_hi=32),
+                      "k1": W.serve(smats, budget, 3 * n, rate=50_000.0, k_lo=1, k_hi=1),
+                      "k1_bf16": W.serve(smats, budget, 3 * n, rate=50_000.0, k_lo=1, k_hi=1, value_type="bf16"),
                       # below the sequential capacity: latency without a queue
-                      "mixed_k_light": W.serve(smats, budget, max(100, args.serving_requests // 2), rate=200.0,
-                                               k_lo=1, k_hi=32)}
+                      "mixed_k_light": W.serve(smats, budget, 300, rate=200.0, k_lo=1, k_hi=32)}
     del smats
     torch.cuda.empty_cache()
     out["serving"]["seconds"] = round(time.perf_counter() - t0, 1)
@@ -1067,7 +1071,8 @@ def run_cocktail_c3(args, peak):
                              "then each SELL / block part re-stored in every slice height / block shape, timed alone, "
                              "the fastest kept when the whole partition gets faster"}
     out["partition"] = mat.summary()
-    dev = mat.to_device()
+    out["runtime"] = {"chosen": res.runtime, "candidates": res.runtime_report}
+    dev = res.to_device()
     h, w = coo.shape
     x = torch.rand(w, device="cuda") * 2 - 1
     y = torch.zeros(h, device="cuda")
@@ -1090,7 +1095,7 @@ def run_cocktail_c3(args, peak):
         return e0.elapsed_time(e1) / reps
 
     ms_fused = timed("fused") if dev.fused_items > 0 else None
-    ms = timed("auto")
+    ms = timed(res.runtime.get("schedule", "auto"))
     stored = sum(p.stored_bytes() for p in mat.parts().values())
     ab = stored + 4 * w + 8 * h
     out.update(rows=h, nnz=int(coo.nnz), ms=round(ms, 4), gflops=round(2 * coo.nnz / (ms * 1e-3) / 1e9, 1),

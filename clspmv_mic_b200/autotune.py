@@ -153,10 +153,21 @@ def _partition_key(m: CocktailMatrix):
     return tuple(sorted((k, v["nnz"]) for k, v in m.summary().items() if isinstance(v, dict) and "nnz" in v))
 
 
-def measure_ms(m: CocktailMatrix, reps: int = 10) -> float:
+def apply_runtime(dev, runtime: dict) -> None:
+    """Runtime settings of a tuned partition on its device handle: schedule
+    ("per_part" / "fused") and the CSR part's lanes per row (0: chunks)."""
+    if runtime.get("schedule", "per_part") != "per_part":
+        dev.set_schedule(runtime["schedule"])
+    if runtime.get("csr_lanes", 0):
+        dev.set_csr_lanes(runtime["csr_lanes"])
+
+
+def measure_ms(m: CocktailMatrix, reps: int = 10, runtime: dict | None = None) -> float:
     """Mean time of y += A x over `reps` runs of the Cocktail runtime."""
     import torch
     dev = m.to_device()
+    if runtime:
+        apply_runtime(dev, runtime)
     try:
         h, w = m.struct.mat_height, m.struct.mat_width
         x = torch.rand(w, device="cuda")
@@ -174,6 +185,35 @@ def measure_ms(m: CocktailMatrix, reps: int = 10) -> float:
         dev.close()
 
 
+CSR_LANES = (0, 1, 2, 4, 8, 16, 32)
+
+
+def tune_runtime(m: CocktailMatrix, reps: int = 10, report: list | None = None) -> tuple:
+    """The launch schedule (one launch per part, or the fused persistent
+    launch when the partition has two or more parts it covers) and, with a
+    CSR part, its threads per row (nonzero chunks, or CSR-vector with 1..32
+    lanes per row), measured in that order. Returns (settings, ms)."""
+    best = {"schedule": "per_part", "csr_lanes": 0}
+    best_ms = measure_ms(m, reps, best)
+    if report is not None:
+        report.append(dict(runtime=dict(best), ms=round(best_ms, 4)))
+    dev = m.to_device()
+    fusable = dev.fused_items > 0
+    dev.close()
+    cands = [{"schedule": "fused", "csr_lanes": 0}] if fusable else []
+    if m.uses("csr"):
+        cands += [{"schedule": "per_part", "csr_lanes": t} for t in CSR_LANES if t]
+    for rt in cands:
+        if rt["csr_lanes"] and best["schedule"] == "fused":
+            continue   # the fused launch runs the CSR part by chunks
+        ms = measure_ms(m, reps, rt)
+        if report is not None:
+            report.append(dict(runtime=dict(rt), ms=round(ms, 4)))
+        if ms < best_ms:
+            best, best_ms = dict(rt), ms
+    return best, best_ms
+
+
 @dataclass
 class TuneResult:
     matrix: CocktailMatrix
@@ -184,6 +224,14 @@ class TuneResult:
     parts: dict = field(default_factory=dict)        # refined part layouts
     part_report: list = field(default_factory=list)
     ms_partition: float | None = None                 # before the part refinement
+    runtime: dict = field(default_factory=dict)      # schedule and CSR lanes per row
+    runtime_report: list = field(default_factory=list)
+
+    def to_device(self):
+        """The tuned partition on the device with its runtime settings."""
+        dev = self.matrix.to_device()
+        apply_runtime(dev, self.runtime)
+        return dev
 
 
 def default_cache() -> Path:
@@ -191,8 +239,10 @@ def default_cache() -> Path:
 
 
 def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None, reps: int = 10,
-         knobs=KNOBS, use_cache: bool = True, refine: bool = True) -> TuneResult:
-    """Fastest measured partition of `coo` over the knob settings."""
+         knobs=KNOBS, use_cache: bool = True, refine: bool = True, runtime: bool = True) -> TuneResult:
+    """Fastest measured partition of `coo` over the knob settings, its parts'
+    layouts (refine) and its runtime settings: launch schedule and the CSR
+    part's threads per row (runtime)."""
     cache = Path(cache) if cache is not None else default_cache()
     sig = signature(coo)
     entries = {}
@@ -204,7 +254,8 @@ def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None
     if use_cache and sig in entries:
         knob, parts = entries[sig]["knob"], entries[sig].get("parts", {})
         m = apply_part_layouts(partition(coo, table_dir, knob), parts)
-        return TuneResult(m, knob, entries[sig]["ms"], from_cache=True, parts=parts)
+        return TuneResult(m, knob, entries[sig]["ms"], from_cache=True, parts=parts,
+                          runtime=entries[sig].get("runtime", {}))
     best, seen, report = None, {}, []
     for ref_knob in knobs:
         base = analyze(coo, table_dir, **ref_knob)
@@ -228,8 +279,13 @@ def tune(coo: HostMatrix, table_dir=None, cache: str | os.PathLike | None = None
             ms = measure_ms(m, reps)
             if ms < best.ms:
                 best.matrix, best.ms, best.parts = m, ms, layouts
-    entries[sig] = {"knob": best.knob, "parts": best.parts, "ms": best.ms, "shape": list(coo.shape),
-                    "nnz": int(coo.nnz)}
+    if runtime:
+        rt, ms = tune_runtime(best.matrix, reps, best.runtime_report)
+        if ms < best.ms:
+            best.ms = ms
+        best.runtime = rt
+    entries[sig] = {"knob": best.knob, "parts": best.parts, "runtime": best.runtime, "ms": best.ms,
+                    "shape": list(coo.shape), "nnz": int(coo.nnz)}
     try:
         cache.parent.mkdir(parents=True, exist_ok=True)
         cache.write_text(json.dumps(entries, indent=1))

@@ -133,6 +133,11 @@ class DeviceCocktail:
         work list; refused where a part is not covered)."""
         check(lib().clspmv_cocktail_set_schedule(self.handle, self.SCHEDULES[schedule]), "cocktail_set_schedule")
 
+    def set_csr_lanes(self, lanes: int) -> None:
+        """CSR part's kernel: 0 nonzero chunks, or CSR-vector with `lanes`
+        lanes per row (1..32, powers of two)."""
+        check(lib().clspmv_cocktail_set_csr_lanes(self.handle, int(lanes)), "cocktail_set_csr_lanes")
+
     @property
     def fused_items(self) -> int:
         """Work-list entries of the fused schedule (0: the handle has none)."""

@@ -28,6 +28,7 @@ struct clspmv_cocktail_handle {
     int nparts = 0;
     FusedPlan* fused = nullptr;       // one persistent launch over all parts (two or more parts)
     int schedule = CLSPMV_SCHEDULE_AUTO;
+    int csr_lanes = 0;                // CSR part: 0 nonzero chunks, T > 0 CSR-vector with T lanes per row
     cudaStream_t streams[9] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[9] = {};
@@ -72,7 +73,9 @@ int launch_part(const clspmv_cocktail_handle* h, int p, const float* x, float* y
         case P_BCSR: return launch_b4csr(&d.bcsr, x, y, alpha, beta, st, atomic);
         case P_SELL: return launch_sell(&d.sell, x, y, alpha, beta, st, atomic);
         case P_ELL: return launch_ell(&d.ell, x, y, alpha, beta, st, atomic);
-        case P_CSR: return launch_csr_chunk(&d.csr, h->chunk_plan, x, y, alpha, beta, st, atomic);
+        case P_CSR:
+            if (h->csr_lanes > 0) return launch_csr_vector(&d.csr, x, y, alpha, beta, h->csr_lanes, st, atomic);
+            return launch_csr_chunk(&d.csr, h->chunk_plan, x, y, alpha, beta, st, atomic);
         case P_COO: return launch_coo(&d.coo, x, y, alpha, beta, st, atomic);
     }
     return CLSPMV_ERR_ARG;
@@ -267,6 +270,18 @@ int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule)
 }
 
 int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h) { return h ? fused_plan_items(h->fused) : -1; }
+
+int clspmv_cocktail_set_csr_lanes(clspmv_cocktail_handle* h, int lanes)
+{
+    if (!h || !(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32))
+        return CLSPMV_ERR_ARG;
+    h->csr_lanes = lanes;
+    if (h->iter_exec) {   // the cached iteration graph was captured with the old kernel
+        cudaGraphExecDestroy(h->iter_exec);
+        h->iter_exec = nullptr;
+    }
+    return CLSPMV_OK;
+}
 
 int clspmv_cocktail_device_view(const clspmv_cocktail_handle* h, clspmv_cocktail_f32* out)
 {

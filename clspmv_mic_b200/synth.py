@@ -203,10 +203,13 @@ def device_csr(rows: int, cols: int, lo: int, hi: int, structure: str = "random"
                device="cuda"):
     """A CSR matrix generated on the device (for workloads too large to
     build on the host): row lengths uniform in [lo, hi]; columns
-    "random" (uniform), "banded" (a contiguous run centred on the diagonal)
-    or "blocked" (runs of 4 at 4-aligned block columns, the same block
-    columns for each group of 4 rows); values N(0, 1). Columns within a row
-    are not sorted and may repeat (both allowed by every CSR kernel)."""
+    "random" (uniform; unsorted within a row and possibly repeated, both
+    allowed by every CSR kernel), "banded" (a contiguous run centred on the
+    diagonal, shifted to stay inside the matrix: sorted, distinct) or
+    "blocked" (4 x 4 blocks: rows of a group of 4 share their block columns,
+    lengths rounded up to whole blocks, block columns of a group ascending
+    and distinct, so that the matrix converts exactly to the block formats);
+    values N(0, 1)."""
     import torch
     from .formats import DeviceMatrix
     g = torch.Generator(device=device)
@@ -214,6 +217,7 @@ def device_csr(rows: int, cols: int, lo: int, hi: int, structure: str = "random"
     lens = torch.randint(lo, hi + 1, (rows,), generator=g, device=device, dtype=torch.int64)
     if structure == "blocked":
         lens = (lens + 3) // 4 * 4
+    lens.clamp_(max=cols if structure != "blocked" else (cols // 4) * 4)
     row_ptr = torch.zeros(rows + 1, dtype=torch.int64, device=device)
     torch.cumsum(lens, 0, out=row_ptr[1:])
     nnz = int(row_ptr[-1].item())
@@ -225,12 +229,18 @@ def device_csr(rows: int, cols: int, lo: int, hi: int, structure: str = "random"
         col = torch.randint(0, cols, (nnz,), generator=g, device=device, dtype=torch.int64)
     elif structure == "banded":
         centre = row_of * cols // rows
-        col = (centre - lens[row_of] // 2 + pos).clamp_(0, cols - 1)
+        start = (centre - lens[row_of] // 2).clamp_(min=0)
+        start = torch.minimum(start, cols - lens[row_of])
+        col = start + pos
     elif structure == "blocked":
         nbc = max(1, cols // 4)
-        key = (row_of // 4) * 1000003 + pos // 4 + int(seed) * 7919
-        bc = (key * 2654435761) % nbc
-        col = (bc * 4 + pos % 4).clamp_(0, cols - 1)
+        maxnb = max(1, (hi + 3) // 4)
+        step = max(1, nbc // (2 * maxnb))
+        span = min(nbc - 1, (maxnb - 1) * step)
+        groups = (rows + 3) // 4
+        base = torch.randint(0, max(1, nbc - span), (groups,), generator=g, device=device, dtype=torch.int64)
+        bc = base[row_of // 4] + (pos // 4) * step
+        col = bc * 4 + pos % 4
     else:
         raise ValueError(structure)
     vals = torch.randn(nnz, generator=g, device=device, dtype=torch.float32)

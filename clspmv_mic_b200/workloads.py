@@ -69,8 +69,9 @@ class Fp64Rows:
         return float(err.max().item()) if err.numel() else 0.0
 
 
-def fp64_of_csr(dev_csr: DeviceMatrix, rows: int = 1 << 16) -> Fp64Rows:
-    return Fp64Rows(dev_csr, rows)
+def fp64_of_csr(dev_csr: DeviceMatrix, rows: int | None = 1 << 16) -> Fp64Rows:
+    """FP64 checker of the first `rows` rows (None: every row)."""
+    return Fp64Rows(dev_csr, dev_csr.shape[0] if rows is None else rows)
 
 
 def fp64_error(ref: Fp64Rows, X, Y, rows: int | None = None) -> float:
@@ -166,11 +167,74 @@ def spmm_tc_sweep(m, A64, ks=(16, 32, 64), reps: int = 10, hbm_gbs=None):
 # ---------------------------------------------------------------------------
 # Batches of uneven matrices (one persistent launch, captured in a graph)
 # ---------------------------------------------------------------------------
+def device_coo_of_csr(m: DeviceMatrix) -> DeviceMatrix:
+    """The entries of a device CSR matrix as a device COO (row ids expanded
+    from row_ptr; column ids and values shared with the CSR)."""
+    import torch
+    t = m.tensors
+    rp = t["csr_row_ptr"].long()
+    rows = torch.repeat_interleave(torch.arange(m.shape[0], device=rp.device, dtype=torch.int32), rp[1:] - rp[:-1])
+    return DeviceMatrix.from_device_arrays("coo", dict(width=m.shape[1], height=m.shape[0], nnz=m.nnz),
+                                           dict(coo_row_id=rows, coo_col_id=t["csr_col_id"], coo_data=t["csr_data"]))
+
+
+# candidate layouts per generated structure: (format, converter arguments); CSR is the generated matrix itself
+LAYOUTS = {
+    "banded": [("dia", ()), ("ell", ()), ("csr", None)],
+    "blocked": [("sbell", (4, 4, 32)), ("b4csr", (4, 4)), ("b4ell", (4, 4)), ("csr", None)],
+    "random": [("csr", None)],
+}
+
+
+def tuned_layout(m_csr: DeviceMatrix, structure: str, ks=(1, 16), reps: int = 3):
+    """The fastest of the structure's candidate layouts (LAYOUTS), timed as
+    one job of the shared batch launch at each k in `ks` (one and many right-
+    hand sides) and ranked by the sum, each candidate converted on the device
+    from the matrix's entries (clspmv_device_coo2<fmt>_f32; the same entries,
+    so the same product). Returns (matrix, format, {format: ms summed})."""
+    import torch
+    from . import _abi
+    from .formats import device_convert
+    rows, cols = m_csr.shape
+    coo = device_coo_of_csr(m_csr)
+    XY = [(torch.rand((cols, k), device="cuda"), torch.zeros((rows, k), device="cuda")) for k in ks]
+    b = Batch(1)
+    best, best_fmt, best_ms, times = m_csr, "csr", None, {}
+    try:
+        for fmt, args in LAYOUTS[structure]:
+            try:
+                cand = m_csr if fmt == "csr" else device_convert(coo, fmt, *args)
+            except _abi.ClspmvError:      # refused (DIA fill rule, block caps) or unsorted input
+                times[fmt] = None
+                continue
+            ms = 0.0
+            for X, Y in XY:
+                b.set([Job(cand, X, Y, alpha=1.0, beta=1.0)])
+                b.run()
+                e0, e1 = _events(torch)
+                e0.record()
+                for _ in range(reps):
+                    b.run()
+                e1.record()
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1) / reps
+            times[fmt] = round(ms, 4)
+            if best_ms is None or ms < best_ms:
+                best, best_fmt, best_ms = cand, fmt, ms
+    finally:
+        b.close()
+    del coo, XY
+    return best, best_fmt, times
+
+
 def uneven_matrices(count: int = 256, rows_lo: int = 1000, rows_hi: int = 500_000, npr_lo: int = 5, npr_hi: int = 64,
-                    seed: int = 1234):
-    """Device CSR matrices: rows log-uniform in [rows_lo, rows_hi], mean
+                    seed: int = 1234, tuned: bool = False, check: int = 0):
+    """Device matrices: rows log-uniform in [rows_lo, rows_hi], mean
     nonzeros per row uniform in [npr_lo, npr_hi], structure banded /
-    blocked / random drawn per matrix."""
+    blocked / random drawn per matrix. Returns (structure, matrix, checker)
+    triples: the matrix as CSR, or (tuned) in the fastest layout for its
+    structure (tuned_layout); checker = the FP64 checker of every row
+    (Fp64Rows of the CSR) for the first `check` matrices, else None."""
     rng = np.random.default_rng(seed)
     mats = []
     for i in range(count):
@@ -178,18 +242,37 @@ def uneven_matrices(count: int = 256, rows_lo: int = 1000, rows_hi: int = 500_00
         npr = int(rng.integers(npr_lo, npr_hi + 1))
         structure = ["banded", "blocked", "random"][int(rng.integers(3))]
         lo, hi = max(1, npr - npr // 4), npr + npr // 4
-        mats.append((structure, synth.device_csr(rows, rows, lo, hi, structure, seed=seed + i)))
+        csr = synth.device_csr(rows, rows, lo, hi, structure, seed=seed + i)
+        ref = fp64_of_csr(csr, None) if i < check else None
+        m = tuned_layout(csr, structure)[0] if tuned else csr
+        mats.append((structure, m, ref))
     return mats
+
+
+def layout_counts(mats) -> dict:
+    """How many matrices of each structure ended in each format."""
+    out = {}
+    for entry in mats:
+        key = f"{entry[0]}->{entry[1].fmt}"
+        out[key] = out.get(key, 0) + 1
+    return out
 
 
 def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: int = 10, check: int = 8):
     """Per (value type, k): all matrices as ONE batch launch replayed from a
-    CUDA graph, against the same jobs as one plain launch per matrix."""
+    CUDA graph, against the same jobs as one plain launch per matrix.
+    `mats`: (structure, matrix[, checker]) entries; the error against FP64
+    covers the entries that carry a checker (else the first `check` CSR
+    matrices, every row)."""
     import torch
     out = {}
-    nnz_total = sum(m.nnz for _, m in mats)
+    nnz_total = sum(e[1].nnz for e in mats)
+    refs = [e[2] if len(e) > 2 else None for e in mats]
+    if not any(r is not None for r in refs):
+        refs = [fp64_of_csr(e[1], None) if i < check and e[1].fmt == "csr" else None for i, e in enumerate(mats)]
+    checked = [i for i, r in enumerate(refs) if r is not None]
+    mats = [(e[0], e[1]) for e in mats]
     packs = {vt: [None if vt == "f32" else m.pack(vt) for _, m in mats] for vt in value_types}
-    A64 = [fp64_of_csr(m) for _, m in mats[:check]]
     gen = torch.Generator(device="cuda")
     gen.manual_seed(7)
     s = torch.cuda.Stream()
@@ -222,7 +305,7 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
                 Y.zero_()
             g.replay()
             torch.cuda.synchronize()
-            err = max(fp64_error(a, X, Y) for a, X, Y in zip(A64, Xs, Ys))
+            err = max((fp64_error(refs[i], Xs[i], Ys[i]) for i in checked), default=0.0)
             # the same jobs, one plain clspmv_spmm launch each
             for j in jobs:
                 j.matrix.spmm(j.X, j.Y, 1.0, 0.0, packed=j.packed)
@@ -246,7 +329,10 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
 # Serving: Poisson arrivals against resident matrices
 # ---------------------------------------------------------------------------
 def serving_matrices(count: int = 64, rows_lo: int = 10_000, rows_hi: int = 4_000_000, nnz_lo: float = 20e6,
-                     nnz_hi: float = 200e6, seed: int = 99):
+                     nnz_hi: float = 200e6, seed: int = 99, tuned: bool = False):
+    """Device matrices for the serving stream (rows log-uniform, nonzeros
+    log-uniform, structure banded / blocked / random), as CSR or (tuned)
+    each in the fastest layout for its structure (tuned_layout)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -255,7 +341,11 @@ def serving_matrices(count: int = 64, rows_lo: int = 10_000, rows_hi: int = 4_00
         npr = max(1, int(round(nnz / rows)))
         npr = min(npr, rows)
         structure = ["banded", "blocked", "random"][int(rng.integers(3))]
-        out.append(synth.device_csr(rows, rows, max(1, npr - npr // 8), npr + npr // 8, structure, seed=seed + i))
+        m = synth.device_csr(rows, rows, max(1, npr - npr // 8), npr + npr // 8, structure, seed=seed + i)
+        if tuned:
+            m = tuned_layout(m, structure)[0]
+            m.structure = structure
+        out.append(m)
     return out
 
 
@@ -268,14 +358,14 @@ def _wait_until(t: float) -> None:
 
 
 def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.0, k_lo: int = 1, k_hi: int = 32,
-          value_type: str = "f32", seed: int = 3, slots: int = 2):
+          value_type: str = "f32", seed: int = 3, slots: int = 2, max_requests: int = 4096):
     """Open-loop Poisson stream of `n_requests` at `rate` req/s, k uniform in
     [k_lo, k_hi], matrix uniform among the admitted ones. Returns the serving
     loop's and the sequential baseline's req/s and p50 / p99 latency."""
     import torch
     from .serving import SpmvServer, latency_stats
     rng = np.random.default_rng(seed)
-    srv = SpmvServer(budget_bytes, slots=slots)
+    srv = SpmvServer(budget_bytes, slots=slots, max_requests=max_requests)
     names = []
     for i, m in enumerate(mats):
         p = None if value_type == "f32" else m.pack(value_type)

@@ -646,6 +646,13 @@ int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule);
 /* Work-list entries of the fused schedule, 0 when the handle has none (one
  * part, or a part the fused kernel does not cover). */
 int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h);
+/* Kernel of the CSR part under the per-part schedule: 0 (default) nonzero
+ * chunks, or CSR-vector with `lanes` (1, 2, 4, 8, 16 or 32) lanes per row,
+ * the reference's threads-per-row knob (its CSR-vector driver sweeps the
+ * work-group count, src/spmv_csr_vector.cpp:106; the Cocktail tables carry
+ * it per part, src/spmv_cocktail.cpp:918-962). The partition tuner measures
+ * the choices. */
+int clspmv_cocktail_set_csr_lanes(clspmv_cocktail_handle* h, int lanes);
 /* The reference's A^k x loop (src/eval.cpp:19-72) kept on the device:
  * `iterations` times y <- alpha*A*x + beta*y, then the first mat_height
  * entries of x <- y (cpy_vector_from_gpu, src/spmv_cocktail.cpp:1510-1556).

@@ -44,3 +44,37 @@ def fp64_error(y, y64, bound):
     with np.errstate(divide="ignore", invalid="ignore"):
         r = np.abs(y.astype(np.float64) - y64) / np.where(bound > 0, bound, 1.0)
     return float(np.max(r)) if r.size else 0.0
+
+
+def columns_reference(coo, X, alpha=1.0):
+    """Per column j of X: y32 = alpha * csr_spmv(A, X[:, j]) (the oracle's
+    FP32 routine), y64 (FP64) and the row scale |alpha| sum_i |a_ri X[i, j]|;
+    arrays of shape (rows, k)."""
+    csr = F.coo2csr(coo)
+    X = np.asarray(X, dtype=np.float32)
+    y32, y64, sc = [], [], []
+    for j in range(X.shape[1]):
+        xj = np.ascontiguousarray(X[:, j])
+        y32.append(np.float32(alpha) * O.spmv_port(csr, xj))
+        a, b = O.csr_f64(csr, xj)
+        y64.append(alpha * a)
+        sc.append(abs(alpha) * b)
+    return np.stack(y32, 1), np.stack(y64, 1), np.stack(sc, 1)
+
+
+# per-row bounds by value type: FP32 values against the FP32 oracle; 16-bit
+# values (rounded to 2^-9 / 2^-11 relative with a per-row power-of-two
+# scale) against FP64
+VALUE_RTOL = {"f32": RTOL, "bf16": 2.0 ** -8, "f16": 2.0 ** -10}
+
+
+def assert_columns_close(got, ref, value_type="f32", what=""):
+    """got (rows x k) within the per-row, per-column bound of `ref` =
+    columns_reference(...): |got - y32| <= 1e-5 scale for FP32 values,
+    |got - y64| <= 2^-8 / 2^-10 scale for BF16 / FP16."""
+    y32, y64, sc = ref
+    g = np.asarray(got, dtype=np.float64)
+    err = np.abs(g - (y32.astype(np.float64) if value_type == "f32" else y64))
+    lim = VALUE_RTOL[value_type] * sc + 1e-30
+    bad = np.argwhere(err > lim)
+    assert bad.size == 0, f"{what}: {len(bad)} entries outside the {value_type} row bound, first {bad[:3].tolist()}"

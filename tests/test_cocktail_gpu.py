@@ -206,6 +206,25 @@ def test_cocktail_hand_partitions(layout, schedule):
         assert_close(yd.cpu().numpy(), y_ref, bound, f"{layout} {schedule} parts={dev.parts}")
 
 
+@pytest.mark.parametrize("lanes", [0, 1, 4, 32])
+def test_cocktail_csr_part_lanes(setup, lanes):
+    """The CSR part run as nonzero chunks (0) or CSR-vector with 1..32 lanes
+    per row (the tuner's threads-per-row choice): the same y within the
+    1e-5 row bound."""
+    import torch
+    coo, ck = setup[("block_partial", "blocks_noise")]
+    dev = ck.to_device()
+    assert "csr" in dev.parts, dev.parts
+    dev.set_csr_lanes(lanes)
+    x = synth.x_vector(coo.shape[1])
+    y0 = np.random.default_rng(4).standard_normal(coo.shape[0]).astype(np.float32)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+    dev.spmv(xd, yd, 1.0, 0.5)
+    torch.cuda.synchronize()
+    y_ref, _, bound = reference_y(coo, x, y0, 1.0, 0.5)
+    assert_close(yd.cpu().numpy(), y_ref, bound, f"csr lanes {lanes}")
+
+
 def test_cocktail_graph_replay(setup):
     """Capture y <- A x + y once, replay it k times: y = y0 + k A x."""
     import torch

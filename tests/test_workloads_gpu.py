@@ -33,6 +33,46 @@ def test_batched_small():
         assert r["ms"] > 0 and r["plain_ms"] > 0
 
 
+def test_batched_tuned_layouts():
+    """The batch with each matrix in the fastest layout for its structure
+    (DIA / ELL for banded, SBELL / BCSR / BELL 4x4 for blocked, converted on
+    the device from the generated CSR): every checked matrix (all rows)
+    within the FP64 bound, and the layouts come from the candidate lists."""
+    mats = W.uneven_matrices(12, rows_lo=500, rows_hi=20_000, npr_lo=5, npr_hi=40, tuned=True, check=12)
+    for structure, m, _ in mats:
+        assert m.fmt in [f for f, _ in W.LAYOUTS[structure]], (structure, m.fmt)
+    out = W.batched(mats, ks=(1, 8), reps=2)
+    for key, r in out.items():
+        bound = 1e-5 if key.endswith("f32") else (2.0 ** -8 if key.endswith("bf16") else 2.0 ** -10)
+        assert r["err_fp64"] <= bound, (key, r)
+
+
+def test_tuned_layout_is_the_same_matrix():
+    """A banded and a blocked generated matrix converted to every candidate
+    layout give the CSR's product (the generators emit sorted, distinct
+    columns for these structures, so the conversion keeps every entry)."""
+    import torch
+    from clspmv_mic_b200 import synth
+    for structure in ("banded", "blocked"):
+        csr = synth.device_csr(3000, 3000, 8, 24, structure, seed=11)
+        coo = W.device_coo_of_csr(csr)
+        ref = W.fp64_of_csr(csr, None)              # every row, FP64, per-row scale sum|a x|
+        x = torch.rand(3000, device="cuda") * 2 - 1
+        converted = 0
+        for fmt, args in W.LAYOUTS[structure]:
+            try:
+                m = csr if fmt == "csr" else F.device_convert(coo, fmt, *args)
+            except __import__("clspmv_mic_b200")._abi.ClspmvError as e:
+                assert e.status == __import__("clspmv_mic_b200")._abi.ERR_REFUSED, (structure, fmt)
+                continue    # the DIA fill rule refuses bands shifted at the matrix edges
+            converted += 1
+            y = torch.full((3000,), float("nan"), device="cuda")
+            m.spmv(x, y, 1.0, 0.0)
+            torch.cuda.synchronize()
+            assert ref.error(x[:, None], y[:, None]) <= 1e-5, (structure, fmt)
+        assert converted >= 2, structure
+
+
 def test_serve_small():
     mats = W.serving_matrices(4, rows_lo=2000, rows_hi=20_000, nnz_lo=2e5, nnz_hi=1e6)
     r = W.serve(mats, 1 << 34, n_requests=60, rate=5000.0, k_lo=1, k_hi=8)
@@ -70,9 +110,10 @@ def test_tune_measures_and_caches(tmp_path):
     assert min(c["ms"] for c in r.report) == pytest.approx(r.ms_partition, abs=1e-4)
     assert r.ms <= r.ms_partition + 1e-9
     again = tune(coo, root, cache=cache)
-    assert again.from_cache and again.knob == r.knob and again.parts == r.parts
+    assert again.from_cache and again.knob == r.knob and again.parts == r.parts and again.runtime == r.runtime
+    assert r.runtime.get("schedule") in ("per_part", "fused") and r.runtime_report
     import torch
-    dev = again.matrix.to_device()
+    dev = again.to_device()
     x = torch.rand(coo.shape[1], device="cuda")
     y = torch.zeros(coo.shape[0], device="cuda")
     dev.spmv(x, y, 1.0, 0.0)
