@@ -147,13 +147,29 @@ __global__ void __launch_bounds__(kBlock) k_csr_merge_plan(int rows, int nnz, co
     csr_merge_search(rows, nnz, row_ptr, (long long)t * kMergeTile, tc + 2 * t);
 }
 
-template <class V, int GX = 0>
-__global__ void __launch_bounds__(kBlock) k_coo(CooArgsT<V> a) { coo_cta<V, GX>(a, blockIdx.x, gridDim.x, nullptr); }
+template <class V, int GX = 0, int MINB = 5>
+__global__ void __launch_bounds__(kBlock, MINB) k_coo(CooArgsT<V> a) { coo_cta<V, GX>(a, blockIdx.x, gridDim.x, nullptr); }
 
-template <class V, int GX = 0>
-__global__ void __launch_bounds__(kBlock) k_csr_chunk(CsrArgsT<V> a, const int* __restrict__ chunk_row)
+template <class V, int GX = 0, int MINB = 5>
+__global__ void __launch_bounds__(kBlock, MINB) k_csr_chunk(CsrArgsT<V> a, const int* __restrict__ chunk_row)
 {
     csr_chunk_cta<V, GX>(a, chunk_row, blockIdx.x, gridDim.x);
+}
+
+// Resident CTAs per SM the gather kernels are compiled for (register cap):
+// 5 (48 registers), 6 (40), 8 (32). Measured on B200 (power-law 2^20): CSR
+// by chunks fits 32 registers without spilling and gains 2 % at 8 CTAs
+// (90.4 -> 88.4 us); COO spills below 48 and loses (84.9 -> 89.1 / 103 us).
+// CLSPMV_GATHER_OCC overrides both (measurements).
+constexpr int kCsrChunkDefaultOcc = 8, kCooDefaultOcc = 5;
+int gather_occ(int dflt)
+{
+    static int f = [] {
+        const char* e = getenv("CLSPMV_GATHER_OCC");
+        const int v = e ? atoi(e) : 0;
+        return v == 5 || v == 6 || v == 8 ? v : 0;
+    }();
+    return f ? f : dflt;
 }
 
 // Form of the scattered x gathers of COO and CSR by chunks (ld_gx): 0 through
@@ -183,6 +199,28 @@ __global__ void __launch_bounds__(kBlock) k_sbell(SbellArgsT<V> a) { sbell_cta<B
 
 template <int BW4, int BH, int T, bool A, class V>
 __global__ void __launch_bounds__(kBlock) k_b4csr(B4csrArgsT<V> a) { b4csr_cta<BW4, BH, T, A>(a, blockIdx.x, gridDim.x, nullptr); }
+
+// The 4x4-block kernels (FP32 values, own rows) compiled for MINB resident
+// CTAs per SM (a register cap); CLSPMV_BLOCK_OCC = 6 or 8 selects them
+// (measurements; 1 = the uncapped kernels above, the default). Measured on
+// B200 (500k x 8 4x4 blocks): all three spill under the cap and lose
+// (BELL 55 -> 63 / 72 us, SBELL 57 -> 66 / 63 us, BCSR 59 -> 61 / 98 us).
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_b4ell_occ(B4ellArgsT<float> a) { b4ell_cta<1, 4, false>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_sbell_occ(SbellArgsT<float> a) { sbell_cta<1, 4, false>(a, blockIdx.x, gridDim.x, nullptr); }
+template <int T, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_b4csr_occ(B4csrArgsT<float> a) { b4csr_cta<1, 4, T, false>(a, blockIdx.x, gridDim.x, nullptr); }
+constexpr int kBlockDefaultOcc = 1;
+int block_occ()
+{
+    static int f = [] {
+        const char* e = getenv("CLSPMV_BLOCK_OCC");
+        const int v = e ? atoi(e) : kBlockDefaultOcc;
+        return v == 6 || v == 8 ? v : 1;
+    }();
+    return f;
+}
 
 // CTAs that fit on the device at once for `kernel` (SM count x resident
 // CTAs per SM), cached per kernel.
@@ -533,10 +571,17 @@ int launch_csr_chunk_v(const clspmv_csr_f32* m, const V* data, const float* scal
     if (!aligned16(m->csr_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
     CsrArgsT<V> a{rows, m->matinfo.nnz, m->csr_row_ptr, m->csr_col_id, data, x, y, alpha, 1.0f, scale};
     const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
-    if (gather_form() == 1)
-        k_csr_chunk<V, 1><<<persistent_grid(k_csr_chunk<V, 1>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
-    else
-        k_csr_chunk<V, 0><<<persistent_grid(k_csr_chunk<V, 0>, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row);
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, nchunks, kBlock / 32), kBlock, 0, st>>>(a, chunk_row); };
+    const int occ = gather_occ(kCsrChunkDefaultOcc);
+    if (gather_form() == 1) {
+        if (occ == 8) go(k_csr_chunk<V, 1, 8>);
+        else if (occ == 6) go(k_csr_chunk<V, 1, 6>);
+        else go(k_csr_chunk<V, 1, 5>);
+    } else {
+        if (occ == 8) go(k_csr_chunk<V, 0, 8>);
+        else if (occ == 6) go(k_csr_chunk<V, 0, 6>);
+        else go(k_csr_chunk<V, 0, 5>);
+    }
     return after_launch(1);
 }
 
@@ -570,8 +615,17 @@ int launch_coo_v(const clspmv_coo_f32* m, const V* data, const float* scale, con
     if (!aligned16(m->coo_row_id) || !aligned16(m->coo_col_id) || !aligned_v4(data)) return CLSPMV_ERR_ALIGN;
     CooArgsT<V> a{m->matinfo.nnz, m->coo_row_id, m->coo_col_id, data, x, y, alpha, scale};
     const long long nchunks = ((long long)m->matinfo.nnz + kCooWarpNnz - 1) / kCooWarpNnz;
-    if (gather_form() == 1) k_coo<V, 1><<<persistent_grid(k_coo<V, 1>, nchunks, kBlock / 32), kBlock, 0, st>>>(a);
-    else k_coo<V, 0><<<persistent_grid(k_coo<V, 0>, nchunks, kBlock / 32), kBlock, 0, st>>>(a);
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, nchunks, kBlock / 32), kBlock, 0, st>>>(a); };
+    const int occ = gather_occ(kCooDefaultOcc);
+    if (gather_form() == 1) {
+        if (occ == 8) go(k_coo<V, 1, 8>);
+        else if (occ == 6) go(k_coo<V, 1, 6>);
+        else go(k_coo<V, 1, 5>);
+    } else {
+        if (occ == 8) go(k_coo<V, 0, 8>);
+        else if (occ == 6) go(k_coo<V, 0, 6>);
+        else go(k_coo<V, 0, 5>);
+    }
     return after_launch(1);
 }
 
@@ -592,6 +646,14 @@ int launch_b4ell_v(const clspmv_b4ell_f32* m, const V* data, const float* scale,
     if ((long long)m->b4ell_row_num * m->b4ell_bheight < rows || m->b4ell_float4_aligned < 4 * m->b4ell_row_num) return CLSPMV_ERR_ARG;
     const B4ellArgsT<V> a{rows, m->matinfo.width, m->b4ell_row_num, m->b4ell_block_num, m->b4ell_height_aligned,
                           m->b4ell_float4_aligned, m->b4ell_col_id, data, x, y, alpha, beta, scale};
+    if constexpr (std::is_same<V, float>::value) {
+        if (!atomic && block_occ() != 1 && m->b4ell_bwidth == 4 && m->b4ell_bheight == 4) {
+            auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, a.nbrow, kBlock), kBlock, 0, st>>>(a); };
+            if (block_occ() == 8) go(k_b4ell_occ<8>);
+            else go(k_b4ell_occ<6>);
+            return after_launch(1);
+        }
+    }
     return dispatch_block(m->b4ell_bwidth, m->b4ell_bheight, [&](auto bw4, auto bh) {
         constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
         if (atomic) k_b4ell<BW4, BH, true, V><<<persistent_grid(k_b4ell<BW4, BH, true, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
@@ -617,6 +679,14 @@ int launch_sbell_v(const clspmv_sbell_f32* m, const V* data, const float* scale,
     if ((long long)m->sbell_row_num * m->sbell_bheight < rows) return CLSPMV_ERR_ARG;
     const SbellArgsT<V> a{rows, m->matinfo.width, m->sbell_row_num, m->sbell_slice_num, (int)m->sbell_slice_height,
                           m->sbell_slice_ptr, m->sbell_col_id, data, x, y, alpha, beta, scale};
+    if constexpr (std::is_same<V, float>::value) {
+        if (!atomic && block_occ() != 1 && m->sbell_bwidth == 4 && m->sbell_bheight == 4) {
+            auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, a.nbrow, kBlock), kBlock, 0, st>>>(a); };
+            if (block_occ() == 8) go(k_sbell_occ<8>);
+            else go(k_sbell_occ<6>);
+            return after_launch(1);
+        }
+    }
     return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
         constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
         if (atomic) k_sbell<BW4, BH, true, V><<<persistent_grid(k_sbell<BW4, BH, true, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
@@ -649,6 +719,19 @@ int launch_b4csr_v(const clspmv_b4csr_f32* m, const V* data, const float* scale,
         return e ? std::max(1, atoi(e)) : 1;
     }();
     const int lanes = pow2_lanes((double)m->b4csr_block_num / m->b4csr_row_num / bpl, 1, 32);
+    if constexpr (std::is_same<V, float>::value) {
+        if (!atomic && block_occ() != 1 && m->b4csr_bwidth == 4 && m->b4csr_bheight == 4 && (lanes == 4 || lanes == 8)) {
+            auto go = [&](auto kernel, int t) { kernel<<<persistent_grid(kernel, a.nbrow, kBlock / t), kBlock, 0, st>>>(a); };
+            if (block_occ() == 8) {
+                if (lanes == 8) go(k_b4csr_occ<8, 8>, 8);
+                else go(k_b4csr_occ<4, 8>, 4);
+            } else {
+                if (lanes == 8) go(k_b4csr_occ<8, 6>, 8);
+                else go(k_b4csr_occ<4, 6>, 4);
+            }
+            return after_launch(1);
+        }
+    }
     return dispatch_block(m->b4csr_bwidth, m->b4csr_bheight, [&](auto bw4, auto bh) {
         return dispatch_lanes(lanes, [&](auto t) {
             constexpr int T = decltype(t)::value;
