@@ -261,6 +261,15 @@ __global__ void k_dia_mark(const int* __restrict__ row, const int* __restrict__ 
     GRID_STRIDE(i, n) flag[(long long)col[i] - row[i] + h - 1] = 1;
 }
 
+// flags[0] = 1 when some row id is >= len
+__global__ void k_rows_at_least(const int* __restrict__ row, long long n, long long len, int* flags)
+{
+    int f = 0;
+    GRID_STRIDE(i, n) if (row[i] >= len) f = 1;
+    f = __reduce_or_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
 __global__ void k_dia_offsets(const int* __restrict__ flag, const int* __restrict__ rank, long long nd, int h, int* off)
 {
     GRID_STRIDE(p, nd)
@@ -620,11 +629,21 @@ int dia_core(const clspmv_coo_f32* src, clspmv_dia_f32* dst, int alignment, cuda
     if (rc) return rc;
     if (flags & 2) return CLSPMV_ERR_ARG;
     // dia_data[row] with row < aligned(min(w, h)): a taller-than-wide matrix
-    // would overflow it, so it is rejected (as by clspmv_coo2dia_f32).
-    if (c.h > c.w) return CLSPMV_ERR_ARG;
+    // converts while every entry sits above that row, and is rejected when one
+    // does not (as by clspmv_coo2dia_f32: the reference writes past its arrays)
+    const long long len = aligned_len(std::min(c.w, c.h), alignment);
+    if (c.h > c.w && c.n > 0) {
+        int* f = S.get<int>(1);
+        if (S.rc) return S.rc;
+        if ((rc = cuda_status(cudaMemsetAsync(f, 0, sizeof(int), st)))) return rc;
+        k_rows_at_least<<<grid_for(c.n), kT, 0, st>>>(c.row, c.n, len, f);
+        if ((rc = launched(st))) return rc;
+        int below = 0;
+        if ((rc = read_back(f, &below, st))) return rc;
+        if (below) return CLSPMV_ERR_ARG;
+    }
     dst->matinfo = src->matinfo;
     dst->dia_length = std::min(c.w, c.h);
-    const long long len = aligned_len(dst->dia_length, alignment);
     dst->dia_length_aligned = (int)len;
     dst->dia_num = 0;
     dst->dia_offsets = nullptr;

@@ -20,7 +20,7 @@ torch = pytest.importorskip("torch")
 
 ALL = sorted(cases())
 ALL_RECT = sorted({**cases(), **rect_cases()})
-WIDE_OK = [n for n in ALL_RECT if n != "tall"]   # DIA / BDIA reject taller-than-wide
+WIDE_OK = [n for n in ALL_RECT if n != "tall"]   # "tall" has entries below row aligned(width): DIA / BDIA reject it
 BLOCK = [(4, 4), (8, 2), (4, 1), (8, 8)]          # (bwidth, bheight)
 
 _HOST_DEFAULTS = {
@@ -189,6 +189,29 @@ def test_block_shape_unsupported(fmt, args):
 
 def test_tall_dia_rejected():
     assert check_pair("dia", coo_of("tall")) == _abi.ERR_ARG
+
+
+@pytest.mark.parametrize("fmt", ["dia", "bdia"])
+@pytest.mark.parametrize("h,w,top", [(300, 100, 128), (300, 100, 140), (129, 97, 97), (64, 30, 32), (500, 37, 64),
+                                     (500, 37, 65)])
+def test_tall_dia_with_entries_above_the_aligned_width(fmt, h, w, top):
+    """A taller-than-wide matrix (a 7-diagonal band in rows < top) converts
+    exactly as on the host (and as by the reference) while every entry sits
+    in a row below aligned(width, 32), and both reject it (CLSPMV_ERR_ARG)
+    when an entry sits at or past it."""
+    rng = np.random.default_rng(h * 7 + w)
+    r = np.repeat(np.arange(min(top, h)), 7)
+    c = r + np.tile(np.arange(-3, 4), min(top, h))
+    keep = (c >= 0) & (c < w)
+    r, c = list(r[keep]), list(c[keep])
+    if top - 1 >= w:                      # one entry in the rows below the square part, at row top - 1
+        r.append(top - 1)
+        c.append(0)
+    r, c = np.array(r), np.array(c)
+    coo = F.coo_matrix(h, w, r, c, rng.standard_normal(r.size).astype(np.float32))
+    aligned = (w + 31) // 32 * 32
+    st = check_pair(fmt, coo)
+    assert st == (_abi.ERR_ARG if r.max() >= aligned else _abi.OK), (st, r.max(), aligned)
 
 
 def test_empty_matrix():
