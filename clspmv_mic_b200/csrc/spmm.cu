@@ -235,6 +235,7 @@ struct Dense {
     float alpha, beta;
     const float* scale;   // per-row scale of packed values, or nullptr
     int lshift;           // log2 of lanes per row group
+    int x_form;           // block-row kernel: X rows through L1 (0), with an L2 evict-last hint (1), past L1 (2)
 };
 
 // Row-walk kernel: one group of 2^lshift lanes per row, grid-stride over rows.
@@ -252,6 +253,139 @@ __global__ void __launch_bounds__(kSpmmBlock) k_spmm_rows(M m, const T* __restri
         for_row(m, (int)r, [&](int col, size_t idx) { acc.fma(to_f(ld_val(vals + idx)), d.X + (size_t)col * d.ldx + c0); });
         const float a = d.scale ? d.alpha * d.scale[r] : d.alpha;
         acc.store(d.Y + (size_t)r * d.ldy + c0, a, d.beta);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Block walks: for_block(m, br, f) calls f(c4, base, s4, sh) for every stored
+// block of block row br. The block's first column is 4 * c4; the value of its
+// row h, column 4 * w4 + w sits at base + w4 * s4 + h * sh + w, so each
+// (w4, h) strip is 4 consecutive values. Same addressing as for_row.
+// ---------------------------------------------------------------------------
+template <class F>
+__device__ __forceinline__ void for_block(const clspmv_b4csr_f32& m, int br, F&& f)
+{
+    const size_t len = (size_t)m.b4csr_aligned_size, bh = m.b4csr_bheight;
+    const int i1 = __ldg(m.b4csr_row_ptr + br + 1);
+    for (int i = __ldg(m.b4csr_row_ptr + br); i < i1; i++) f(__ldg(m.b4csr_col_id + i), (size_t)i * 4, len * bh, len);
+}
+
+template <class F>
+__device__ __forceinline__ void for_block(const clspmv_b4ell_f32& m, int br, F&& f)
+{
+    const size_t len = (size_t)m.b4ell_height_aligned, f4 = (size_t)m.b4ell_float4_aligned;
+    const size_t bh = m.b4ell_bheight, bw4 = m.b4ell_bwidth / 4;
+    for (int j = 0; j < m.b4ell_block_num; j++)
+        f(__ldg(m.b4ell_col_id + (size_t)j * len + br), (size_t)j * f4 * bw4 * bh + (size_t)br * 4, f4 * bh, f4);
+}
+
+template <class F>
+__device__ __forceinline__ void for_block(const clspmv_sbell_f32& m, int br, F&& f)
+{
+    const size_t bh = m.sbell_bheight, bw4 = m.sbell_bwidth / 4, sh = m.sbell_slice_height;
+    const int sl = (int)(br / sh), s = br - sl * (int)sh;
+    const int start = __ldg(m.sbell_slice_ptr + sl);
+    const int width = (__ldg(m.sbell_slice_ptr + sl + 1) - start) / (int)sh;
+    const size_t base = (size_t)start * bw4 * 4 * bh + (size_t)s * 4;
+    for (int j = 0; j < width; j++)
+        f(__ldg(m.sbell_col_id + (size_t)start + s + (size_t)j * sh), base + (size_t)j * bw4 * bh * sh * 4, bh * sh * 4,
+          sh * 4);
+}
+
+// 4 consecutive values of a block strip. b4csr keeps a block row's blocks
+// side by side (block i at 4 * i in each (w4, h) plane), so a group's next
+// blocks share the line of this one: those loads allocate in L1 and carry no
+// evict-first hint, so that the line is still in L2 when L1 has lost it. In
+// b4ell and SBELL the neighbouring groups (block rows) read the rest of the
+// line in the same instruction, and the loads stream past L1.
+template <class M> struct StripsInL1 { static constexpr bool value = false; };
+__device__ __forceinline__ float4 ld_x4_na(const float* p)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+    return v;
+}
+template <> struct StripsInL1<clspmv_b4csr_f32> { static constexpr bool value = true; };
+
+__device__ __forceinline__ uint2 ld_l1_u2(const void* p) { return __ldg(reinterpret_cast<const uint2*>(p)); }
+template <bool L1> __device__ __forceinline__ float4 strip4(const float* p, uint64_t pol)
+{
+    return L1 ? __ldg(reinterpret_cast<const float4*>(p)) : ld_stream_f4(p, pol);
+}
+template <bool L1> __device__ __forceinline__ float4 strip4(const __nv_bfloat16* p, uint64_t pol)
+{
+    const uint2 u = L1 ? ld_l1_u2(p) : ld_stream_u2(p, pol);
+    return make_float4(bf16_lo(u.x), bf16_hi(u.x), bf16_lo(u.y), bf16_hi(u.y));
+}
+template <bool L1> __device__ __forceinline__ float4 strip4(const __half* p, uint64_t pol)
+{
+    const uint2 u = L1 ? ld_l1_u2(p) : ld_stream_u2(p, pol);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ float4 load_x(const float* p, int form, uint64_t pol)
+{
+    return form == 0 ? __ldg(reinterpret_cast<const float4*>(p)) : form == 1 ? ld_x4(p, pol) : ld_x4_na(p);
+}
+
+// Block-row kernel for the 4-wide block formats: one group of 2^lshift lanes
+// per BH-high block row, each lane holding its VEC columns of all BH rows of
+// Y. A block's 4 x VEC slice of X is loaded once and multiplies its BH rows
+// from registers (the row-walk kernel loads it once per row), and each (w4, h)
+// strip of values is one 4-value load. Every row accumulates in the same
+// order as the row walk (block, strip, column), so the two give the same bits.
+template <int BH, int BW4, int VEC, class T, class M>
+__global__ void __launch_bounds__(kSpmmBlock, BH >= 8 ? 1 : 4) k_spmm_blocks(M m, const T* __restrict__ vals, Dense d)
+{
+    const long long t = (long long)blockIdx.x * kSpmmBlock + threadIdx.x;
+    const int lane = (int)(t & ((1 << d.lshift) - 1));
+    const int c0 = lane * VEC;
+    if (c0 >= d.k) return;
+    const long long groups = ((long long)gridDim.x * kSpmmBlock) >> d.lshift;
+    const int height = m.matinfo.height, width = m.matinfo.width;
+    const long long nbr = ((long long)height + BH - 1) / BH;
+    const uint64_t pol = policy_evict_first(), xpol = policy_evict_last();
+    static_assert(VEC == 4, "128-bit X rows");
+    for (long long br = t >> d.lshift; br < nbr; br += groups) {
+        Acc<VEC> acc[BH];
+        for_block(m, (int)br, [&](int c4, size_t base, size_t s4, size_t sh) {
+#pragma unroll
+            for (int w4 = 0; w4 < BW4; w4++) {
+                float4 a[BH];
+#pragma unroll
+                for (int h = 0; h < BH; h++)
+                    a[h] = strip4<StripsInL1<M>::value>(vals + base + (size_t)w4 * s4 + (size_t)h * sh, pol);
+                const int col0 = (c4 + w4) * 4;
+                const int ncol = min(4, width - col0);   // the reference stops a block at the matrix width
+                float4 xv[4];
+                if (ncol == 4) {                         // the 4 X rows in flight together
+#pragma unroll
+                    for (int w = 0; w < 4; w++) xv[w] = load_x(d.X + (size_t)(col0 + w) * d.ldx + c0, d.x_form, xpol);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < 4; w++)
+                        xv[w] = w < ncol ? load_x(d.X + (size_t)(col0 + w) * d.ldx + c0, d.x_form, xpol) : Acc<VEC>::zero();
+                }
+#pragma unroll
+                for (int w = 0; w < 4; w++) {
+                    if (w >= ncol) break;
+#pragma unroll
+                    for (int h = 0; h < BH; h++) {
+                        const float av = w == 0 ? a[h].x : w == 1 ? a[h].y : w == 2 ? a[h].z : a[h].w;
+                        acc[h].fma_v(av, xv[w]);
+                    }
+                }
+            }
+        });
+#pragma unroll
+        for (int h = 0; h < BH; h++) {
+            const long long r = br * BH + h;
+            if (r >= height) break;
+            const float al = d.scale ? d.alpha * d.scale[r] : d.alpha;
+            acc[h].store(d.Y + (size_t)r * d.ldy + c0, al, d.beta);
+        }
     }
 }
 
@@ -744,6 +878,72 @@ int launch_rows(const M& m, const void* vals, Dense d, int vec, cudaStream_t st)
     return after_launch(1);
 }
 
+// CLSPMV_SPMM_BLOCK_ROWS=0 keeps the row walk for the block formats (measurements).
+bool block_rows_enabled()
+{
+    static const bool on = [] {
+        const char* e = getenv("CLSPMV_SPMM_BLOCK_ROWS");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
+inline int bheight_of(const clspmv_b4csr_f32& m) { return (int)m.b4csr_bheight; }
+inline int bheight_of(const clspmv_b4ell_f32& m) { return (int)m.b4ell_bheight; }
+inline int bheight_of(const clspmv_sbell_f32& m) { return (int)m.sbell_bheight; }
+inline int bwidth_of(const clspmv_b4csr_f32& m) { return (int)m.b4csr_bwidth; }
+inline int bwidth_of(const clspmv_b4ell_f32& m) { return (int)m.b4ell_bwidth; }
+inline int bwidth_of(const clspmv_sbell_f32& m) { return (int)m.sbell_bwidth; }
+// strides of for_block in values, which 4-value loads need to be multiples of 4
+inline bool strips_aligned(const clspmv_b4csr_f32& m) { return m.b4csr_aligned_size % 4 == 0; }
+inline bool strips_aligned(const clspmv_b4ell_f32& m) { return m.b4ell_float4_aligned % 4 == 0; }
+inline bool strips_aligned(const clspmv_sbell_f32&) { return true; }
+
+// CLSPMV_SPMM_X_FORM: how the block-row kernel reads X rows (Dense::x_form; measurements)
+int x_form()
+{
+    static const int f = [] {
+        const char* e = getenv("CLSPMV_SPMM_X_FORM");
+        return e ? atoi(e) : 0;
+    }();
+    return f;
+}
+
+template <int BH, int BW4, class T, class M>
+void launch_block_kernel(const M& m, const T* v, Dense d, cudaStream_t st)
+{
+    d.x_form = x_form();
+    const long long nbr = ((long long)m.matinfo.height + BH - 1) / BH;
+    k_spmm_blocks<BH, BW4, 4, T, M><<<grid_of(nbr << d.lshift), kSpmmBlock, 0, st>>>(m, v, d);
+}
+
+// Block formats with 128-bit X rows: the block-row kernel; otherwise (X rows
+// of single columns, or strips off a 4-value boundary) the row walk.
+template <class T, class M>
+int launch_blocks(const M& m, const void* vals, Dense d, int vec, cudaStream_t st)
+{
+    const T* v = static_cast<const T*>(vals);
+    const int bh = bheight_of(m), bw4 = bwidth_of(m) / 4;
+    if (vec != 4 || !block_rows_enabled() || !strips_aligned(m) || ((uintptr_t)v % (4 * sizeof(T))) != 0 ||
+        (bw4 != 1 && bw4 != 2))
+        return launch_rows<T>(m, vals, d, vec, st);
+    if (m.matinfo.height <= 0) return CLSPMV_OK;
+#define BLK(BH)                                                        \
+    case BH:                                                           \
+        if (bw4 == 1) launch_block_kernel<BH, 1, T>(m, v, d, st);      \
+        else launch_block_kernel<BH, 2, T>(m, v, d, st);               \
+        break;
+    switch (bh) {
+        BLK(1)
+        BLK(2)
+        BLK(4)
+        BLK(8)
+        default: return launch_rows<T>(m, vals, d, vec, st);
+    }
+#undef BLK
+    return after_launch(1);
+}
+
 // CLSPMV_SPMM_WARP_ROWS=0 keeps the nonzero-chunk kernel for long CSR rows (measurements).
 bool warp_rows_enabled()
 {
@@ -828,10 +1028,16 @@ int spmm_typed(int format, const void* dev, const void* vals, Dense d, int vec, 
         ROWS(CLSPMV_FORMAT_BDIA, clspmv_bdia_f32)
         ROWS(CLSPMV_FORMAT_ELL, clspmv_ell_f32)
         ROWS(CLSPMV_FORMAT_SELL, clspmv_sell_f32)
-        ROWS(CLSPMV_FORMAT_B4CSR, clspmv_b4csr_f32)
-        ROWS(CLSPMV_FORMAT_B4ELL, clspmv_b4ell_f32)
-        ROWS(CLSPMV_FORMAT_SBELL, clspmv_sbell_f32)
 #undef ROWS
+#define BLOCKS(FMT, TYPE)                                                            \
+    case FMT: {                                                                      \
+        const auto& m = *static_cast<const TYPE*>(dev);                              \
+        return launch_blocks<T>(m, vals ? vals : values_of(m), d, vec, st);          \
+    }
+        BLOCKS(CLSPMV_FORMAT_B4CSR, clspmv_b4csr_f32)
+        BLOCKS(CLSPMV_FORMAT_B4ELL, clspmv_b4ell_f32)
+        BLOCKS(CLSPMV_FORMAT_SBELL, clspmv_sbell_f32)
+#undef BLOCKS
     }
     return CLSPMV_ERR_ARG;
 }

@@ -215,3 +215,50 @@ def test_csr_long_rows_warp_kernel(k, value_type):
         ref, bound = spmm_reference(coo, X, Y0, alpha, beta)
         err = np.abs(Yd.cpu().numpy().astype(np.float64) - ref)
         assert np.all(err <= RTOL[value_type] * bound + 1e-6 * abs(beta) * np.abs(Y0) + 1e-30), (k, value_type, alpha, beta)
+
+
+_BLOCK_WALK_SCRIPT = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[2])
+from clspmv_mic_b200 import formats as F
+from tests.matrices import coo_of
+out = {}
+for name in ("blocks_odd", "blocks300", "ragged_tail"):
+    coo = coo_of(name)
+    m, n = coo.shape
+    for fmt in ("b4csr", "b4ell", "sbell"):
+        for bw, bh in [(4, 1), (4, 2), (4, 4), (4, 8), (8, 1), (8, 2), (8, 4), (8, 8)]:
+            dev = F.DeviceMatrix(getattr(F, "coo2" + fmt)(coo, bw, bh))
+            for k, vt in [(16, "f32"), (32, "f32"), (8, "bf16"), (128, "f16")]:
+                rng = np.random.default_rng(k + bw * 3 + bh)
+                X = torch.from_numpy(rng.uniform(-1, 1, (n, k)).astype(np.float32)).cuda()
+                Y = torch.from_numpy(rng.uniform(-1, 1, (m, k)).astype(np.float32)).cuda()
+                dev.spmm(X, Y, 0.75, -0.5, packed=None if vt == "f32" else dev.pack(vt))
+                out[f"{name}-{fmt}-{bw}x{bh}-{k}-{vt}"] = Y.cpu().numpy()
+np.savez(sys.argv[1], **out)
+"""
+
+
+def test_block_rows_kernel_matches_row_walk(tmp_path):
+    """The block-row SpMM kernel of the 4-wide block formats (X slice loaded
+    once per block, all rows of the block from registers) gives the same
+    bits as the row walk (CLSPMV_SPMM_BLOCK_ROWS=0) for all 8 block shapes of
+    b4csr / b4ell / SBELL, FP32 and 16-bit values, alpha and beta."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = str(Path(__file__).resolve().parents[1])
+    script = tmp_path / "walk.py"
+    script.write_text(_BLOCK_WALK_SCRIPT)
+    res = {}
+    for flag in ("1", "0"):
+        env = dict(os.environ, CLSPMV_SPMM_BLOCK_ROWS=flag)
+        out = tmp_path / f"y{flag}.npz"
+        subprocess.run([sys.executable, str(script), str(out), root], env=env, check=True, cwd=root, timeout=600)
+        res[flag] = np.load(out)
+    assert sorted(res["1"].files) == sorted(res["0"].files) and len(res["1"].files) == 3 * 3 * 8 * 4
+    for key in res["1"].files:
+        assert np.array_equal(res["1"][key].view(np.uint32), res["0"][key].view(np.uint32)), key
