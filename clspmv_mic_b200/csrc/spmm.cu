@@ -330,63 +330,70 @@ __device__ __forceinline__ float4 load_x(const float* p, int form, uint64_t pol)
     return form == 0 ? __ldg(reinterpret_cast<const float4*>(p)) : form == 1 ? ld_x4(p, pol) : ld_x4_na(p);
 }
 
+// One block row of the block-row kernel: the group's lane holds columns
+// c0 .. c0+3 of all BH rows of Y. A block's 4 x 4 slice of X is loaded once
+// (the 4 X rows in flight together) and multiplies its BH rows from registers
+// (the row walk loads it once per row), and each (w4, h) strip of values is
+// one 4-value load. Every row accumulates in the same order as the row walk
+// (block, strip, column), so the two give the same bits.
+template <int BH, int BW4, class T, class M>
+__device__ __forceinline__ void block_row(const M& m, const T* __restrict__ vals, int br, int c0, const float* __restrict__ X,
+                                          int ldx, float* __restrict__ Y, int ldy, float alpha, float beta,
+                                          const float* __restrict__ scale, int x_form)
+{
+    const int height = m.matinfo.height, width = m.matinfo.width;
+    const uint64_t pol = policy_evict_first(), xpol = policy_evict_last();
+    Acc<4> acc[BH];
+    for_block(m, br, [&](int c4, size_t base, size_t s4, size_t sh) {
+#pragma unroll
+        for (int w4 = 0; w4 < BW4; w4++) {
+            float4 a[BH];
+#pragma unroll
+            for (int h = 0; h < BH; h++)
+                a[h] = strip4<StripsInL1<M>::value>(vals + base + (size_t)w4 * s4 + (size_t)h * sh, pol);
+            const int col0 = (c4 + w4) * 4;
+            const int ncol = min(4, width - col0);   // the reference stops a block at the matrix width
+            float4 xv[4];
+            if (ncol == 4) {                         // the 4 X rows in flight together
+#pragma unroll
+                for (int w = 0; w < 4; w++) xv[w] = load_x(X + (size_t)(col0 + w) * ldx + c0, x_form, xpol);
+            } else {
+#pragma unroll
+                for (int w = 0; w < 4; w++)
+                    xv[w] = w < ncol ? load_x(X + (size_t)(col0 + w) * ldx + c0, x_form, xpol) : Acc<4>::zero();
+            }
+#pragma unroll
+            for (int w = 0; w < 4; w++) {
+                if (w >= ncol) break;
+#pragma unroll
+                for (int h = 0; h < BH; h++) {
+                    const float av = w == 0 ? a[h].x : w == 1 ? a[h].y : w == 2 ? a[h].z : a[h].w;
+                    acc[h].fma_v(av, xv[w]);
+                }
+            }
+        }
+    });
+#pragma unroll
+    for (int h = 0; h < BH; h++) {
+        const long long r = (long long)br * BH + h;
+        if (r >= height) break;
+        const float al = scale ? alpha * scale[r] : alpha;
+        acc[h].store(Y + (size_t)r * ldy + c0, al, beta);
+    }
+}
+
 // Block-row kernel for the 4-wide block formats: one group of 2^lshift lanes
-// per BH-high block row, each lane holding its VEC columns of all BH rows of
-// Y. A block's 4 x VEC slice of X is loaded once and multiplies its BH rows
-// from registers (the row-walk kernel loads it once per row), and each (w4, h)
-// strip of values is one 4-value load. Every row accumulates in the same
-// order as the row walk (block, strip, column), so the two give the same bits.
-template <int BH, int BW4, int VEC, class T, class M>
+// per BH-high block row (block_row), grid-stride over block rows.
+template <int BH, int BW4, class T, class M>
 __global__ void __launch_bounds__(kSpmmBlock, BH >= 8 ? 1 : 4) k_spmm_blocks(M m, const T* __restrict__ vals, Dense d)
 {
     const long long t = (long long)blockIdx.x * kSpmmBlock + threadIdx.x;
-    const int lane = (int)(t & ((1 << d.lshift) - 1));
-    const int c0 = lane * VEC;
+    const int c0 = (int)(t & ((1 << d.lshift) - 1)) * 4;
     if (c0 >= d.k) return;
     const long long groups = ((long long)gridDim.x * kSpmmBlock) >> d.lshift;
-    const int height = m.matinfo.height, width = m.matinfo.width;
-    const long long nbr = ((long long)height + BH - 1) / BH;
-    const uint64_t pol = policy_evict_first(), xpol = policy_evict_last();
-    static_assert(VEC == 4, "128-bit X rows");
-    for (long long br = t >> d.lshift; br < nbr; br += groups) {
-        Acc<VEC> acc[BH];
-        for_block(m, (int)br, [&](int c4, size_t base, size_t s4, size_t sh) {
-#pragma unroll
-            for (int w4 = 0; w4 < BW4; w4++) {
-                float4 a[BH];
-#pragma unroll
-                for (int h = 0; h < BH; h++)
-                    a[h] = strip4<StripsInL1<M>::value>(vals + base + (size_t)w4 * s4 + (size_t)h * sh, pol);
-                const int col0 = (c4 + w4) * 4;
-                const int ncol = min(4, width - col0);   // the reference stops a block at the matrix width
-                float4 xv[4];
-                if (ncol == 4) {                         // the 4 X rows in flight together
-#pragma unroll
-                    for (int w = 0; w < 4; w++) xv[w] = load_x(d.X + (size_t)(col0 + w) * d.ldx + c0, d.x_form, xpol);
-                } else {
-#pragma unroll
-                    for (int w = 0; w < 4; w++)
-                        xv[w] = w < ncol ? load_x(d.X + (size_t)(col0 + w) * d.ldx + c0, d.x_form, xpol) : Acc<VEC>::zero();
-                }
-#pragma unroll
-                for (int w = 0; w < 4; w++) {
-                    if (w >= ncol) break;
-#pragma unroll
-                    for (int h = 0; h < BH; h++) {
-                        const float av = w == 0 ? a[h].x : w == 1 ? a[h].y : w == 2 ? a[h].z : a[h].w;
-                        acc[h].fma_v(av, xv[w]);
-                    }
-                }
-            }
-        });
-#pragma unroll
-        for (int h = 0; h < BH; h++) {
-            const long long r = br * BH + h;
-            if (r >= height) break;
-            const float al = d.scale ? d.alpha * d.scale[r] : d.alpha;
-            acc[h].store(d.Y + (size_t)r * d.ldy + c0, al, d.beta);
-        }
-    }
+    const long long nbr = ((long long)m.matinfo.height + BH - 1) / BH;
+    for (long long br = t >> d.lshift; br < nbr; br += groups)
+        block_row<BH, BW4>(m, vals, (int)br, c0, d.X, d.ldx, d.Y, d.ldy, d.alpha, d.beta, d.scale, d.x_form);
 }
 
 // Nonzero-chunk kernel for CSR (row_ptr) and row-sorted COO (row_id). Y must
@@ -914,7 +921,7 @@ void launch_block_kernel(const M& m, const T* v, Dense d, cudaStream_t st)
 {
     d.x_form = x_form();
     const long long nbr = ((long long)m.matinfo.height + BH - 1) / BH;
-    k_spmm_blocks<BH, BW4, 4, T, M><<<grid_of(nbr << d.lshift), kSpmmBlock, 0, st>>>(m, v, d);
+    k_spmm_blocks<BH, BW4, T, M><<<grid_of(nbr << d.lshift), kSpmmBlock, 0, st>>>(m, v, d);
 }
 
 // Block formats with 128-bit X rows: the block-row kernel; otherwise (X rows
@@ -1129,6 +1136,7 @@ constexpr int kBatchLongRow = 256;
 
 struct BatchJob {
     int format, value_type, k, lshift, vec, rows;
+    int bh;                    // 4: a 4x4-block job, one lane group per block row (block_row); 0: rows
     int chunk, nnz;            // CSR accumulating into Y (beta 1): nonzeros per lane group, else 0 (row mode)
     long long task_begin;
     int ldx, ldy;
@@ -1171,6 +1179,17 @@ __device__ __forceinline__ void batch_dispatch(const BatchJob& J, int r, int c0)
         case CLSPMV_FORMAT_B4CSR: batch_row<VEC, T>(J.m.b4csr, J, r, c0); break;
         case CLSPMV_FORMAT_B4ELL: batch_row<VEC, T>(J.m.b4ell, J, r, c0); break;
         case CLSPMV_FORMAT_SBELL: batch_row<VEC, T>(J.m.sbell, J, r, c0); break;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void batch_blocks(const BatchJob& J, int br, int c0)
+{
+    const T* v = static_cast<const T*>(J.values);
+    switch (J.format) {
+        case CLSPMV_FORMAT_B4CSR: block_row<4, 1>(J.m.b4csr, v, br, c0, J.X, J.ldx, J.Y, J.ldy, J.alpha, J.beta, J.scale, 0); break;
+        case CLSPMV_FORMAT_B4ELL: block_row<4, 1>(J.m.b4ell, v, br, c0, J.X, J.ldx, J.Y, J.ldy, J.alpha, J.beta, J.scale, 0); break;
+        case CLSPMV_FORMAT_SBELL: block_row<4, 1>(J.m.sbell, v, br, c0, J.X, J.ldx, J.Y, J.ldy, J.alpha, J.beta, J.scale, 0); break;
     }
 }
 
@@ -1256,20 +1275,56 @@ __global__ void __launch_bounds__(kSpmmBlock) k_batch(const BatchJob* __restrict
     }
 }
 
-int batch_grid()
+// The 4x4-block jobs of a batch (bh = 4) in their own persistent launch: warp
+// tasks of 32 / G block rows, one lane group per block row (block_row). Kept
+// apart from k_batch, whose other jobs would otherwise run at this path's
+// register count.
+__global__ void __launch_bounds__(kSpmmBlock, 3) k_batch_blocks(const BatchJob* __restrict__ jobs, int njobs, long long tasks)
 {
-    static int grid = 0;
-    if (!grid) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * kSpmmBlock) >> 5;
+    for (long long t = ((long long)blockIdx.x * kSpmmBlock + threadIdx.x) >> 5; t < tasks; t += nwarps) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].task_begin <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchJob& J = jobs[lo];
+        const long long br = (t - J.task_begin) * (32 >> J.lshift) + (lane >> J.lshift);
+        const int c0 = (lane & ((1 << J.lshift) - 1)) * 4;
+        if (br >= (J.rows + 3) / 4 || c0 >= J.k) continue;
+        if (J.value_type == CLSPMV_VALUES_F32) batch_blocks<float>(J, (int)br, c0);
+        else if (J.value_type == CLSPMV_VALUES_BF16) batch_blocks<__nv_bfloat16>(J, (int)br, c0);
+        else batch_blocks<__half>(J, (int)br, c0);
+    }
+}
+
+int persistent_grid(const void* kernel, int* cache)
+{
+    if (!*cache) {
         int dev = 0, nsm = 148, per = 1;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch, kSpmmBlock, 0) != cudaSuccess || per < 1) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kSpmmBlock, 0) != cudaSuccess || per < 1) {
             cudaGetLastError();
             per = 1;
         }
-        grid = nsm * per;
+        *cache = nsm * per;
     }
-    return grid;
+    return *cache;
+}
+
+int batch_blocks_grid()
+{
+    static int grid = 0;
+    return persistent_grid((const void*)k_batch_blocks, &grid);
+}
+
+int batch_grid()
+{
+    static int grid = 0;
+    return persistent_grid((const void*)k_batch, &grid);
 }
 
 // Fills one device job from a caller's job description.
@@ -1307,6 +1362,17 @@ int make_job(const clspmv_spmm_job& in, BatchJob& out)
     }
     if (in.value_type != CLSPMV_VALUES_F32) out.values = in.values;
     if (out.format == CLSPMV_FORMAT_CSR && !out.m.csr.csr_row_ptr) return CLSPMV_ERR_ARG;
+    // 4x4 blocks with 128-bit X rows: one lane group per block row, as clspmv_spmm does
+    const size_t vsize = in.value_type == CLSPMV_VALUES_F32 ? 4 : 2;
+    if (out.vec == 4 && block_rows_enabled() && ((uintptr_t)out.values % (4 * vsize)) == 0) {
+        bool four = false;
+        switch (out.format) {
+            case CLSPMV_FORMAT_B4CSR: four = bheight_of(out.m.b4csr) == 4 && bwidth_of(out.m.b4csr) == 4 && strips_aligned(out.m.b4csr); break;
+            case CLSPMV_FORMAT_B4ELL: four = bheight_of(out.m.b4ell) == 4 && bwidth_of(out.m.b4ell) == 4 && strips_aligned(out.m.b4ell); break;
+            case CLSPMV_FORMAT_SBELL: four = bheight_of(out.m.sbell) == 4 && bwidth_of(out.m.sbell) == 4; break;
+        }
+        if (four) out.bh = 4;
+    }
     // CSR adding into Y with long rows (mean >= kBatchLongRow entries): equal chunks of
     // nonzeros, so long rows are shared between groups (shorter rows: one group per row
     // is faster, measured on B200)
@@ -1323,7 +1389,9 @@ int make_job(const clspmv_spmm_job& in, BatchJob& out)
 struct clspmv_batch {
     int capacity = 0;
     int njobs = 0;
+    int nrow_jobs = 0;            // jobs [0, nrow_jobs) run in k_batch, the rest (4x4 blocks) in k_batch_blocks
     long long tasks = 0;
+    long long block_tasks = 0;
     BatchJob* host = nullptr;     // pinned staging of the job table
     BatchJob* dev = nullptr;
     cudaEvent_t copied = nullptr; // the last table upload has left `host`
@@ -1453,21 +1521,35 @@ int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, cl
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     int rc = cuda_status(cudaEventSynchronize(b->copied));   // staging free again
     if (rc) return rc;
-    long long tasks = 0;
+    // row jobs first (k_batch), then the 4x4-block jobs (k_batch_blocks), each
+    // with its own task numbering; a job's place in the table changes nothing
+    // in its Y
+    b->njobs = 0;
+    b->tasks = b->block_tasks = 0;
+    b->nrow_jobs = 0;
+    int nblock = 0;
     for (int i = 0; i < njobs; i++) {
-        BatchJob& J = b->host[i];
+        BatchJob J;
         if ((rc = make_job(jobs[i], J))) {
             if (bad_job) *bad_job = i;
-            b->njobs = 0;
-            b->tasks = 0;
             return rc;
         }
-        J.task_begin = tasks;
-        const long long units = J.chunk > 0 ? ((long long)J.nnz + J.chunk - 1) / J.chunk : J.rows;
-        tasks += (units + (32 >> J.lshift) - 1) / (32 >> J.lshift);
+        if (J.bh) b->host[njobs - 1 - nblock++] = J;   // filled from the end, reversed below
+        else b->host[b->nrow_jobs++] = J;
+    }
+    std::reverse(b->host + b->nrow_jobs, b->host + njobs);
+    long long tasks = 0, block_tasks = 0;
+    for (int i = 0; i < njobs; i++) {
+        BatchJob& J = b->host[i];
+        long long& t = J.bh ? block_tasks : tasks;
+        J.task_begin = t;
+        const long long units = J.chunk > 0 ? ((long long)J.nnz + J.chunk - 1) / J.chunk
+                                : J.bh ? ((long long)J.rows + J.bh - 1) / J.bh : J.rows;
+        t += (units + (32 >> J.lshift) - 1) / (32 >> J.lshift);
     }
     b->njobs = njobs;
     b->tasks = tasks;
+    b->block_tasks = block_tasks;
     if (njobs == 0) return CLSPMV_OK;
     rc = cuda_status(cudaMemcpyAsync(b->dev, b->host, sizeof(BatchJob) * njobs, cudaMemcpyHostToDevice, st));
     if (!rc) rc = cuda_status(cudaEventRecord(b->copied, st));
@@ -1477,11 +1559,19 @@ int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, cl
 int clspmv_batch_run(clspmv_batch* b, clspmv_stream_t stream)
 {
     if (!b) return CLSPMV_ERR_ARG;
-    if (b->tasks == 0) return CLSPMV_OK;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const long long grid = std::min<long long>(batch_grid(), (b->tasks + 7) / 8);
-    k_batch<<<(int)grid, kSpmmBlock, 0, st>>>(b->dev, b->njobs, b->tasks);
-    return after_launch(1);
+    int n = 0;
+    if (b->tasks > 0) {
+        const long long grid = std::min<long long>(batch_grid(), (b->tasks + 7) / 8);
+        k_batch<<<(int)grid, kSpmmBlock, 0, st>>>(b->dev, b->nrow_jobs, b->tasks);
+        n++;
+    }
+    if (b->block_tasks > 0) {
+        const long long grid = std::min<long long>(batch_blocks_grid(), (b->block_tasks + 7) / 8);
+        k_batch_blocks<<<(int)grid, kSpmmBlock, 0, st>>>(b->dev + b->nrow_jobs, b->njobs - b->nrow_jobs, b->block_tasks);
+        n++;
+    }
+    return n ? after_launch(n) : CLSPMV_OK;
 }
 
 int clspmv_batch_free(clspmv_batch* b)

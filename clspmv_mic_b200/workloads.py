@@ -17,6 +17,7 @@ import numpy as np
 
 from .batch import Batch, Job
 from .formats import DeviceMatrix
+from . import formats as F
 from . import synth
 
 VALUE_BYTES = {"f32": 4, "bf16": 2, "f16": 2}
@@ -132,7 +133,6 @@ def spmm_tc_sweep(m, A64, ks=(16, 32, 64), reps: int = 10, hbm_gbs=None):
     lane-group kernel, per k: time, GFLOP/s, GB/s over matrix bytes +
     k (4n + 4m), error against FP64."""
     import torch
-    from . import formats as F
     out = {}
     rows, cols = m.shape
     nnz = int(m.nnz)
@@ -288,6 +288,9 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
                 b.set(jobs, s)
                 for _ in range(3):
                     b.run(s)
+                n0 = F.launch_count()
+                b.run(s)
+                launches = F.launch_count() - n0     # 1, or 2 with 4x4-block jobs (their own launch)
             torch.cuda.current_stream().wait_stream(s)
             torch.cuda.synchronize()
             g = torch.cuda.CUDAGraph()
@@ -320,7 +323,7 @@ def batched(mats, ks=(1, 4, 16, 32), value_types=("f32", "bf16", "f16"), reps: i
             b.close()
             out[f"k{k}/{vt}"] = dict(ms=round(t_batch, 4), gflops=round(2.0 * nnz_total * k / (t_batch * 1e-3) / 1e9, 1),
                                      plain_ms=round(t_seq, 4), speedup=round(t_seq / t_batch, 2), err_fp64=err,
-                                     launches=1)
+                                     launches=launches)
         del Xs, Ys
     return out
 

@@ -565,12 +565,14 @@ typedef struct {
 } clspmv_spmm_job;
 
 /* A batch runs many jobs (different matrices, formats, value types and k)
- * in ONE persistent kernel launch: the rows of all jobs are cut into warp
- * tasks that every warp of a device-filling grid strides through. A CSR job
- * with beta == 1 (Y += alpha * A * X) whose rows hold 256 entries or more on
- * average is cut by nonzeros instead of rows, so very long rows do not
- * serialise one warp; for such matrices prefer beta == 1 (zero Y first for a
- * plain product). */
+ * in one persistent kernel launch: the rows of all jobs are cut into warp
+ * tasks that every warp of a device-filling grid strides through. Jobs on
+ * 4x4 blocks (b4csr, b4ell, SBELL) with 16-byte X / Y rows run in a second
+ * persistent launch, one lane group per block row, as clspmv_spmm runs them.
+ * A CSR job with beta == 1 (Y += alpha * A * X) whose rows hold 256 entries
+ * or more on average is cut by nonzeros instead of rows, so very long rows
+ * do not serialise one warp; for such matrices prefer beta == 1 (zero Y
+ * first for a plain product). */
 typedef struct clspmv_batch clspmv_batch;
 
 /* Allocates the device job table for up to max_jobs jobs (and a pinned
@@ -582,9 +584,9 @@ int clspmv_batch_create(int max_jobs, clspmv_batch** out);
  * not NULL, its index; the batch is then empty. Waits only for this batch's
  * previous upload to leave the staging buffer. */
 int clspmv_batch_set(clspmv_batch* b, const clspmv_spmm_job* jobs, int njobs, clspmv_stream_t stream, int* bad_job);
-/* Runs the jobs last set: one kernel launch on `stream`, no allocation and no
- * host synchronisation, so it can be captured in a CUDA graph. Jobs must
- * not write overlapping Y. */
+/* Runs the jobs last set: one kernel launch on `stream` (two when 4x4-block
+ * jobs are among them), no allocation and no host synchronisation, so it can
+ * be captured in a CUDA graph. Jobs must not write overlapping Y. */
 int clspmv_batch_run(clspmv_batch* b, clspmv_stream_t stream);
 int clspmv_batch_free(clspmv_batch* b);
 

@@ -93,6 +93,43 @@ def test_batch_matches_alone(graph):
     b.close()
 
 
+def test_batch_block_jobs_same_bits_as_alone():
+    """4x4-block jobs with 128-bit X rows run in the batch's block-row launch
+    (k_batch_blocks), the others in the row launch: with the two kinds
+    interleaved in the caller's list, every block job's Y equals the same
+    product run alone (the same block-row code) bit for bit, and every job
+    meets the oracle's per-row bound."""
+    import torch
+    rng = np.random.default_rng(11)
+    specs = []
+    for name in ("blocks300", "blocks_odd", "ragged_tail"):
+        for fmt in ("b4csr", "b4ell", "sbell"):
+            specs.append((name, fmt, (4, 4)))
+        specs.append((name, "csr", ()))
+    jobs, alone = [], []
+    for i, (name, fmt, args) in enumerate(specs):
+        dev = _device(name, fmt, args)
+        vt = ["f32", "bf16"][i % 2]
+        packed = None if vt == "f32" else dev.pack(vt)
+        k = [4, 16, 32, 8][i % 4]
+        X = torch.from_numpy(rng.uniform(-1, 1, (dev.shape[1], k)).astype(np.float32)).cuda()
+        Y = torch.full((dev.shape[0], k), float("nan"), device="cuda")
+        jobs.append(Job(dev, X, Y, alpha=0.5, beta=0.0, packed=packed))
+        alone.append(_alone(dev, X, 0.5, packed))
+    b = Batch(len(jobs))
+    b.set(jobs)
+    b.run()
+    torch.cuda.synchronize()
+    for i, (j, a, (name, fmt, _)) in enumerate(zip(jobs, alone, specs)):
+        got = j.Y.cpu().numpy()
+        vt = ["f32", "bf16"][i % 2]
+        cref = columns_reference(coo_of(name), j.X.cpu().numpy(), 0.5)
+        assert_columns_close(got, cref, vt, f"batch {name} {fmt} {vt}")
+        if fmt != "csr":
+            assert np.array_equal(got.view(np.uint32), a.cpu().numpy().view(np.uint32)), (name, fmt, vt)
+    b.close()
+
+
 def test_batch_rejects():
     import torch
     coo = coo_of("laplace16")
