@@ -268,7 +268,7 @@ def _declare(lib):
         sigs[f"clspmv_{fmt}2coo_f32"] = (I32, [S[fmt], S["coo"]])
     for fmt in FORMATS:
         sigs[f"clspmv_free_{fmt}_f32"] = (None, [S[fmt]])
-    for fmt in ("coo", "csr", "dia", "bdia", "ell", "sell", "b4csr", "b4ell", "sbell"):
+    for fmt in ("coo", "csr", "dia", "bdia", "ell", "sell", "bcsr", "bell", "b4csr", "b4ell", "sbell"):
         sigs[f"clspmv_upload_{fmt}_f32"] = (I32, [S[fmt], S[fmt]])
         sigs[f"clspmv_device_free_{fmt}_f32"] = (I32, [S[fmt]])
     sigs.update({
@@ -279,6 +279,8 @@ def _declare(lib):
         "clspmv_device_coo2ell_f32": (I32, [S["coo"], S["ell"], I32, I32, VP]),
         "clspmv_device_coo2sell_f32": (I32, [S["coo"], S["sell"], U32, VP]),
         "clspmv_device_coo2b4csr_f32": (I32, [S["coo"], S["b4csr"], U32, U32, I32, VP]),
+        "clspmv_device_coo2bcsr_f32": (I32, [S["coo"], S["bcsr"], U32, U32, I32, VP]),
+        "clspmv_device_coo2bell_f32": (I32, [S["coo"], S["bell"], U32, U32, I32, I32, VP]),
         "clspmv_device_coo2b4ell_f32": (I32, [S["coo"], S["b4ell"], U32, U32, I32, I32, VP]),
         "clspmv_device_coo2sbell_f32": (I32, [S["coo"], S["sbell"], U32, U32, U32, VP]),
     })

@@ -330,9 +330,10 @@ __global__ void k_block_list(const unsigned long long* __restrict__ keys, const 
     }
 }
 
-__global__ void k_b4_colid(const int* __restrict__ bcol, long long nb, int bw, int* out)
+// col_id of block b: its first column / unit (4 for b4csr, 1 for bcsr)
+__global__ void k_b4_colid(const int* __restrict__ bcol, long long nb, int bw, int unit, int* out)
 {
-    GRID_STRIDE(b, nb) out[b] = bcol[b] * bw / 4;
+    GRID_STRIDE(b, nb) out[b] = bcol[b] * bw / unit;
 }
 
 // Block formats: where an entry of block b lands. inner row hh, column
@@ -349,6 +350,22 @@ struct B4ellPlace {   // data[j*colsz + hh*f4 + w4*w4sz + r*4 + w] (include/matr
     __device__ long long operator()(int r, int j, long long, int hh, int w4, int w) const
     {
         return j * colsz + hh * f4 + w4 * w4sz + (long long)r * 4 + w;
+    }
+};
+struct BcsrPlace {    // data[k*len + b], k = inner row * bw + inner column (include/matrix_storage.h:1728)
+    long long len;
+    int bw;
+    __device__ long long operator()(int, int, long long b, int hh, int w4, int w) const
+    {
+        return ((long long)hh * bw + w4 * 4 + w) * len + b;
+    }
+};
+struct BellPlace {    // data[r + k*len + j*colsz] (include/matrix_storage.h:1992)
+    long long len, colsz;
+    int bw;
+    __device__ long long operator()(int r, int j, long long, int hh, int w4, int w) const
+    {
+        return (long long)r + ((long long)hh * bw + w4 * 4 + w) * len + j * colsz;
     }
 };
 struct SbellPlace {   // include/matrix_storage.h:2387
@@ -383,9 +400,10 @@ __global__ void k_block_scatter(const int* __restrict__ idx, const int* __restri
     }
 }
 
-// b4ell col ids, slot (j, r): block j of block row r in float4 units, else the
+// b4ell / bell col ids, slot (j, r): the first column of block j of block row
+// r, over unit (4: float4 units for b4ell, 1: columns for bell), else the
 // row's last (0 for an empty or missing row).
-__global__ void k_b4ell_cols(const int* __restrict__ brp, const int* __restrict__ bcol, int nbr, int bw,
+__global__ void k_b4ell_cols(const int* __restrict__ brp, const int* __restrict__ bcol, int nbr, int bw, int unit,
                              long long len, long long total, int* out)
 {
     GRID_STRIDE(t, total)
@@ -394,8 +412,8 @@ __global__ void k_b4ell_cols(const int* __restrict__ brp, const int* __restrict_
         int c = 0;
         if (r < nbr) {
             const int a = brp[r], e = brp[r + 1];
-            if (j < e - a) c = bcol[a + j] * bw / 4;
-            else if (e > a) c = bcol[e - 1] * bw / 4;
+            if (j < e - a) c = bcol[a + j] * bw / unit;
+            else if (e > a) c = bcol[e - 1] * bw / unit;
         }
         out[t] = c;
     }
@@ -913,7 +931,7 @@ int clspmv_device_coo2b4csr_f32(const clspmv_coo_f32* src, clspmv_b4csr_f32* dst
         return rc;
     if ((rc = cuda_status(cudaMemsetAsync(data, 0, sizeof(float) * ndata, st)))) return rc;
     if (B.nb > 0) {
-        k_b4_colid<<<grid_for(B.nb), kT, 0, st>>>(B.bcol, B.nb, bw, colid);
+        k_b4_colid<<<grid_for(B.nb), kT, 0, st>>>(B.bcol, B.nb, bw, 4, colid);
         if ((rc = launched(st))) return rc;
     }
     if ((rc = scatter_blocks(c, B, bw, bh, B4csrPlace{len, len * bh}, data, st))) return rc;
@@ -925,6 +943,95 @@ int clspmv_device_coo2b4csr_f32(const clspmv_coo_f32* src, clspmv_b4csr_f32* dst
     dst->b4csr_row_ptr = rp;
     dst->b4csr_col_id = colid;
     dst->b4csr_data = data;
+    return CLSPMV_OK;
+}
+
+int clspmv_device_coo2bcsr_f32(const clspmv_coo_f32* src, clspmv_bcsr_f32* dst, unsigned int bwidth,
+                               unsigned int bheight, int alignment, clspmv_stream_t stream)
+{
+    if (!coo_args_ok(src) || !dst || bwidth == 0 || bheight == 0 || bwidth > (unsigned)INT_MAX ||
+        bheight > (unsigned)INT_MAX || alignment <= 0)
+        return CLSPMV_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const Coo c = view(src);
+    Allocs S, O;
+    int rc = sorted_front(c, st, S, true);
+    if (rc) return rc;
+    const int bw = (int)bwidth, bh = (int)bheight;
+    const size_t bs = (size_t)bw * bh;
+    dst->matinfo = src->matinfo;
+    dst->bcsr_bwidth = bwidth;
+    dst->bcsr_bheight = bheight;
+    Blocks B;
+    if ((rc = make_blocks(c, bw, bh, st, S, B))) return rc;
+    const long long len = aligned_len(B.nb, alignment);
+    const size_t ndata = (size_t)len * bs;
+    int* rp = O.get<int>((size_t)B.nbr + 1);
+    int* colid = O.get<int>((size_t)B.nb);
+    float* data = O.get<float>(ndata);
+    if (O.rc) return O.rc;
+    if ((rc = cuda_status(cudaMemcpyAsync(rp, B.brp, sizeof(int) * ((size_t)B.nbr + 1), cudaMemcpyDeviceToDevice, st))))
+        return rc;
+    if (ndata && (rc = cuda_status(cudaMemsetAsync(data, 0, sizeof(float) * ndata, st)))) return rc;
+    if (B.nb > 0) {
+        k_b4_colid<<<grid_for(B.nb), kT, 0, st>>>(B.bcol, B.nb, bw, 1, colid);
+        if ((rc = launched(st))) return rc;
+    }
+    if ((rc = scatter_blocks(c, B, bw, bh, BcsrPlace{len, bw}, data, st))) return rc;
+    if ((rc = finish(st))) return rc;
+    O.keep = true;
+    dst->bcsr_row_num = B.nbr;
+    dst->bcsr_aligned_size = (int)len;
+    dst->bcsr_block_num = (int)B.nb;
+    dst->bcsr_row_ptr = rp;
+    dst->bcsr_col_id = colid;
+    dst->bcsr_data = data;
+    return CLSPMV_OK;
+}
+
+int clspmv_device_coo2bell_f32(const clspmv_coo_f32* src, clspmv_bell_f32* dst, unsigned int bwidth,
+                               unsigned int bheight, int alignment, int ellnum, clspmv_stream_t stream)
+{
+    if (!coo_args_ok(src) || !dst || bwidth == 0 || bheight == 0 || bwidth > (unsigned)INT_MAX ||
+        bheight > (unsigned)INT_MAX || alignment <= 0 || ellnum < 0)
+        return CLSPMV_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const Coo c = view(src);
+    Allocs S, O;
+    int rc = sorted_front(c, st, S, true);
+    if (rc) return rc;
+    const int bw = (int)bwidth, bh = (int)bheight;
+    const size_t bs = (size_t)bw * bh;
+    dst->matinfo = src->matinfo;
+    dst->bell_bwidth = bwidth;
+    dst->bell_bheight = bheight;
+    dst->bell_float4_aligned = 0;
+    dst->bell_col_id = nullptr;
+    dst->bell_data = nullptr;
+    Blocks B;
+    if ((rc = make_blocks(c, bw, bh, st, S, B))) return rc;
+    int maxw = 0;
+    if ((rc = max_len(B.brp, B.nbr, st, S, &maxw))) return rc;
+    const int num = ellnum == 0 ? maxw : ellnum;
+    const long long len = aligned_len(B.nbr, alignment);
+    dst->bell_block_num = num;
+    dst->bell_row_num = B.nbr;
+    dst->bell_height_aligned = (int)len;
+    if (maxw > num) return CLSPMV_ERR_ARG;   // a block row longer than ellnum (include/matrix_storage.h:1975)
+    const size_t ncol = (size_t)len * num, colsz = (size_t)len * bs, ndata = colsz * num;
+    int* col = O.get<int>(ncol);
+    float* data = O.get<float>(ndata);
+    if (O.rc) return O.rc;
+    if (ndata && (rc = cuda_status(cudaMemsetAsync(data, 0, sizeof(float) * ndata, st)))) return rc;
+    if (ncol > 0) {
+        k_b4ell_cols<<<grid_for((long long)ncol), kT, 0, st>>>(B.brp, B.bcol, B.nbr, bw, 1, len, (long long)ncol, col);
+        if ((rc = launched(st))) return rc;
+    }
+    if ((rc = scatter_blocks(c, B, bw, bh, BellPlace{len, (long long)colsz, bw}, data, st))) return rc;
+    if ((rc = finish(st))) return rc;
+    O.keep = true;
+    dst->bell_col_id = col;
+    dst->bell_data = data;
     return CLSPMV_OK;
 }
 
@@ -958,7 +1065,7 @@ int clspmv_device_coo2b4ell_f32(const clspmv_coo_f32* src, clspmv_b4ell_f32* dst
     if (O.rc) return O.rc;
     if ((rc = cuda_status(cudaMemsetAsync(data, 0, sizeof(float) * ndata, st)))) return rc;
     if (ncol > 0) {
-        k_b4ell_cols<<<grid_for((long long)ncol), kT, 0, st>>>(B.brp, B.bcol, B.nbr, bw, len, (long long)ncol, col);
+        k_b4ell_cols<<<grid_for((long long)ncol), kT, 0, st>>>(B.brp, B.bcol, B.nbr, bw, 4, len, (long long)ncol, col);
         if ((rc = launched(st))) return rc;
     }
     if ((rc = scatter_blocks(c, B, bw, bh, B4ellPlace{f4, f4 * w4n * bh, f4 * bh}, data, st))) return rc;

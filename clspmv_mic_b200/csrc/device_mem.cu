@@ -143,6 +143,28 @@ int clspmv_upload_b4csr_f32(const clspmv_b4csr_f32* h, clspmv_b4csr_f32* d)
     return u.finish();
 }
 
+int clspmv_upload_bcsr_f32(const clspmv_bcsr_f32* h, clspmv_bcsr_f32* d)
+{
+    if (!h || !d || h->bcsr_row_num < 0 || h->bcsr_block_num < 0 || h->bcsr_aligned_size < 0) return CLSPMV_ERR_ARG;
+    *d = *h;
+    Uploader u;
+    u.add(&d->bcsr_row_ptr, h->bcsr_row_ptr, (size_t)h->bcsr_row_num + 1);
+    u.add(&d->bcsr_col_id, h->bcsr_col_id, (size_t)h->bcsr_block_num);
+    u.add(&d->bcsr_data, h->bcsr_data, (size_t)h->bcsr_aligned_size * h->bcsr_bwidth * h->bcsr_bheight);
+    return u.finish();
+}
+
+int clspmv_upload_bell_f32(const clspmv_bell_f32* h, clspmv_bell_f32* d)
+{
+    if (!h || !d || h->bell_block_num < 0 || h->bell_height_aligned < 0) return CLSPMV_ERR_ARG;
+    *d = *h;
+    const size_t ncol = (size_t)h->bell_height_aligned * h->bell_block_num;
+    Uploader u;
+    u.add(&d->bell_col_id, h->bell_col_id, ncol);
+    u.add(&d->bell_data, h->bell_data, ncol * h->bell_bwidth * h->bell_bheight);
+    return u.finish();
+}
+
 int clspmv_upload_b4ell_f32(const clspmv_b4ell_f32* h, clspmv_b4ell_f32* d)
 {
     if (!h || !d || h->b4ell_block_num < 0 || h->b4ell_height_aligned < 0) return CLSPMV_ERR_ARG;
@@ -174,6 +196,8 @@ int clspmv_device_free_bdia_f32(clspmv_bdia_f32* d) { if (!d) return CLSPMV_ERR_
 int clspmv_device_free_ell_f32(clspmv_ell_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->ell_col_id); release(d->ell_data); return CLSPMV_OK; }
 int clspmv_device_free_sell_f32(clspmv_sell_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->sell_slice_ptr); release(d->sell_col_id); release(d->sell_data); return CLSPMV_OK; }
 int clspmv_device_free_b4csr_f32(clspmv_b4csr_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->b4csr_row_ptr); release(d->b4csr_col_id); release(d->b4csr_data); return CLSPMV_OK; }
+int clspmv_device_free_bcsr_f32(clspmv_bcsr_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->bcsr_row_ptr); release(d->bcsr_col_id); release(d->bcsr_data); return CLSPMV_OK; }
+int clspmv_device_free_bell_f32(clspmv_bell_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->bell_col_id); release(d->bell_data); return CLSPMV_OK; }
 int clspmv_device_free_b4ell_f32(clspmv_b4ell_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->b4ell_col_id); release(d->b4ell_data); return CLSPMV_OK; }
 int clspmv_device_free_sbell_f32(clspmv_sbell_f32* d) { if (!d) return CLSPMV_ERR_ARG; release(d->sbell_slice_ptr); release(d->sbell_col_id); release(d->sbell_data); return CLSPMV_OK; }
 

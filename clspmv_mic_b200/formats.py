@@ -227,8 +227,6 @@ class DeviceMatrix:
 
     def __init__(self, host: HostMatrix, device="cuda"):
         import torch
-        if host.fmt in ("bcsr", "bell"):
-            raise ValueError(f"{host.fmt} is a host-only format; use b4csr / b4ell on the device")
         self.fmt = host.fmt
         self.struct = type(host.struct).from_buffer_copy(host.struct)
         self.tensors = {}
@@ -331,6 +329,7 @@ class DeviceMatrix:
         column-major reads."""
         L = lib()
         s = _stream_handle(stream)
+        _computable(self.fmt)
         if packed is not None:
             if self.fmt == "csr" and variant == "chunk" and not ((self.struct.csr_col_id or 0) % 16
                                                                  or packed.values.data_ptr() % 8):
@@ -392,6 +391,14 @@ class DeviceMatrix:
         device_spmm(self, X, Y, alpha, beta, packed, stream)
 
 
+def _computable(fmt: str) -> None:
+    """The generic BCSR / BELL (any block shape) are storage formats: only
+    the reference's serial bcsr_spmv / bell_spmv read them, and no GPU kernel
+    does (the device kernels take b4csr / b4ell / SBELL)."""
+    if fmt in ("bcsr", "bell"):
+        raise ValueError(f"no GPU kernel reads the generic {fmt}; convert to b4{fmt[1:]} for SpMV")
+
+
 class _DeviceArrays:
     """Arrays a device converter cudaMalloc'ed, released with
     clspmv_device_free_<fmt>_f32 when the last tensor viewing them is gone."""
@@ -423,6 +430,8 @@ _DEVICE_CONVERT = {
     "bdia": ("clspmv_device_coo2bdia_f32", 0, (GPU_ALIGNMENT,)),
     "ell": ("clspmv_device_coo2ell_f32", 0, (GPU_ALIGNMENT, 0)),
     "sell": ("clspmv_device_coo2sell_f32", 0, (WARPSIZE,)),
+    "bcsr": ("clspmv_device_coo2bcsr_f32", 2, (GPU_ALIGNMENT,)),
+    "bell": ("clspmv_device_coo2bell_f32", 2, (GPU_ALIGNMENT, 0)),
     "b4csr": ("clspmv_device_coo2b4csr_f32", 2, (GPU_ALIGNMENT,)),
     "b4ell": ("clspmv_device_coo2b4ell_f32", 2, (GPU_ALIGNMENT, 0)),
     "sbell": ("clspmv_device_coo2sbell_f32", 2, (WARPSIZE,)),

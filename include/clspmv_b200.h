@@ -264,6 +264,8 @@ int clspmv_upload_bdia_f32(const clspmv_bdia_f32* host, clspmv_bdia_f32* dev);
 int clspmv_upload_ell_f32(const clspmv_ell_f32* host, clspmv_ell_f32* dev);
 int clspmv_upload_sell_f32(const clspmv_sell_f32* host, clspmv_sell_f32* dev);
 int clspmv_upload_b4csr_f32(const clspmv_b4csr_f32* host, clspmv_b4csr_f32* dev);
+int clspmv_upload_bcsr_f32(const clspmv_bcsr_f32* host, clspmv_bcsr_f32* dev);
+int clspmv_upload_bell_f32(const clspmv_bell_f32* host, clspmv_bell_f32* dev);
 int clspmv_upload_b4ell_f32(const clspmv_b4ell_f32* host, clspmv_b4ell_f32* dev);
 int clspmv_upload_sbell_f32(const clspmv_sbell_f32* host, clspmv_sbell_f32* dev);
 int clspmv_device_free_coo_f32(clspmv_coo_f32* dev);
@@ -273,6 +275,8 @@ int clspmv_device_free_bdia_f32(clspmv_bdia_f32* dev);
 int clspmv_device_free_ell_f32(clspmv_ell_f32* dev);
 int clspmv_device_free_sell_f32(clspmv_sell_f32* dev);
 int clspmv_device_free_b4csr_f32(clspmv_b4csr_f32* dev);
+int clspmv_device_free_bcsr_f32(clspmv_bcsr_f32* dev);
+int clspmv_device_free_bell_f32(clspmv_bell_f32* dev);
 int clspmv_device_free_b4ell_f32(clspmv_b4ell_f32* dev);
 int clspmv_device_free_sbell_f32(clspmv_sbell_f32* dev);
 
@@ -304,6 +308,15 @@ int clspmv_device_coo2sell_f32(const clspmv_coo_f32* coo, clspmv_sell_f32* dev, 
 /* coo2b4csr (:1740-1897). */
 int clspmv_device_coo2b4csr_f32(const clspmv_coo_f32* coo, clspmv_b4csr_f32* dev, unsigned int bwidth,
                                 unsigned int bheight, int alignment, clspmv_stream_t stream);
+/* coo2bcsr (:1593-1737), any block shape: the generic block CSR that only
+ * the serial bcsr_spmv reads (col_id = a block's first column, data[k * len
+ * + block], k = inner row * bwidth + inner column). */
+int clspmv_device_coo2bcsr_f32(const clspmv_coo_f32* coo, clspmv_bcsr_f32* dev, unsigned int bwidth,
+                               unsigned int bheight, int alignment, clspmv_stream_t stream);
+/* coo2bell (:1940-2006), any block shape; ellnum 0 = most blocks in a block
+ * row, CLSPMV_ERR_ARG when a block row holds more than a given ellnum. */
+int clspmv_device_coo2bell_f32(const clspmv_coo_f32* coo, clspmv_bell_f32* dev, unsigned int bwidth,
+                               unsigned int bheight, int alignment, int ellnum, clspmv_stream_t stream);
 /* coo2b4ell (:2008-2200); ellnum 0 = most blocks in a block row. */
 int clspmv_device_coo2b4ell_f32(const clspmv_coo_f32* coo, clspmv_b4ell_f32* dev, unsigned int bwidth,
                                 unsigned int bheight, int alignment, int ellnum, clspmv_stream_t stream);

@@ -2,8 +2,9 @@
 converters, which the converter tests pin to the reference's own templates:
 every array byte for byte, every scalar, and the same status on the inputs
 the host converters reject or refuse (unsorted COO, ids outside the matrix,
-unsupported block shapes, the DIA padding rule, ELL / b4ell widths, the
-MAX_MEM_OBJ caps). Plus the device sort against the host's stable sort."""
+unsupported block shapes, the DIA padding rule, ELL / b4ell / BELL widths,
+the MAX_MEM_OBJ caps), for the eight GPU formats and the generic BCSR / BELL
+of any block shape. Plus the device sort against the host's stable sort."""
 import ctypes as C
 
 import numpy as np
@@ -26,7 +27,9 @@ BLOCK = [(4, 4), (8, 2), (4, 1), (8, 8)]          # (bwidth, bheight)
 _HOST_DEFAULTS = {
     "csr": (0, ()), "dia": (0, (32,)), "bdia": (0, (32,)), "ell": (0, (32, 0)), "sell": (0, (32,)),
     "b4csr": (2, (32,)), "b4ell": (2, (32, 0)), "sbell": (2, (32,)),
+    "bcsr": (2, (32,)), "bell": (2, (32, 0)),
 }
+GENERIC = [(4, 4), (1, 1), (3, 2), (2, 5), (8, 8), (7, 3)]     # (bwidth, bheight): any shape
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -110,6 +113,44 @@ def test_block_formats(name, fmt, shape):
     check_pair(fmt, coo_of(name), bw, bh)
 
 
+@pytest.mark.parametrize("name", ALL_RECT)
+@pytest.mark.parametrize("fmt", ["bcsr", "bell"])
+@pytest.mark.parametrize("shape", GENERIC)
+def test_generic_block_formats(name, fmt, shape):
+    """The generic BCSR / BELL of any block shape (the layouts only the
+    serial bcsr_spmv / bell_spmv read) equal the host converters' arrays."""
+    bw, bh = shape
+    assert check_pair(fmt, coo_of(name), bw, bh) == _abi.OK
+
+
+@pytest.mark.parametrize("fmt,args", [("bcsr", (3, 2, 1)), ("bcsr", (4, 4, 7)), ("bell", (3, 2, 1, 0)),
+                                      ("bell", (4, 4, 32, 1)), ("bell", (4, 4, 32, 40)), ("bell", (5, 1, 5, 0)),
+                                      ("bcsr", (0, 4)), ("bell", (4, 0)), ("bell", (4, 4, 32, -1))])
+def test_generic_block_arguments(fmt, args):
+    """Alignments, ellnum (too small: CLSPMV_ERR_ARG on both sides) and zero
+    block dimensions (CLSPMV_ERR_ARG)."""
+    check_pair(fmt, coo_of("powerlaw3k"), *args)
+
+
+def test_generic_bell_too_few_slots_rejected():
+    assert check_pair("bell", coo_of("blocks300"), 4, 4, 32, 1) == _abi.ERR_ARG
+
+
+@pytest.mark.parametrize("fmt", ["bcsr", "bell"])
+def test_generic_block_upload_roundtrip(fmt):
+    """clspmv_upload_<fmt>_f32 of the host arrays holds what the device
+    converter makes."""
+    coo = coo_of("blocks_odd")
+    host = getattr(F, f"coo2{fmt}")(coo, 3, 2)
+    up = F.DeviceMatrix(host)
+    dev = F.device_convert(device_coo(coo), fmt, 3, 2)
+    for field, _, _ in _abi.FORMATS[fmt][1]:
+        a, b = up.tensors[field].cpu().numpy(), dev.tensors[field].cpu().numpy()
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), field
+    with pytest.raises(ValueError):
+        dev.spmv(torch.zeros(coo.shape[1], device="cuda"), torch.zeros(coo.shape[0], device="cuda"))
+
+
 @pytest.mark.parametrize("sh", [1, 3, 32])
 def test_sbell_slice_heights(sh):
     assert check_pair("sbell", coo_of("blocks_odd"), 4, 4, sh) == _abi.OK
@@ -150,7 +191,8 @@ def _with_duplicates(name, seed=0):
 
 
 @pytest.mark.parametrize("fmt,args", [("csr", ()), ("ell", ()), ("sell", ()), ("dia", ()),
-                                      ("b4csr", (4, 4)), ("b4ell", (8, 2)), ("sbell", (4, 2))])
+                                      ("b4csr", (4, 4)), ("b4ell", (8, 2)), ("sbell", (4, 2)),
+                                      ("bcsr", (3, 2)), ("bell", (2, 3))])
 def test_repeated_entries_keep_last(fmt, args):
     h, w, r, c, v, order = _with_duplicates("banded7" if fmt == "dia" else "blocks_odd")
     coo = F.coo_matrix(h, w, r[order], c[order], v[order])
@@ -168,7 +210,7 @@ def test_dia_unsorted_input(name):
 
 
 @pytest.mark.parametrize("fmt,args", [("csr", ()), ("ell", ()), ("sell", ()), ("b4csr", (4, 4)),
-                                      ("b4ell", (4, 4)), ("sbell", (4, 4))])
+                                      ("b4ell", (4, 4)), ("sbell", (4, 4)), ("bcsr", (3, 3)), ("bell", (4, 4))])
 def test_unsorted_rejected(fmt, args):
     h, w, r, c, v = cases()["random_sparse"]
     perm = np.random.default_rng(1).permutation(len(r))
@@ -176,7 +218,8 @@ def test_unsorted_rejected(fmt, args):
     assert check_pair(fmt, coo, *args) == _abi.ERR_NOT_SORTED
 
 
-@pytest.mark.parametrize("fmt,args", [("csr", ()), ("dia", ()), ("sell", ()), ("b4csr", (4, 4))])
+@pytest.mark.parametrize("fmt,args", [("csr", ()), ("dia", ()), ("sell", ()), ("b4csr", (4, 4)), ("bcsr", (2, 2)),
+                                      ("bell", (2, 2))])
 def test_out_of_range_rejected(fmt, args):
     coo = F.coo_matrix(10, 10, [0, 3, 10], [1, 2, 3], [1.0, 2.0, 3.0])
     assert check_pair(fmt, coo, *args) == _abi.ERR_ARG
@@ -217,7 +260,7 @@ def test_tall_dia_with_entries_above_the_aligned_width(fmt, h, w, top):
 def test_empty_matrix():
     coo = F.coo_matrix(37, 41, np.zeros(0, int), np.zeros(0, int), np.zeros(0, np.float32))
     for fmt, args in [("csr", ()), ("ell", ()), ("sell", ()), ("dia", ()), ("bdia", ()),
-                      ("b4csr", (4, 4)), ("b4ell", (4, 4)), ("sbell", (4, 4))]:
+                      ("b4csr", (4, 4)), ("b4ell", (4, 4)), ("sbell", (4, 4)), ("bcsr", (3, 5)), ("bell", (3, 5))]:
         check_pair(fmt, coo, *args)
 
 
