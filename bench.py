@@ -747,6 +747,9 @@ def run_ours(args):
         detail["sharded_akx"] = run_sharded_akx(world, dev)
         if rank == 0:
             print(json.dumps({"detail": "sharded_akx", **detail["sharded_akx"]}), flush=True)
+        detail["sharded_serving"] = run_sharded_serving(world, rank, dev)
+        if rank == 0:
+            print(json.dumps({"detail": "sharded_serving", **detail["sharded_serving"]}), flush=True)
     if not args.no_extras and not args.only and world == 1:
         for name, fn in (("extras", lambda: run_extras(args, items, mats, peak)),
                          ("cocktail_c3", lambda: run_cocktail_c3(args, peak)),
@@ -833,6 +836,38 @@ def run_sharded_akx(world: int, dev, n: int = 128, steps: int = 40):
             "ms_per_step": round(ms, 4), "gflops": round(2 * total / (ms * 1e-3) / 1e9, 1),
             "gather_bytes_per_step": 4 * s.block * world, "x_finite": finite,
             "note": "rows split evenly, each rank's slab built from its own rows; one all_gather_into_tensor per step"}
+
+
+def run_sharded_serving(world: int, rank: int, dev, n_requests: int = 3000, rate: float = 30_000.0):
+    """Serving across the node's GPUs as independent units: 16 matrices
+    (banded, power-law, 4x4 blocks; 0.5-3M nonzeros) placed whole by
+    serving.place over the ranks' equal budgets, one Poisson stream of
+    requests (k uniform in [1, 8]) of which each rank serves those of its own
+    matrices on its own GPU (serving.ShardedServer on that device), at the
+    stream's arrival times. No data crosses between GPUs. Whole-job req/s =
+    all requests over the slowest rank's span; p50 / p99 from rank 0."""
+    import torch
+    import torch.distributed as dist
+    from clspmv_mic_b200 import serving as SV
+    from clspmv_mic_b200 import workloads as W
+    hosts = W.sharded_serving_hosts()
+    budget = 16 << 30
+    assign = SV.place({i: SV.resident_bytes(h) for i, (_, h) in enumerate(hosts)}, [budget] * world)
+    owned = [i for i, r in assign.items() if r == rank]
+    if world > 1:
+        dist.barrier()
+    res = W.serve_sharded(hosts, [dev], budget, n_requests=n_requests, rate=rate, owned=owned)
+    span = torch.tensor([res.get("span_s", 0.0)], dtype=torch.float64, device=dev)
+    count = torch.tensor([float(res["requests"])], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(span, op=dist.ReduceOp.MAX)
+        dist.all_reduce(count)
+    total = float(count.item())
+    return {"ranks": world, "matrices": len(hosts), "requests": int(total), "offered_req_per_s": rate, "k": [1, 8],
+            "req_per_s": round(total / float(span.item()), 1) if span.item() > 0 else None,
+            "rank0": {k: res[k] for k in ("matrices", "requests", "served") if k in res},
+            "note": "matrices placed whole (serving.place), each rank serves its own on its GPU; "
+                    "req/s = all requests / slowest rank's span"}
 
 
 def run_device_convert(items):

@@ -360,6 +360,87 @@ def _wait_until(t: float) -> None:
         time.sleep(dt)
 
 
+def sharded_serving_hosts(count: int = 16, seed: int = 21):
+    """Host matrices for the multi-GPU serving leg: banded, power-law and
+    4x4-block matrices of 0.5-3M nonzeros, as CSR."""
+    from . import formats as Fm
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = ("banded", "powerlaw", "blocked")[i % 3]
+        if kind == "banded":
+            arrs = synth.banded(int(rng.integers(100_000, 400_000)), 7, seed=seed + i)
+        elif kind == "powerlaw":
+            arrs = synth.powerlaw(int(rng.integers(50_000, 150_000)), mean=16.0, maxlen=2000, seed=seed + i)
+        else:
+            arrs = synth.block_rows(int(rng.integers(10_000, 40_000)), 8, seed=seed + i)
+        out.append((kind, Fm.coo2csr(Fm.coo_matrix(*arrs))))
+    return out
+
+
+def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000, rate: float = 20_000.0,
+                  k_lo: int = 1, k_hi: int = 8, seed: int = 5, owned=None):
+    """serving.ShardedServer over `devices`: the host matrices registered
+    whole on the device with the most budget left, an open-loop Poisson
+    stream of `n_requests` (k uniform in [k_lo, k_hi], matrix uniform over
+    all `hosts`), each request routed to its matrix's device. With `owned`
+    (indices into `hosts`), only those matrices are registered and only
+    their requests are submitted, at the stream's arrival times: the share
+    of one process of a node that serves a placement (serving.place) on its
+    own GPU. Returns served req/s, p50 / p99, the time from the first
+    submission to the last completion, and matrices / requests per device."""
+    import torch
+    from .serving import ShardedServer, latency_stats
+    rng = np.random.default_rng(seed)
+    pick_all = rng.integers(len(hosts), size=n_requests)
+    ks_all = rng.integers(k_lo, k_hi + 1, size=n_requests)
+    arrivals_all = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    mine = set(range(len(hosts))) if owned is None else set(int(i) for i in owned)
+    srv = ShardedServer(budget_per_device, devices=devices)
+    for i in sorted(mine):
+        if srv.register(f"m{i}", hosts[i][1]) is None:
+            raise RuntimeError(f"matrix {i} fits no device")
+    sel = [j for j in range(n_requests) if int(pick_all[j]) in mine]
+    # one (width x k_hi) block of right-hand sides per matrix, on the matrix's device
+    pools = {}
+    for i in sorted(mine):
+        d = srv.devices[srv.owner[f"m{i}"]]
+        gen = torch.Generator(device=d)
+        gen.manual_seed(seed + i)
+        pools[i] = torch.rand((hosts[i][1].shape[1], k_hi), generator=gen, device=d)
+    for d in srv.devices:
+        torch.cuda.synchronize(d)
+    futures = []
+    with srv:
+        for i in sorted(mine):   # warm every matrix's path once
+            srv.submit(f"m{i}", pools[i][:, :1], keep_result=False).result(timeout=600)
+
+        def client():
+            t_start = time.perf_counter()
+            for j in sel:
+                _wait_until(t_start + arrivals_all[j])
+                futures.append(srv.submit(f"m{int(pick_all[j])}", pools[int(pick_all[j])][:, :int(ks_all[j])],
+                                          keep_result=False))
+
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        for f in futures:
+            f.result(timeout=600)
+    out = dict(devices=len(srv.devices), matrices=len(mine), requests=len(sel), offered_req_per_s=rate,
+               k=[k_lo, k_hi],
+               matrices_per_device=[sum(1 for i in mine if srv.owner[f"m{i}"] == j) for j in range(len(srv.devices))],
+               requests_per_device=[sum(1 for j in sel if srv.owner[f"m{int(pick_all[j])}"] == d)
+                                    for d in range(len(srv.devices))])
+    if futures:
+        st = latency_stats(futures)
+        reqs = [f.request for f in futures]
+        out["span_s"] = max(r.t_done for r in reqs) - min(r.t_submit for r in reqs)
+        out["served"] = dict(req_per_s=round(st["req_per_s"], 1), p50_ms=round(st["p50_ms"], 3),
+                             p99_ms=round(st["p99_ms"], 3))
+    return out
+
+
 def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.0, k_lo: int = 1, k_hi: int = 32,
           value_type: str = "f32", seed: int = 3, slots: int = 2, max_requests: int = 4096):
     """Open-loop Poisson stream of `n_requests` at `rate` req/s, k uniform in

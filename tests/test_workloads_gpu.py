@@ -81,6 +81,25 @@ def test_serve_small():
     assert r["served"]["p99_ms"] >= r["served"]["p50_ms"]
 
 
+def test_serve_sharded_shares_cover_the_stream():
+    """The multi-GPU serving leg's split: each process serves the requests
+    of the matrices placed on it; the shares of a 3-way placement, run one
+    after another on this GPU, serve every request of the stream once."""
+    from clspmv_mic_b200 import serving as SV
+    hosts = W.sharded_serving_hosts(count=6)
+    whole = W.serve_sharded(hosts, ["cuda:0"], 1 << 32, n_requests=150, rate=20_000.0)
+    assert whole["requests"] == 150 and whole["matrices"] == 6 and whole["served"]["req_per_s"] > 0
+    assign = SV.place({i: SV.resident_bytes(h) for i, (_, h) in enumerate(hosts)}, [1 << 32] * 3)
+    assert sorted(assign) == list(range(6))
+    total = 0
+    for r in range(3):
+        owned = [i for i, d in assign.items() if d == r]
+        part = W.serve_sharded(hosts, ["cuda:0"], 1 << 32, n_requests=150, rate=20_000.0, owned=owned)
+        assert part["matrices"] == len(owned)
+        total += part["requests"]
+    assert total == 150
+
+
 def test_measure_tables_small(tmp_path, monkeypatch):
     """Device-measured .ben tables are readable by the partitioner and give
     positive rates for every grid point."""
