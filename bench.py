@@ -9,12 +9,14 @@ best variant per format, e.g. src/spmv_csr_vector.cpp:649-656):
 
   stencil27   3D 27-point stencil 128^3 (2,097,152 rows, 55,742,968 nnz):  DIA, BDIA
   powerlaw    2^20 rows, Zipf(2.0) lengths on [1,10000] scaled to mean 16:  CSR (nonzero-chunk kernel),
-              COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32
+              COO, ELL (ELL(K) + COO tail, K by the 1/3-of-rows rule), SELL-32 (read
+              through its length plan: real entries only)
   blocks4x4   500,000 block rows x 8 dense 4x4 blocks (2,000,000 rows, 64M nnz):  BELL, SBELL, BCSR
 
 The merge-path, CSR-vector and CSR-scalar kernels (the last two are the
-reference's CSR drivers' mappings) and SELL read through its length plan
-are timed separately and reported under "variants".
+reference's CSR drivers' mappings) and SELL read slot by slot, padding
+included (the reference's SELL kernel's reads), are timed separately and
+reported under "variants".
 
 value = sum of useful flops (2 nnz per SpMV) / sum of kernel times, GFLOP/s.
 Kernel times are CUDA events on the launching stream; every matrix is larger
@@ -94,9 +96,9 @@ def split_hyb(coo_arrays, k):
     return (h, w, r[head], c[head], v[head]), (h, w, r[~head], c[~head], v[~head])
 
 
-VARIANT_KEYS = {"csr_merge", "csr_vector", "csr_scalar", "sell32_planned"}
+VARIANT_KEYS = {"csr_merge", "csr_vector", "csr_scalar", "sell32_padded"}
 FORMAT_KEYS = {"stencil27": ["dia", "bdia"],
-               "powerlaw": ["csr_chunk", "csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32", "sell32_planned"],
+               "powerlaw": ["csr_chunk", "csr_merge", "csr_vector", "csr_scalar", "coo", "ell", "ell_tail_coo", "sell32", "sell32_padded"],
                "blocks4x4": ["bell", "sbell", "bcsr"]}
 
 
@@ -151,8 +153,9 @@ def build_workload(small: bool, only=None):
                 conv=(ell_part, "ell", (32, k)))
             add("ell_tail_coo", "powerlaw", lambda: F.coo_matrix(*coo_tail), part_of="ell")
         sell = once(lambda: F.coo2sell(coo, 32))
-        add("sell32", "powerlaw", sell, conv=(pl, "sell", (32,)))                # every stored slot
-        add("sell32_planned", "powerlaw", sell, {"variant": "planned"})          # real entries only (length plan)
+        # with its length plan (real entries only, tails' column ids compact), and every stored slot
+        add("sell32", "powerlaw", sell, {"variant": "planned"}, conv=(pl, "sell", (32,)))
+        add("sell32_padded", "powerlaw", sell)
     if "blocks4x4" in mats:
         bl = mats["blocks4x4"]
         coo = F.coo_matrix(*bl)
@@ -165,8 +168,9 @@ def build_workload(small: bool, only=None):
 def algorithmic_bytes(it) -> int:
     """Arrays the kernel must stream (values, indices, pointers, padding),
     plus x read once and y read and written once. SELL with its length plan
-    reads, of each slice column, only the 32-byte sectors holding real
-    entries: those sectors of col and data, the row lengths and the slice
+    reads, of each slice column, only the 128-byte lines holding real
+    entries (B200 moves whole lines between DRAM and L2), the tails' column
+    ids from the plan's compact copy, the plan's arrays and the slice
     pointers."""
     if it.get("needed") is not None:
         return int(it["needed"] + 4 * it["cols"] + 8 * it["rows"])
@@ -551,9 +555,11 @@ def run_ours(args):
         if it["host"].fmt == "csr" and it["kw"].get("variant") == "chunk":
             it["dev"].chunk_plan(stream)
         if it["host"].fmt == "sell" and it["kw"].get("variant") == "planned":
-            # the sectors holding real entries, the row lengths and the slice pointers
+            # the 128-byte lines holding real entries (a data line per tail
+            # entry, the tails' column ids compact), the plan's arrays and
+            # the slice pointers
             d = it["dev"]
-            it["needed"] = d.sell_plan_sector_bytes() + 4 * it["rows"] + 4 * (it["host"].struct.sell_slice_num + 1)
+            it["needed"] = d.sell_plan_line_bytes() + 4 * (it["host"].struct.sell_slice_num + 1)
         it.pop("host")
     torch.cuda.synchronize()
 

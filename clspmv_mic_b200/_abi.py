@@ -257,6 +257,7 @@ def _declare(lib):
         "clspmv_sell_plan_entries": (C.c_longlong, [VP]),
         "clspmv_sell_plan_items": (C.c_longlong, [VP]),
         "clspmv_sell_plan_sector_bytes": (C.c_longlong, [VP]),
+        "clspmv_sell_plan_line_bytes": (C.c_longlong, [VP]),
         "clspmv_sell_plan_free": (I32, [VP]),
         "clspmv_pack_values": (I32, [I32, VP, I32, VP, VP, VP]),
         "clspmv_batch_create": (I32, [I32, P(VP)]),

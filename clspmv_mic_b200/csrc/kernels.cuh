@@ -469,6 +469,34 @@ __device__ __forceinline__ void sell_tail_cta(const SellArgs& a, const int* __re
     }
 }
 
+// sell_tail_cta with the tail column ids copied by the plan into one
+// compact array (tail_col[tail_off[it] + k - item.y]): the lanes of a warp
+// read an item's column ids from consecutive words, and only its values
+// from the slice's stride-sh column-major layout.
+__device__ __forceinline__ void sell_tail_compact_cta(const SellArgs& a, const int* __restrict__ rlen,
+                                                      const int2* __restrict__ items, const int* __restrict__ tail_off,
+                                                      const int* __restrict__ tail_col, long long nitems, int cta, int ncta)
+{
+    const uint64_t pe = policy_evict_first(), pl = policy_evict_last();
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = (long long)ncta * (kBlock / 32);
+    const int sh = a.slice_height;
+    for (long long it = (long long)cta * (kBlock / 32) + (threadIdx.x >> 5); it < nitems; it += nwarps) {
+        const int2 item = __ldg(items + it);
+        const int s = item.x / sh, lr = item.x - s * sh;
+        const size_t base = (size_t)__ldg(a.slice_ptr + s) + lr;
+        const int n = __ldg(tail_off + it + 1) - __ldg(tail_off + it);
+        const int* __restrict__ tc = tail_col + __ldg(tail_off + it) - item.y;
+        float acc = 0.f;
+#pragma unroll 4
+        for (int k = item.y + lane; k < item.y + n; k += 32)
+            acc = fmaf(ld_stream_f(a.data + base + (size_t)k * sh, pe), ld_x(a.x + ld_stream_i(tc + k, pe), pl), acc);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
+        if (lane == 0) atomicAdd(a.y + item.x, a.alpha * acc);
+    }
+}
+
 // SELL with the padding skipped, on the column-balanced mapping of sell_cta:
 // the Q lanes of a column each own 4 rows of the slice, and a lane issues its
 // 128-bit loads only for the columns before the longest real length of its 4

@@ -127,6 +127,26 @@ __global__ void __launch_bounds__(kBlock) k_sell_tail(SellArgs a, const int* __r
     sell_tail_cta(a, rlen, items, nitems, blockIdx.x, gridDim.x);
 }
 
+__global__ void __launch_bounds__(kBlock) k_sell_tail_compact(SellArgs a, const int* __restrict__ rlen,
+                                                              const int2* __restrict__ items, const int* __restrict__ tail_off,
+                                                              const int* __restrict__ tail_col, long long nitems)
+{
+    sell_tail_compact_cta(a, rlen, items, tail_off, tail_col, nitems, blockIdx.x, gridDim.x);
+}
+
+// tail_col[tail_off[t] + j] = column id of entry item.y + j of split item t
+__global__ void k_sell_tail_cols(const int2* __restrict__ items, const int* __restrict__ tail_off, long long nitems,
+                                 const int* __restrict__ slice_ptr, const int* __restrict__ col, int sh, int* tail_col)
+{
+    for (long long t = blockIdx.x; t < nitems; t += gridDim.x) {
+        const int2 item = items[t];
+        const int s = item.x / sh, lr = item.x - s * sh;
+        const size_t base = (size_t)slice_ptr[s] + lr;
+        const int o = tail_off[t], n = tail_off[t + 1] - o;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) tail_col[o + j] = col[base + (size_t)(item.y + j) * sh];
+    }
+}
+
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_csr_scalar(CsrArgs a) { csr_scalar_cta<A>(a, blockIdx.x, gridDim.x, nullptr); }
 
@@ -468,8 +488,8 @@ int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha,
 // kSellTailCols entries (split_items). Other slice heights: each row's first
 // kSellHead entries with a thread per row, then the tails (items).
 int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* items, long long nitems, const int* head,
-                        const int2* split_items, long long nsplit, const float* x, float* y, float alpha, float beta,
-                        cudaStream_t st, bool atomic)
+                        const int2* split_items, long long nsplit, const int* tail_off, const int* tail_col,
+                        const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
 {
     if (!m || !x || !y || !m->sell_slice_ptr || !rlen || (nitems > 0 && !items)) return CLSPMV_ERR_ARG;
     const int rows = m->matinfo.height;
@@ -492,7 +512,11 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
             return after_launch(1);
         });
         if (rc || !head || nsplit == 0) return rc;
-        k_sell_tail<<<persistent_grid(k_sell_tail, nsplit, kBlock / 32), kBlock, 0, st>>>(a, rlen, split_items, nsplit);
+        if (tail_col)
+            k_sell_tail_compact<<<persistent_grid(k_sell_tail_compact, nsplit, kBlock / 32), kBlock, 0, st>>>(
+                a, rlen, split_items, tail_off, tail_col, nsplit);
+        else
+            k_sell_tail<<<persistent_grid(k_sell_tail, nsplit, kBlock / 32), kBlock, 0, st>>>(a, rlen, split_items, nsplit);
         return after_launch(1);
     }
     if (atomic) k_sell_head<true><<<persistent_grid(k_sell_head<true>, rows, kBlock), kBlock, 0, st>>>(a, rlen);
@@ -893,9 +917,13 @@ struct clspmv_sell_plan {
     int2* items = nullptr;     // device: (row, first entry) of each tail item past the first kSellHead entries
     int* head = nullptr;       // device: prefix of per-slice widths up to the second-longest row
     int2* split_items = nullptr;   // device: (longest row, first entry) of each tail item past its slice's head
+    int* tail_off = nullptr;   // device: prefix of the split items' entry counts (nsplit + 1)
+    int* tail_col = nullptr;   // device: the split items' column ids, item after item (null: read in place)
     long long rows = 0, nitems = 0, nsplit = 0, entries = 0;
     long long sector_bytes = 0;   // col + data bytes of the 32-byte sectors holding real entries
+    long long line_bytes = 0;     // bytes the split walk must read in 128-byte lines (see clspmv_sell_plan_line_bytes)
     bool split = true;         // walk the heads and the tails apart (power-of-two slice heights)
+    bool compact = true;       // the tails' column ids from tail_col
 };
 
 int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
@@ -942,9 +970,55 @@ int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
         if (!rc) rc = cuda_status(cudaMalloc(&p->split_items, sizeof(int2) * std::max<size_t>(1, split.size())));
         if (!rc && !split.empty())
             rc = cuda_status(cudaMemcpy(p->split_items, split.data(), sizeof(int2) * split.size(), cudaMemcpyHostToDevice));
-        // CLSPMV_SELL_SPLIT=0 walks every column instead (for measurements)
+        // the split items' column ids in one compact array (structure only: the
+        // values stay in the matrix, so a plan stays valid while they change)
+        std::vector<int> off(split.size() + 1, 0);
+        for (size_t t = 0; t < split.size(); t++)
+            off[t + 1] = off[t] + std::min(kSellTailCols, rlen[(size_t)split[t].x] - split[t].y);
+        if (!rc) rc = cuda_status(cudaMalloc(&p->tail_off, sizeof(int) * off.size()));
+        if (!rc) rc = cuda_status(cudaMemcpy(p->tail_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+        if (!rc) rc = cuda_status(cudaMalloc(&p->tail_col, sizeof(int) * std::max(1, off.back())));
+        if (!rc && !split.empty()) {
+            k_sell_tail_cols<<<(unsigned)std::min<size_t>(split.size(), 148 * 32), kBlock>>>(
+                p->split_items, p->tail_off, (long long)split.size(), m->sell_slice_ptr, m->sell_col_id,
+                (int)m->sell_slice_height, p->tail_col);
+            rc = after_launch(1);
+            if (!rc) rc = cuda_status(cudaDeviceSynchronize());
+        }
+        // The DRAM bytes of the split walk at 128-byte line granularity: the
+        // lines of col and data holding a head entry, the data line of every
+        // tail entry, the tails' compact column ids, and the plan's arrays
+        // (row lengths, head table, items, item offsets).
+        std::vector<int> sp((size_t)ns + 1);
+        if (!rc) rc = cuda_status(cudaMemcpy(sp.data(), m->sell_slice_ptr, sizeof(int) * sp.size(), cudaMemcpyDeviceToHost));
+        if (!rc) {
+            const long long nlines = ((long long)sp[(size_t)ns] + 31) / 32 + 1;
+            std::vector<uint64_t> dline((size_t)(nlines + 63) / 64, 0), cline((size_t)(nlines + 63) / 64, 0);
+            auto mark = [](std::vector<uint64_t>& bm, long long l) { bm[(size_t)(l >> 6)] |= 1ull << (l & 63); };
+            long long tail_entries = 0;
+            for (long long sl = 0; sl < ns; sl++) {
+                const int l2 = head[(size_t)sl + 1] - head[(size_t)sl];
+                for (long long r = sl * shs; r < std::min(rows, (sl + 1) * shs); r++) {
+                    const int len = rlen[(size_t)r];
+                    for (int k = 0; k < len; k++) {
+                        const long long pos = (long long)sp[(size_t)sl] + (long long)k * shs + (r - sl * shs);
+                        mark(dline, pos >> 5);
+                        if (k < l2) mark(cline, pos >> 5);
+                        else tail_entries++;
+                    }
+                }
+            }
+            long long lines = 0;
+            for (uint64_t w : dline) lines += __builtin_popcountll(w);
+            for (uint64_t w : cline) lines += __builtin_popcountll(w);
+            p->line_bytes = 128 * lines + 4 * tail_entries + 4 * rows + 4 * (ns + 1) + 12 * (long long)split.size() + 4;
+        }
+        // CLSPMV_SELL_SPLIT=0 walks every column instead, CLSPMV_SELL_TAIL_COMPACT=0
+        // reads the tails' column ids in place (for measurements)
         const char* e = getenv("CLSPMV_SELL_SPLIT");
         p->split = !(e && atoi(e) == 0);
+        const char* tcmp = getenv("CLSPMV_SELL_TAIL_COMPACT");
+        p->compact = !(tcmp && atoi(tcmp) == 0);
     }
     if (!rc) {
         // a 32-byte sector of one slice column holds 8 consecutive rows (slice
@@ -973,13 +1047,14 @@ int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* 
                               float beta, clspmv_stream_t s)
 {
     if (!p) return CLSPMV_ERR_ARG;
-    return launch_sell_planned(m, p->rlen, p->items, p->nitems, p->split ? p->head : nullptr, p->split_items, p->nsplit, x, y,
-                               alpha, beta, S(s), false);
+    return launch_sell_planned(m, p->rlen, p->items, p->nitems, p->split ? p->head : nullptr, p->split_items, p->nsplit,
+                               p->tail_off, p->compact ? p->tail_col : nullptr, x, y, alpha, beta, S(s), false);
 }
 
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* p) { return p ? p->entries : -1; }
 long long clspmv_sell_plan_items(const clspmv_sell_plan* p) { return p ? p->nitems : -1; }
 long long clspmv_sell_plan_sector_bytes(const clspmv_sell_plan* p) { return p ? p->sector_bytes : -1; }
+long long clspmv_sell_plan_line_bytes(const clspmv_sell_plan* p) { return p ? p->line_bytes : -1; }
 
 int clspmv_sell_plan_free(clspmv_sell_plan* p)
 {
@@ -988,6 +1063,8 @@ int clspmv_sell_plan_free(clspmv_sell_plan* p)
     if (p->items) cudaFree(p->items);
     if (p->head) cudaFree(p->head);
     if (p->split_items) cudaFree(p->split_items);
+    if (p->tail_off) cudaFree(p->tail_off);
+    if (p->tail_col) cudaFree(p->tail_col);
     delete p;
     return CLSPMV_OK;
 }

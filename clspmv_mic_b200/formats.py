@@ -283,6 +283,10 @@ class DeviceMatrix:
         """Stored entries the padding-free SELL SpMV reads."""
         return int(lib().clspmv_sell_plan_entries(self.sell_plan()))
 
+    def sell_plan_line_bytes(self) -> int:
+        """Bytes the planned SpMV must read in 128-byte lines (clspmv_sell_plan_line_bytes)."""
+        return int(lib().clspmv_sell_plan_line_bytes(self.sell_plan()))
+
     def sell_plan_sector_bytes(self) -> int:
         """col + data bytes of the 32-byte sectors holding real entries (what
         the padding-free SELL SpMV must move from the matrix arrays)."""

@@ -448,8 +448,11 @@ int clspmv_sell_spmv_f32(const clspmv_sell_f32* dev, const float* x, float* y,
  * 16-byte aligned arrays the planned SpMV walks the slot space like
  * clspmv_sell_spmv_f32 (equal runs of slice columns per warp, 4 rows per
  * lane) but each lane loads a column only while one of its 4 rows still has
- * real entries, so the tail columns of a slice padded to one long row fetch
- * that row's 32-byte sectors only; other slice heights sum each row's first
+ * real entries, and only up to the slice's second-longest row; the longest
+ * row's entries past it go to a warp per 256 entries, which reads their
+ * column ids from a compact copy the plan made (structure only: the values
+ * stay in the matrix, so the plan holds while they change, not while the
+ * column ids do) and their values in place; other slice heights sum each row's first
  * 32 entries with a thread per row and longer rows' tails with a warp per
  * 256 entries. Same y as clspmv_sell_spmv_f32 up to summation order, except
  * where x holds Inf or NaN at a skipped padding column. No counterpart in
@@ -464,6 +467,11 @@ long long clspmv_sell_plan_items(const clspmv_sell_plan* plan);
 /* bytes of col and data in the 32-byte sectors that hold real entries: what
  * the planned SpMV must move from the matrix arrays */
 long long clspmv_sell_plan_sector_bytes(const clspmv_sell_plan* plan);
+/* bytes the planned SpMV (slice heights 4..128) must read at the 128-byte
+ * line granularity of B200's DRAM traffic: the col and data lines holding
+ * the heads' entries, a data line per tail entry, the tails' compact column
+ * ids and the plan's own arrays */
+long long clspmv_sell_plan_line_bytes(const clspmv_sell_plan* plan);
 int clspmv_sell_plan_free(clspmv_sell_plan* plan);
 
 /* BELL = b4ell, block shapes {1,2,4,8} x {4,8}. Replaces the 32 kernels of

@@ -22,7 +22,7 @@ def _full_headline():
     clocks = {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 120}
     cpu = {"value": 1.712, "unit": bench.UNIT, "cores": 1, "kind": "reference",
            "sample": "csr_spmv on stencil27 best of 50, powerlaw best of 50, blocks4x4 best of 50, 1 thread"}
-    parity = {"checked": keys[:4] + keys[5:] + ["csr_merge", "csr_vector", "csr_scalar", "sell32_planned"],
+    parity = {"checked": keys[:4] + keys[5:] + ["csr_merge", "csr_vector", "csr_scalar", "sell32_padded"],
               "rows_over_bound": 0, "max_err_fp64": 2.34e-07, "ref_err_fp64": 3.1e-07,
               "bound": "per row |y - csr_spmv y| <= 1e-5 sum|a x|, full-size matrices"}
     return bench.headline(value=747.51, world=8, steps=200, warmup=5, ms_per_step=0.98582, small=False,
