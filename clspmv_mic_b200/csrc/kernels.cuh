@@ -537,8 +537,14 @@ __device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __
         long long c = c0;
         while (c < c1) {
             const long long sb = cptr[s] / cdiv, se = cptr[s + 1] / cdiv;
-            if (se <= c) {
-                s++;
+            if (se <= c) {   // the next slice with a column at or past c (runs of empty slices are skipped at once)
+                int l = s + 1, h = a.nslice - 1;
+                while (l < h) {
+                    const int mid = (l + h) >> 1;
+                    if ((long long)cptr[mid + 1] <= c * cdiv) l = mid + 1;
+                    else h = mid;
+                }
+                s = l;
                 continue;
             }
             const long long ce = min(c1, se);
