@@ -409,15 +409,32 @@ __device__ __forceinline__ void sell_rows4_cta(const SellArgsT<V>& a, int cta, i
 constexpr int kSellHead = 32;
 constexpr int kSellTailCols = 256;
 
+// Scans back from the slice's last column 16 slots at a time (the loads of a
+// group are independent, so a row padded over thousands of columns costs
+// hundreds of round trips, not thousands); the first slot always counts.
 __device__ __forceinline__ int sell_row_length(const int* slice_ptr, const int* col, const float* data, int sh, long long row)
 {
+    constexpr int C = 16;
     const int s = (int)(row / sh), lr = (int)(row - (long long)s * sh);
     const int start = slice_ptr[s];
     int k = (slice_ptr[s + 1] - start) / sh;
+    const size_t base = (size_t)start + lr;
     while (k > 1) {
-        const size_t i = (size_t)start + (size_t)(k - 1) * sh + lr;
-        if (col[i] != col[i - sh] || data[i] != 0.0f) break;
-        k--;
+        const int lo = max(1, k - C);   // slots lo .. k-1 are examined
+        int c[C + 1];
+        float d[C];
+#pragma unroll
+        for (int t = 0; t <= C; t++) {
+            const int j = k - 1 - t;     // slot j, and j - 1 for the comparison
+            c[t] = j >= lo - 1 ? col[base + (size_t)j * sh] : 0;
+            if (t < C) d[t] = j >= lo ? data[base + (size_t)j * sh] : 0.0f;
+        }
+#pragma unroll
+        for (int t = 0; t < C; t++) {
+            const int j = k - 1 - t;
+            if (j >= lo && (c[t] != c[t + 1] || d[t] != 0.0f)) return j + 1;
+        }
+        k = lo;
     }
     return k;
 }
