@@ -9,6 +9,7 @@ error is max |Y - Y64| / scale.
 """
 from __future__ import annotations
 
+import gc
 import math
 import threading
 import time
@@ -411,6 +412,8 @@ def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000
     for d in srv.devices:
         torch.cuda.synchronize(d)
     futures = []
+    gc.collect()
+    gc.freeze()
     with srv:
         for i in sorted(mine):   # warm every matrix's path once
             srv.submit(f"m{i}", pools[i][:, :1], keep_result=False).result(timeout=600)
@@ -427,6 +430,7 @@ def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000
         th.join()
         for f in futures:
             f.result(timeout=600)
+    gc.unfreeze()
     out = dict(devices=len(srv.devices), matrices=len(mine), requests=len(sel), offered_req_per_s=rate,
                k=[k_lo, k_hi],
                matrices_per_device=[sum(1 for i in mine if srv.owner[f"m{i}"] == j) for j in range(len(srv.devices))],
@@ -480,8 +484,13 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
     span_seq = time.perf_counter() - t0
     lat_seq = np.array(lat_seq) * 1e3
 
-    # the serving loop, fed by a client thread on the same schedule
+    # the serving loop, fed by a client thread on the same schedule; the
+    # objects alive before the stream are moved out of the cyclic collector's
+    # reach for its duration (a full collection over a large process can
+    # stall the loop thread for a whole batch)
     futures = [None] * n_requests
+    gc.collect()
+    gc.freeze()
     srv.start()
     # warm the loop's batches once
     srv.submit(names[pick[0]], Xs[0], keep_result=False).result(timeout=600)
@@ -500,6 +509,7 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
     stats = latency_stats(futures)
     batches = srv.batches_run
     srv.stop()
+    gc.unfreeze()
     return dict(requests=n_requests, offered_req_per_s=rate, k=[k_lo, k_hi], value_type=value_type,
                 matrices=len(names), resident_gb=round(admitted_bytes / 1e9, 2),
                 served=dict(req_per_s=round(stats["req_per_s"], 1), p50_ms=round(stats["p50_ms"], 3),
