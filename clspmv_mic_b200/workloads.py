@@ -412,25 +412,27 @@ def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000
     for d in srv.devices:
         torch.cuda.synchronize(d)
     futures = []
+
+    def client():
+        t_start = time.perf_counter()
+        for j in sel:
+            _wait_until(t_start + arrivals_all[j])
+            futures.append(srv.submit(f"m{int(pick_all[j])}", pools[int(pick_all[j])][:, :int(ks_all[j])],
+                                      keep_result=False))
+
     gc.collect()
     gc.freeze()
-    with srv:
-        for i in sorted(mine):   # warm every matrix's path once
-            srv.submit(f"m{i}", pools[i][:, :1], keep_result=False).result(timeout=600)
-
-        def client():
-            t_start = time.perf_counter()
-            for j in sel:
-                _wait_until(t_start + arrivals_all[j])
-                futures.append(srv.submit(f"m{int(pick_all[j])}", pools[int(pick_all[j])][:, :int(ks_all[j])],
-                                          keep_result=False))
-
-        th = threading.Thread(target=client)
-        th.start()
-        th.join()
-        for f in futures:
-            f.result(timeout=600)
-    gc.unfreeze()
+    try:
+        with srv:
+            for i in sorted(mine):   # warm every matrix's path once
+                srv.submit(f"m{i}", pools[i][:, :1], keep_result=False).result(timeout=600)
+            th = threading.Thread(target=client)
+            th.start()
+            th.join()
+            for f in futures:
+                f.result(timeout=600)
+    finally:
+        gc.unfreeze()
     out = dict(devices=len(srv.devices), matrices=len(mine), requests=len(sel), offered_req_per_s=rate,
                k=[k_lo, k_hi],
                matrices_per_device=[sum(1 for i in mine if srv.owner[f"m{i}"] == j) for j in range(len(srv.devices))],
@@ -489,27 +491,27 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
     # reach for its duration (a full collection over a large process can
     # stall the loop thread for a whole batch)
     futures = [None] * n_requests
-    gc.collect()
-    gc.freeze()
-    srv.start()
-    # warm the loop's batches once
-    srv.submit(names[pick[0]], Xs[0], keep_result=False).result(timeout=600)
-
     def client():
         t_start = time.perf_counter()
         for i in range(n_requests):
             _wait_until(t_start + arrivals[i])
             futures[i] = srv.submit(names[pick[i]], Xs[i], keep_result=False)
 
-    th = threading.Thread(target=client)
-    th.start()
-    th.join()
-    for f in futures:
-        f.result(timeout=600)
+    gc.collect()
+    gc.freeze()
+    try:
+        with srv:
+            # warm the loop's batches once
+            srv.submit(names[pick[0]], Xs[0], keep_result=False).result(timeout=600)
+            th = threading.Thread(target=client)
+            th.start()
+            th.join()
+            for f in futures:
+                f.result(timeout=600)
+            batches = srv.batches_run
+    finally:
+        gc.unfreeze()
     stats = latency_stats(futures)
-    batches = srv.batches_run
-    srv.stop()
-    gc.unfreeze()
     return dict(requests=n_requests, offered_req_per_s=rate, k=[k_lo, k_hi], value_type=value_type,
                 matrices=len(names), resident_gb=round(admitted_bytes / 1e9, 2),
                 served=dict(req_per_s=round(stats["req_per_s"], 1), p50_ms=round(stats["p50_ms"], 3),
