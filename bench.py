@@ -871,7 +871,7 @@ def run_sharded_serving(world: int, rank: int, dev, n_requests: int = 3000, rate
     total = float(count.item())
     return {"ranks": world, "matrices": len(hosts), "requests": int(total), "offered_req_per_s": rate, "k": [1, 8],
             "req_per_s": round(total / float(span.item()), 1) if span.item() > 0 else None,
-            "rank0": {k: res[k] for k in ("matrices", "requests", "served") if k in res},
+            "rank0": {k: res[k] for k in ("matrices", "requests", "served", "standalone", "allocator") if k in res},
             "note": "matrices placed whole (serving.place), each rank serves its own on its GPU; "
                     "req/s = all requests / slowest rank's span"}
 

@@ -353,6 +353,14 @@ def serving_matrices(count: int = 64, rows_lo: int = 10_000, rows_hi: int = 4_00
     return out
 
 
+def _alloc_counts(torch) -> dict:
+    """The caching allocator's device allocations, frees and retries so far
+    (a retry frees every cached block and synchronises the device)."""
+    st = torch.cuda.memory_stats()
+    return {"device_allocs": int(st.get("num_device_alloc", 0)), "device_frees": int(st.get("num_device_free", 0)),
+            "retries": int(st.get("num_alloc_retries", 0))}
+
+
 def _wait_until(t: float) -> None:
     """Sleep until perf_counter() reaches t. Sleeping (not spinning) leaves
     the interpreter lock to the serving loop's thread."""
@@ -422,6 +430,8 @@ def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000
 
     gc.collect()
     gc.freeze()
+    torch.cuda.empty_cache()
+    a0 = _alloc_counts(torch)
     try:
         with srv:
             for i in sorted(mine):   # warm every matrix's path once
@@ -433,11 +443,14 @@ def serve_sharded(hosts, devices, budget_per_device: int, n_requests: int = 2000
                 f.result(timeout=600)
     finally:
         gc.unfreeze()
+    a1 = _alloc_counts(torch)
     out = dict(devices=len(srv.devices), matrices=len(mine), requests=len(sel), offered_req_per_s=rate,
                k=[k_lo, k_hi],
                matrices_per_device=[sum(1 for i in mine if srv.owner[f"m{i}"] == j) for j in range(len(srv.devices))],
                requests_per_device=[sum(1 for j in sel if srv.owner[f"m{int(pick_all[j])}"] == d)
-                                    for d in range(len(srv.devices))])
+                                    for d in range(len(srv.devices))],
+               standalone=sum(1 for s in srv.servers for r in s.mats.values() if r.standalone),
+               allocator={k: a1[k] - a0[k] for k in a0})
     if futures:
         st = latency_stats(futures)
         reqs = [f.request for f in futures]
@@ -499,6 +512,8 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
 
     gc.collect()
     gc.freeze()
+    torch.cuda.empty_cache()   # blocks cached by earlier work go back; the stream's own allocations stay cached
+    a0 = _alloc_counts(torch)
     try:
         with srv:
             # warm the loop's batches once
@@ -511,6 +526,7 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
             batches = srv.batches_run
     finally:
         gc.unfreeze()
+    a1 = _alloc_counts(torch)
     stats = latency_stats(futures)
     return dict(requests=n_requests, offered_req_per_s=rate, k=[k_lo, k_hi], value_type=value_type,
                 matrices=len(names), resident_gb=round(admitted_bytes / 1e9, 2),
@@ -518,4 +534,6 @@ def serve(mats, budget_bytes: int, n_requests: int = 1000, rate: float = 20_000.
                             p99_ms=round(stats["p99_ms"], 3), batches=batches - 1),
                 sequential=dict(req_per_s=round(n_requests / span_seq, 1), p50_ms=round(float(np.percentile(lat_seq, 50)), 3),
                                 p99_ms=round(float(np.percentile(lat_seq, 99)), 3)),
-                speedup=round(stats["req_per_s"] / (n_requests / span_seq), 2))
+                speedup=round(stats["req_per_s"] / (n_requests / span_seq), 2),
+                standalone=sum(1 for nm in names if srv.mats[nm].standalone),
+                allocator={k: a1[k] - a0[k] for k in a0})
