@@ -946,24 +946,26 @@ def run_extras(args, items, mats, peak):
         y = torch.zeros(it["rows"], device="cuda")
         for vt in ("bf16", "f16"):
             p = m.pack(vt)
-            m.spmv(x, y, 1.0, 0.0, packed=p)
+            m.spmv(x, y, 1.0, 0.0, packed=p, **it["kw"])
             err = csr64[it["matrix"]].error(x[:, None], y[:, None])
             for _ in range(3):
-                m.spmv(x, y, 1.0, 0.0, packed=p)
+                m.spmv(x, y, 1.0, 0.0, packed=p, **it["kw"])
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(20):
-                m.spmv(x, y, 1.0, 0.0, packed=p)
+                m.spmv(x, y, 1.0, 0.0, packed=p, **it["kw"])
             e1.record()
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / 20
-            ab = W.matrix_bytes(m, vt) + 4 * it["cols"] + 8 * it["rows"]
-            spmv16[f"{key}/{vt}"] = {"ms": round(ms, 5), "gflops": round(2 * it["nnz"] / (ms * 1e-3) / 1e9, 1),
-                                     "gbs": round(ab / (ms * 1e-3) / 1e9, 1), "frac": round(ab / (ms * 1e-3) / 1e9 / peak, 3),
-                                     "alg_bytes": ab, "err_fp64": err}
+            res = {"ms": round(ms, 5), "gflops": round(2 * it["nnz"] / (ms * 1e-3) / 1e9, 1), "err_fp64": err}
+            if it["kw"].get("variant") != "planned":   # SELL through its plan reads less than its stored bytes
+                ab = W.matrix_bytes(m, vt) + 4 * it["cols"] + 8 * it["rows"]
+                res.update(gbs=round(ab / (ms * 1e-3) / 1e9, 1), frac=round(ab / (ms * 1e-3) / 1e9 / peak, 3), alg_bytes=ab)
+            spmv16[f"{key}/{vt}"] = res
             del p
     out["spmv16"] = {"note": "y = A x with values stored as BF16 / FP16 (per-row power-of-two scale, FP32 "
-                             "accumulation) in each format's own kernel; GB/s over the bytes at 2-byte values",
+                             "accumulation) in each format's own kernel (SELL-32 through its plan, as in the sweep); "
+                             "GB/s over the stored bytes at 2-byte values (none for the planned SELL, which reads less)",
                      "results": spmv16}
     entries = [(k, by_key[k]["dev"], csr64[by_key[k]["matrix"]]) for k in ("dia", "csr_chunk", "bcsr", "sbell")
                if k in by_key]

@@ -254,6 +254,7 @@ def _declare(lib):
         "clspmv_spmv_packed": (I32, [I32, VP, I32, VP, VP, VP, VP, VP, f32, f32, VP]),
         "clspmv_sell_plan_create": (I32, [S["sell"], P(VP)]),
         "clspmv_sell_plan_spmv_f32": (I32, [S["sell"], VP, VP, VP, f32, f32, VP]),
+        "clspmv_sell_plan_spmv_packed": (I32, [S["sell"], VP, I32, VP, VP, VP, VP, f32, f32, VP]),
         "clspmv_sell_plan_entries": (C.c_longlong, [VP]),
         "clspmv_sell_plan_items": (C.c_longlong, [VP]),
         "clspmv_sell_plan_sector_bytes": (C.c_longlong, [VP]),

@@ -490,7 +490,8 @@ __device__ __forceinline__ void sell_tail_cta(const SellArgs& a, const int* __re
 // compact array (tail_col[tail_off[it] + k - item.y]): the lanes of a warp
 // read an item's column ids from consecutive words, and only its values
 // from the slice's stride-sh column-major layout.
-__device__ __forceinline__ void sell_tail_compact_cta(const SellArgs& a, const int* __restrict__ rlen,
+template <class V = float>
+__device__ __forceinline__ void sell_tail_compact_cta(const SellArgsT<V>& a, const int* __restrict__ rlen,
                                                       const int2* __restrict__ items, const int* __restrict__ tail_off,
                                                       const int* __restrict__ tail_col, long long nitems, int cta, int ncta)
 {
@@ -507,10 +508,10 @@ __device__ __forceinline__ void sell_tail_compact_cta(const SellArgs& a, const i
         float acc = 0.f;
 #pragma unroll 4
         for (int k = item.y + lane; k < item.y + n; k += 32)
-            acc = fmaf(ld_stream_f(a.data + base + (size_t)k * sh, pe), ld_x(a.x + ld_stream_i(tc + k, pe), pl), acc);
+            acc = fmaf(ldv(a.data + base + (size_t)k * sh, pe), ld_x(a.x + ld_stream_i(tc + k, pe), pl), acc);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(kFull, acc, off);
-        if (lane == 0) atomicAdd(a.y + item.x, a.alpha * acc);
+        if (lane == 0) atomicAdd(a.y + item.x, row_alpha(a.alpha, scl(a), item.x) * acc);
     }
 }
 
@@ -528,8 +529,8 @@ __device__ __forceinline__ void sell_tail_compact_cta(const SellArgs& a, const i
 // only the first head[s+1] - head[s] columns of slice s are walked: the
 // columns up to its second-longest row, the rest of its longest row being
 // left to sell_tail_cta.
-template <int Q, bool ATOMIC_ALL>
-__device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __restrict__ rlen, int cta, int ncta,
+template <int Q, bool ATOMIC_ALL, class V = float>
+__device__ __forceinline__ void sell_masked_cta(const SellArgsT<V>& a, const int* __restrict__ rlen, int cta, int ncta,
                                                 const int* __restrict__ head = nullptr)
 {
     constexpr int G = 32 / Q;             // columns per warp step
@@ -583,7 +584,7 @@ __device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __
                 if (cc < klim) {
                     const size_t base = (size_t)(sbase + cc * sh) + 4 * q;
                     const int4 cv = ld_stream_i4(a.col + base, pe);
-                    const float4 v = ld_stream_f4(a.data + base, pe);
+                    const float4 v = ldv4(a.data + base, pe);
                     acc[0] = fmaf(v.x, ld_x(a.x + cv.x, pl), acc[0]);
                     acc[1] = fmaf(v.y, ld_x(a.x + cv.y, pl), acc[1]);
                     acc[2] = fmaf(v.z, ld_x(a.x + cv.z, pl), acc[2]);
@@ -600,8 +601,9 @@ __device__ __forceinline__ void sell_masked_cta(const SellArgs& a, const int* __
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
                     if (row0 + i < a.rows) {
-                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += a.alpha * acc[i];
-                        else atomicAdd(a.y + row0 + i, a.alpha * acc[i]);
+                        const float al = row_alpha(a.alpha, scl(a), row0 + i);
+                        if (whole && !ATOMIC_ALL) a.y[row0 + i] += al * acc[i];
+                        else atomicAdd(a.y + row0 + i, al * acc[i]);
                     }
                 }
             }

@@ -114,10 +114,11 @@ __global__ void __launch_bounds__(kBlock) k_sell_rlen(const int* __restrict__ sl
 // power-law SELL-32 heads, 0.273 ms for the planned SpMV against 0.292 at 6
 // CTAs (40 registers) and 0.318 at 4 (62 registers): the walk is latency
 // bound, so warps in flight count more than the spills
-template <int Q, bool A>
-__global__ void __launch_bounds__(kBlock, 8) k_sell_masked(SellArgs a, const int* __restrict__ rlen, const int* __restrict__ head)
+template <int Q, bool A, class V = float>
+__global__ void __launch_bounds__(kBlock, 8) k_sell_masked(SellArgsT<V> a, const int* __restrict__ rlen,
+                                                           const int* __restrict__ head)
 {
-    sell_masked_cta<Q, A>(a, rlen, blockIdx.x, gridDim.x, head);
+    sell_masked_cta<Q, A, V>(a, rlen, blockIdx.x, gridDim.x, head);
 }
 template <bool A>
 __global__ void __launch_bounds__(kBlock) k_sell_head(SellArgs a, const int* __restrict__ rlen)
@@ -131,11 +132,12 @@ __global__ void __launch_bounds__(kBlock) k_sell_tail(SellArgs a, const int* __r
     sell_tail_cta(a, rlen, items, nitems, blockIdx.x, gridDim.x);
 }
 
-__global__ void __launch_bounds__(kBlock) k_sell_tail_compact(SellArgs a, const int* __restrict__ rlen,
+template <class V = float>
+__global__ void __launch_bounds__(kBlock) k_sell_tail_compact(SellArgsT<V> a, const int* __restrict__ rlen,
                                                               const int2* __restrict__ items, const int* __restrict__ tail_off,
                                                               const int* __restrict__ tail_col, long long nitems)
 {
-    sell_tail_compact_cta(a, rlen, items, tail_off, tail_col, nitems, blockIdx.x, gridDim.x);
+    sell_tail_compact_cta<V>(a, rlen, items, tail_off, tail_col, nitems, blockIdx.x, gridDim.x);
 }
 
 // tail_col[tail_off[t] + j] = column id of entry item.y + j of split item t
@@ -517,7 +519,7 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
         });
         if (rc || !head || nsplit == 0) return rc;
         if (tail_col)
-            k_sell_tail_compact<<<persistent_grid(k_sell_tail_compact, nsplit, kBlock / 32), kBlock, 0, st>>>(
+            k_sell_tail_compact<float><<<persistent_grid(k_sell_tail_compact<float>, nsplit, kBlock / 32), kBlock, 0, st>>>(
                 a, rlen, split_items, tail_off, tail_col, nsplit);
         else
             k_sell_tail<<<persistent_grid(k_sell_tail, nsplit, kBlock / 32), kBlock, 0, st>>>(a, rlen, split_items, nsplit);
@@ -528,6 +530,34 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
     int rc = after_launch(1);
     if (rc || nitems == 0) return rc;
     k_sell_tail<<<persistent_grid(k_sell_tail, nitems, kBlock / 32), kBlock, 0, st>>>(a, rlen, items, nitems);
+    return after_launch(1);
+}
+
+// The planned walk with 16-bit values (per-row scales): slice heights
+// 4..128 with the heads / compact tails split; otherwise the padded read.
+template <class V>
+int launch_sell_planned_packed(const clspmv_sell_f32* m, const V* data, const float* scale, const int* rlen, const int* head,
+                               const int2* split_items, long long nsplit, const int* tail_off, const int* tail_col,
+                               const float* x, float* y, float alpha, float beta, cudaStream_t st)
+{
+    if (!m || !x || !y || !m->sell_slice_ptr || !rlen || !data || !scale) return CLSPMV_ERR_ARG;
+    const int rows = m->matinfo.height;
+    if (rows <= 0) return CLSPMV_OK;
+    const int sh = (int)m->sell_slice_height;
+    if (!(head && tail_col && aligned16(m->sell_col_id) && aligned_v4(data) && aligned16(rlen) &&
+          (sh == 4 || sh == 8 || sh == 16 || sh == 32 || sh == 64 || sh == 128)))
+        return launch_sell_v<V>(m, data, scale, x, y, alpha, beta, st, false);
+    SellArgsT<V> a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, data, x, y, alpha, 1.0f, scale};
+    int rc = prescale(y, rows, beta, st);
+    if (rc) return rc;
+    rc = dispatch_lanes(sh / 4, [&](auto q) {
+        constexpr int Q = decltype(q)::value;
+        k_sell_masked<Q, false, V><<<persistent_grid(k_sell_masked<Q, false, V>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen, head);
+        return after_launch(1);
+    });
+    if (rc || nsplit == 0) return rc;
+    k_sell_tail_compact<V><<<persistent_grid(k_sell_tail_compact<V>, nsplit, kBlock / 32), kBlock, 0, st>>>(
+        a, rlen, split_items, tail_off, tail_col, nsplit);
     return after_launch(1);
 }
 
@@ -1053,6 +1083,21 @@ int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* 
     if (!p) return CLSPMV_ERR_ARG;
     return launch_sell_planned(m, p->rlen, p->items, p->nitems, p->split ? p->head : nullptr, p->split_items, p->nsplit,
                                p->tail_off, p->compact ? p->tail_col : nullptr, x, y, alpha, beta, S(s), false);
+}
+
+int clspmv_sell_plan_spmv_packed(const clspmv_sell_f32* m, const clspmv_sell_plan* p, int value_type, const void* values,
+                                 const float* row_scale, const float* x, float* y, float alpha, float beta, clspmv_stream_t s)
+{
+    if (!p) return CLSPMV_ERR_ARG;
+    const int* head = p->split ? p->head : nullptr;
+    const int* tc = p->compact ? p->tail_col : nullptr;
+    if (value_type == CLSPMV_VALUES_BF16)
+        return launch_sell_planned_packed(m, static_cast<const __nv_bfloat16*>(values), row_scale, p->rlen, head,
+                                          p->split_items, p->nsplit, p->tail_off, tc, x, y, alpha, beta, S(s));
+    if (value_type == CLSPMV_VALUES_F16)
+        return launch_sell_planned_packed(m, static_cast<const __half*>(values), row_scale, p->rlen, head, p->split_items,
+                                          p->nsplit, p->tail_off, tc, x, y, alpha, beta, S(s));
+    return CLSPMV_ERR_ARG;
 }
 
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* p) { return p ? p->entries : -1; }

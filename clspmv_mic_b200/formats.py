@@ -342,6 +342,12 @@ class DeviceMatrix:
                                                      self.chunk_plan(stream).data_ptr(), x.data_ptr(), y.data_ptr(),
                                                      alpha, beta, s), "csr_chunk_spmv_packed")
                 return
+            if self.fmt == "sell" and variant == "planned":
+                check(L.clspmv_sell_plan_spmv_packed(C.byref(self.struct), self.sell_plan(),
+                                                     _abi.VALUE_TYPES[packed.value_type], packed.values.data_ptr(),
+                                                     packed.row_scale.data_ptr(), x.data_ptr(), y.data_ptr(), alpha, beta,
+                                                     s), "sell_plan_spmv_packed")
+                return
             plan = self.merge_plan(stream).data_ptr() if self.fmt == "csr" else None
             check(L.clspmv_spmv_packed(_abi.FORMAT_IDS[self.fmt], C.byref(self.struct), _abi.VALUE_TYPES[packed.value_type],
                                        packed.values.data_ptr(), packed.row_scale.data_ptr(), plan, x.data_ptr(),

@@ -461,6 +461,12 @@ typedef struct clspmv_sell_plan clspmv_sell_plan;
 int clspmv_sell_plan_create(const clspmv_sell_f32* dev, clspmv_sell_plan** out);
 int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* dev, const clspmv_sell_plan* plan, const float* x, float* y,
                               float alpha, float beta, clspmv_stream_t stream);
+/* The planned SpMV with 16-bit values (clspmv_pack_values of this matrix:
+ * CLSPMV_VALUES_BF16 / _F16 and the per-row scales); slice heights other than
+ * 4..128 (powers of two) take the padded 16-bit read. */
+int clspmv_sell_plan_spmv_packed(const clspmv_sell_f32* dev, const clspmv_sell_plan* plan, int value_type,
+                                 const void* values, const float* row_scale, const float* x, float* y, float alpha,
+                                 float beta, clspmv_stream_t stream);
 /* stored entries the plan reads (real entries and explicit zeros before them), and its tail items */
 long long clspmv_sell_plan_entries(const clspmv_sell_plan* plan);
 long long clspmv_sell_plan_items(const clspmv_sell_plan* plan);

@@ -175,6 +175,35 @@ def test_spmv_packed_dedicated(name, fmt, args, value_type):
 
 
 @pytest.mark.parametrize("value_type", ["bf16", "f16"])
+@pytest.mark.parametrize("name,sh", [("powerlaw3k", 32), ("powerlaw3k", 8), ("powerlaw3k", 128), ("random_empty_rows", 32),
+                                     ("random_empty_rows", 20), ("one_entry", 4)])
+def test_sell_planned_packed(name, sh, value_type):
+    """SELL through its length plan with 16-bit values (heads column-balanced,
+    long tails from the compact column ids; slice height 20 takes the padded
+    16-bit read) against the FP64 oracle at the 16-bit bound, and against
+    the padded 16-bit read."""
+    import torch
+    coo = coo_of(name)
+    m, n = coo.shape
+    dev = device_of(coo, "sell", sh)
+    p = dev.pack(value_type)
+    x = synth.x_vector(n, seed=6)
+    y0 = np.random.default_rng(5).uniform(-1, 1, m).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (-0.5, 1.5)]:
+        ys = {}
+        for variant in ("planned", "padded"):
+            xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+            dev.spmv(xd, yd, alpha, beta, packed=p, variant=variant)
+            torch.cuda.synchronize()
+            ys[variant] = yd.cpu().numpy().astype(np.float64)
+        ref, bound = spmm_reference(coo, x[:, None], y0[:, None], alpha, beta)
+        lim = RTOL[value_type] * bound[:, 0] + 1e-6 * abs(beta) * np.abs(y0) + 1e-30
+        for variant, y in ys.items():
+            assert np.all(np.abs(y - ref[:, 0]) <= lim), (name, sh, value_type, variant)
+        assert np.all(np.abs(ys["planned"] - ys["padded"]) <= 2e-5 * bound[:, 0] + 1e-6 * abs(beta) * np.abs(y0) + 1e-30)
+
+
+@pytest.mark.parametrize("value_type", ["bf16", "f16"])
 @pytest.mark.parametrize("variant", ["chunk", "merge"])
 def test_csr_packed_both_kernels(value_type, variant):
     """16-bit CSR values in the chunked and the merge-path kernel."""
