@@ -270,12 +270,32 @@ int resident_ctas(const void* kernel, int smem_bytes)
 }
 
 // Grid for a persistent launch: all resident CTAs, but no more CTAs than
-// passes of work.
+// passes of work. With `whole`, when the work takes more than one wave of
+// resident CTAs, as many CTAs as give every CTA the same whole number of
+// passes (the last pass of a share otherwise runs part-empty on every CTA):
+// measured on B200 over the 27-point stencil 128^3, DIA 53.7 -> 49.6 us and
+// BDIA 53.3 -> 51.2 us; the gather-bound and block kernels lose 1-4 % with
+// it, so only the diagonal formats take it. CLSPMV_WHOLE_PASSES=0|1
+// overrides it for every kernel (measurements).
+int whole_passes_override()
+{
+    static const int v = [] {
+        const char* e = getenv("CLSPMV_WHOLE_PASSES");
+        return e ? atoi(e) : -1;
+    }();
+    return v;
+}
+
 template <class K>
-unsigned persistent_grid(K kernel, long long units, long long units_per_pass, int smem_bytes = 0)
+unsigned persistent_grid(K kernel, long long units, long long units_per_pass, int smem_bytes = 0, bool whole = false)
 {
     const long long passes = (units + units_per_pass - 1) / units_per_pass;
     const long long res = resident_ctas(reinterpret_cast<const void*>(kernel), smem_bytes);
+    const int ov = whole_passes_override();
+    if ((ov >= 0 ? ov != 0 : whole) && passes > res) {
+        const long long k = (passes + res - 1) / res;
+        return (unsigned)((passes + k - 1) / k);
+    }
     return (unsigned)std::max(1LL, std::min(passes, res));
 }
 
@@ -363,7 +383,7 @@ int launch_dia_v(const clspmv_dia_f32* m, const V* data, const float* scale, con
             return launch_diag_bulk(rows, m->matinfo.width, m->dia_num, m->dia_length_aligned, m->dia_offsets, nullptr, 0,
                                     data, x, y, alpha, beta, st);
     }
-    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kDiaRowsPerPass), kBlock, 0, st>>>(a); };
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kDiaRowsPerPass, 0, true), kBlock, 0, st>>>(a); };
     if (atomic) {
         if (form == 3) go(k_dia<true, V, 3>);
         else if (form == 2) go(k_dia_occ<true, V, 1>);
@@ -399,7 +419,7 @@ int launch_bdia_v(const clspmv_bdia_f32* m, const V* data, const float* scale, c
             return launch_diag_bulk(rows, m->matinfo.width, 0, m->bdia_length_aligned, m->bdia_offsets, m->bdia_bptr,
                                     m->bdia_band_num, data, x, y, alpha, beta, st);
     }
-    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kBdiaRowsPerPass), kBlock, 0, st>>>(a); };
+    auto go = [&](auto kernel) { kernel<<<persistent_grid(kernel, rows, kBdiaRowsPerPass, 0, true), kBlock, 0, st>>>(a); };
     if (atomic) {
         if (form == 2) go(k_bdia_occ<true, V, true>);
         else if (form == 1) go(k_bdia<true, V, true>);
