@@ -274,9 +274,9 @@ int resident_ctas(const void* kernel, int smem_bytes)
 // resident CTAs, as many CTAs as give every CTA the same whole number of
 // passes (the last pass of a share otherwise runs part-empty on every CTA):
 // measured on B200 over the 27-point stencil 128^3, DIA 53.7 -> 49.6 us and
-// BDIA 53.3 -> 51.2 us; the gather-bound and block kernels lose 1-4 % with
-// it, so only the diagonal formats take it. CLSPMV_WHOLE_PASSES=0|1
-// overrides it for every kernel (measurements).
+// BDIA 53.3 -> 51.2 us, and over the 4x4-block matrix SBELL 55.6 -> 53.5 us;
+// the gather-bound kernels and BELL lose 1-4 % with it and keep the full
+// grid. CLSPMV_WHOLE_PASSES=0|1 overrides it for every kernel (measurements).
 int whole_passes_override()
 {
     static const int v = [] {
@@ -768,7 +768,7 @@ int launch_sbell_v(const clspmv_sbell_f32* m, const V* data, const float* scale,
     return dispatch_block(m->sbell_bwidth, m->sbell_bheight, [&](auto bw4, auto bh) {
         constexpr int BW4 = decltype(bw4)::value, BH = decltype(bh)::value;
         if (atomic) k_sbell<BW4, BH, true, V><<<persistent_grid(k_sbell<BW4, BH, true, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
-        else k_sbell<BW4, BH, false, V><<<persistent_grid(k_sbell<BW4, BH, false, V>, a.nbrow, kBlock), kBlock, 0, st>>>(a);
+        else k_sbell<BW4, BH, false, V><<<persistent_grid(k_sbell<BW4, BH, false, V>, a.nbrow, kBlock, 0, true), kBlock, 0, st>>>(a);
         return after_launch(1);
     });
 }
