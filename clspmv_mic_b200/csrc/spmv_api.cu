@@ -140,6 +140,37 @@ __global__ void __launch_bounds__(kBlock) k_sell_tail_compact(SellArgsT<V> a, co
     sell_tail_compact_cta<V>(a, rlen, items, tail_off, tail_col, nitems, blockIdx.x, gridDim.x);
 }
 
+// The planned SELL walk in one launch: CTAs [0, ntail) take the long rows'
+// tails, the rest the slice heads (every head update atomic, since a tail
+// CTA may add to the same row meanwhile), so the latency-bound head walk and
+// the bandwidth-bound tails share the SMs instead of running one after the
+// other.
+template <int Q, class V>
+__global__ void __launch_bounds__(kBlock, 8) k_sell_planned_one(SellArgsT<V> a, const int* __restrict__ rlen,
+                                                                const int* __restrict__ head, const int2* __restrict__ items,
+                                                                const int* __restrict__ tail_off,
+                                                                const int* __restrict__ tail_col, long long nitems, int ntail)
+{
+    if ((int)blockIdx.x < ntail)
+        sell_tail_compact_cta<V>(a, rlen, items, tail_off, tail_col, nitems, blockIdx.x, ntail);
+    else
+        sell_masked_cta<Q, true, V>(a, rlen, blockIdx.x - ntail, gridDim.x - ntail, head);
+}
+
+// Share of the one launch's CTAs on the tails, per mille: measured on B200
+// over the power-law SELL-32 (0.271 ms in two launches), 0.240 ms at 180,
+// 0.250 at 250-300, 0.268 at 400, 0.308 at 550 (the latency-bound heads
+// want most of the warps). CLSPMV_SELL_ONE overrides it (0: two launches;
+// measurements).
+int sell_one_permille()
+{
+    static const int v = [] {
+        const char* e = getenv("CLSPMV_SELL_ONE");
+        return e ? atoi(e) : 180;
+    }();
+    return v;
+}
+
 // tail_col[tail_off[t] + j] = column id of entry item.y + j of split item t
 __global__ void k_sell_tail_cols(const int2* __restrict__ items, const int* __restrict__ tail_off, long long nitems,
                                  const int* __restrict__ slice_ptr, const int* __restrict__ col, int sh, int* tail_col)
@@ -506,13 +537,33 @@ int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha,
     return launch_sell_v<float>(m, m ? m->sell_data : nullptr, nullptr, x, y, alpha, beta, st, atomic);
 }
 
+// Launches the planned walk as one kernel (k_sell_planned_one): tail CTAs
+// by sell_one_permille, but no more than the tail items keep busy (a CTA
+// walks 8 items at a time).
+template <class V>
+int launch_sell_one(const SellArgsT<V>& a, int sh, const int* rlen, const int* head, const int2* split_items,
+                    long long nsplit, const int* tail_off, const int* tail_col, cudaStream_t st)
+{
+    return dispatch_lanes(sh / 4, [&](auto q) {
+        constexpr int Q = decltype(q)::value;
+        auto k = k_sell_planned_one<Q, V>;
+        const unsigned grid = persistent_grid(k, 1LL << 40, 1);
+        long long ntail = (long long)grid * sell_one_permille() / 1000;
+        ntail = std::min(ntail, (nsplit + kBlock / 32 - 1) / (kBlock / 32));
+        ntail = std::max(1LL, std::min((long long)grid - 1, ntail));
+        k<<<grid, kBlock, 0, st>>>(a, rlen, head, split_items, tail_off, tail_col, nsplit, (int)ntail);
+        return after_launch(1);
+    });
+}
+
 // Padding-free SELL. Power-of-two slice heights with 16-byte aligned arrays:
 // the column-balanced walk with each lane's loads cut at its rows' real
 // length, either over every column of every slice (head == nullptr), or over
 // each slice's columns up to its second-longest row (head: prefix table of
-// those widths) followed by the longest rows' tails, a warp per item of up to
-// kSellTailCols entries (split_items). Other slice heights: each row's first
-// kSellHead entries with a thread per row, then the tails (items).
+// those widths) and the longest rows' tails, a warp per item of up to
+// kSellTailCols entries (split_items); with the tails' compact column ids
+// both run in one launch (launch_sell_one). Other slice heights: each row's
+// first kSellHead entries with a thread per row, then the tails (items).
 int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* items, long long nitems, const int* head,
                         const int2* split_items, long long nsplit, const int* tail_off, const int* tail_col,
                         const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic)
@@ -531,6 +582,8 @@ int launch_sell_planned(const clspmv_sell_f32* m, const int* rlen, const int2* i
             if (rc) return rc;
         }
         a.beta = 1.0f;
+        if (head && tail_col && nsplit > 0 && sell_one_permille() > 0)
+            return launch_sell_one<float>(a, sh, rlen, head, split_items, nsplit, tail_off, tail_col, st);
         int rc = dispatch_lanes(sh / 4, [&](auto q) {
             constexpr int Q = decltype(q)::value;
             if (atomic) k_sell_masked<Q, true><<<persistent_grid(k_sell_masked<Q, true>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen, head);
@@ -570,6 +623,8 @@ int launch_sell_planned_packed(const clspmv_sell_f32* m, const V* data, const fl
     SellArgsT<V> a{rows, sh, m->sell_slice_num, m->sell_slice_ptr, m->sell_col_id, data, x, y, alpha, 1.0f, scale};
     int rc = prescale(y, rows, beta, st);
     if (rc) return rc;
+    if (nsplit > 0 && sell_one_permille() > 0)
+        return launch_sell_one<V>(a, sh, rlen, head, split_items, nsplit, tail_off, tail_col, st);
     rc = dispatch_lanes(sh / 4, [&](auto q) {
         constexpr int Q = decltype(q)::value;
         k_sell_masked<Q, false, V><<<persistent_grid(k_sell_masked<Q, false, V>, 1LL << 40, 1), kBlock, 0, st>>>(a, rlen, head);

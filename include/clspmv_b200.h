@@ -452,7 +452,8 @@ int clspmv_sell_spmv_f32(const clspmv_sell_f32* dev, const float* x, float* y,
  * row's entries past it go to a warp per 256 entries, which reads their
  * column ids from a compact copy the plan made (structure only: the values
  * stay in the matrix, so the plan holds while they change, not while the
- * column ids do) and their values in place; other slice heights sum each row's first
+ * column ids do) and their values in place, the heads and the tails in one
+ * launch (about a fifth of its CTAs on the tails); other slice heights sum each row's first
  * 32 entries with a thread per row and longer rows' tails with a warp per
  * 256 entries. Same y as clspmv_sell_spmv_f32 up to summation order, except
  * where x holds Inf or NaN at a skipped padding column. No counterpart in
