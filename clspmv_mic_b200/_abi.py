@@ -239,6 +239,7 @@ def _declare(lib):
         "clspmv_cocktail_iterate_f32": (I32, [VP, VP, VP, f32, f32, I32, VP]),
         "clspmv_cocktail_set_schedule": (I32, [VP, I32]),
         "clspmv_cocktail_fused_items": (I32, [VP]),
+        "clspmv_cocktail_sell_planned": (I32, [VP]),
         "clspmv_cocktail_set_csr_lanes": (I32, [VP, I32]),
         "clspmv_cocktail_free": (I32, [VP]),
         "clspmv_run_method_f32": (I32, [S["coo"], I32, I32, I32, P(BenchResult)]),

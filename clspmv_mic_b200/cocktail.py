@@ -139,6 +139,11 @@ class DeviceCocktail:
         check(lib().clspmv_cocktail_set_csr_lanes(self.handle, int(lanes)), "cocktail_set_csr_lanes")
 
     @property
+    def sell_planned(self) -> bool:
+        """The SELL part runs through a length plan (clspmv_cocktail_sell_planned)."""
+        return lib().clspmv_cocktail_sell_planned(self.handle) == 1
+
+    @property
     def fused_items(self) -> int:
         """Work-list entries of the fused schedule (0: the handle has none)."""
         return int(lib().clspmv_cocktail_fused_items(self.handle))

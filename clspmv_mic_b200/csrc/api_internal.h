@@ -17,6 +17,8 @@ int launch_dia(const clspmv_dia_f32* m, const float* x, float* y, float alpha, f
 int launch_bdia(const clspmv_bdia_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_ell(const clspmv_ell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_sell(const clspmv_sell_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
+int launch_sell_plan(const clspmv_sell_f32* m, const clspmv_sell_plan* plan, const float* x, float* y, float alpha,
+                     float beta, cudaStream_t st, bool atomic);
 int launch_csr_scalar(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);
 int launch_csr_vector(const clspmv_csr_f32* m, const float* x, float* y, float alpha, float beta, int tpr, cudaStream_t st, bool atomic);
 int launch_csr_merge(const clspmv_csr_f32* m, const int* tc, const float* x, float* y, float alpha, float beta, cudaStream_t st, bool atomic);

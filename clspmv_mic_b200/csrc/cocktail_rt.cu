@@ -27,6 +27,7 @@ struct clspmv_cocktail_handle {
     int* chunk_plan = nullptr;        // first row of every nonzero chunk of the CSR part
     int nparts = 0;
     FusedPlan* fused = nullptr;       // one persistent launch over all parts (two or more parts)
+    clspmv_sell_plan* sell_plan = nullptr;   // the SELL part's length plan, when it reads well under the stored slots
     int schedule = CLSPMV_SCHEDULE_AUTO;
     int csr_lanes = 0;                // CSR part: 0 nonzero chunks, T > 0 CSR-vector with T lanes per row
     cudaStream_t streams[9] = {};
@@ -44,6 +45,16 @@ struct clspmv_cocktail_handle {
 namespace {
 
 enum Part { P_BDIA, P_DIA, P_SBELL, P_BELL, P_BCSR, P_SELL, P_ELL, P_CSR, P_COO, P_COUNT };
+
+// CLSPMV_COCKTAIL_SELL_PLAN=0 keeps the padded SELL read for SELL parts (measurements)
+bool sell_plan_disabled()
+{
+    static const bool v = [] {
+        const char* e = getenv("CLSPMV_COCKTAIL_SELL_PLAN");
+        return e && atoi(e) == 0;
+    }();
+    return v;
+}
 
 bool uses(const clspmv_cocktail_f32& c, int p)
 {
@@ -71,7 +82,9 @@ int launch_part(const clspmv_cocktail_handle* h, int p, const float* x, float* y
         case P_SBELL: return launch_sbell(&d.sbell, x, y, alpha, beta, st, atomic);
         case P_BELL: return launch_b4ell(&d.bell, x, y, alpha, beta, st, atomic);
         case P_BCSR: return launch_b4csr(&d.bcsr, x, y, alpha, beta, st, atomic);
-        case P_SELL: return launch_sell(&d.sell, x, y, alpha, beta, st, atomic);
+        case P_SELL:
+            if (h->sell_plan) return launch_sell_plan(&d.sell, h->sell_plan, x, y, alpha, beta, st, atomic);
+            return launch_sell(&d.sell, x, y, alpha, beta, st, atomic);
         case P_ELL: return launch_ell(&d.ell, x, y, alpha, beta, st, atomic);
         case P_CSR:
             if (h->csr_lanes > 0) return launch_csr_vector(&d.csr, x, y, alpha, beta, h->csr_lanes, st, atomic);
@@ -99,6 +112,7 @@ void release(clspmv_cocktail_handle* h)
         if (h->join[i]) cudaEventDestroy(h->join[i]);
     }
     if (h->fork) cudaEventDestroy(h->fork);
+    if (h->sell_plan) clspmv_sell_plan_free(h->sell_plan);
     if (h->fused) fused_plan_free(h->fused);
     if (h->iter_exec) cudaGraphExecDestroy(h->iter_exec);
     if (h->cap) cudaStreamDestroy(h->cap);
@@ -185,6 +199,17 @@ int clspmv_cocktail_upload_f32(const clspmv_cocktail_f32* host, clspmv_cocktail_
     UP(ifusecsr, csr, clspmv_upload_csr_f32)
     UP(ifusecoo, coo, clspmv_upload_coo_f32)
 #undef UP
+    if (!rc && d.ifusesell && !sell_plan_disabled()) {
+        // SELL parts of uneven rows (slices padded to their longest row) take
+        // the padding-free walk when its lines come to under 3/4 of the slots
+        clspmv_sell_plan* sp = nullptr;
+        if (clspmv_sell_plan_create(&d.sell, &sp) == CLSPMV_OK) {
+            const long long slots = 8LL * (c.sell.sell_slice_ptr ? c.sell.sell_slice_ptr[c.sell.sell_slice_num] : 0);
+            if (clspmv_sell_plan_line_bytes(sp) < slots * 3 / 4) h->sell_plan = sp;
+            else clspmv_sell_plan_free(sp);
+        }
+        cudaGetLastError();
+    }
     if (!rc && d.ifusecsr) {
         const int nplan = clspmv_csr_chunk_plan_size(d.csr.matinfo.nnz);
         rc = cuda_status(cudaMalloc(&h->chunk_plan, sizeof(int) * (size_t)(nplan > 0 ? nplan : 1)));
@@ -270,6 +295,8 @@ int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule)
 }
 
 int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h) { return h ? fused_plan_items(h->fused) : -1; }
+
+int clspmv_cocktail_sell_planned(const clspmv_cocktail_handle* h) { return h ? (h->sell_plan != nullptr) : -1; }
 
 int clspmv_cocktail_set_csr_lanes(clspmv_cocktail_handle* h, int lanes)
 {

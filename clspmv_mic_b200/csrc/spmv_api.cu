@@ -1152,6 +1152,22 @@ int clspmv_sell_plan_create(const clspmv_sell_f32* m, clspmv_sell_plan** out)
     return CLSPMV_OK;
 }
 
+}  // extern "C"
+
+namespace clspmv {
+// The planned walk for a caller that already applied beta and adds into y
+// with the other parts of a Cocktail matrix (atomic = true).
+int launch_sell_plan(const clspmv_sell_f32* m, const clspmv_sell_plan* p, const float* x, float* y, float alpha, float beta,
+                     cudaStream_t st, bool atomic)
+{
+    if (!p) return CLSPMV_ERR_ARG;
+    return launch_sell_planned(m, p->rlen, p->items, p->nitems, p->split ? p->head : nullptr, p->split_items, p->nsplit,
+                               p->tail_off, p->compact ? p->tail_col : nullptr, x, y, alpha, beta, st, atomic);
+}
+}  // namespace clspmv
+
+extern "C" {
+
 int clspmv_sell_plan_spmv_f32(const clspmv_sell_f32* m, const clspmv_sell_plan* p, const float* x, float* y, float alpha,
                               float beta, clspmv_stream_t s)
 {

@@ -676,6 +676,11 @@ int clspmv_cocktail_set_schedule(clspmv_cocktail_handle* h, int schedule);
 /* Work-list entries of the fused schedule, 0 when the handle has none (one
  * part, or a part the fused kernel does not cover). */
 int clspmv_cocktail_fused_items(const clspmv_cocktail_handle* h);
+/* 1 when the SELL part runs through a length plan (made at upload when the
+ * plan's line bytes come to under 3/4 of the part's stored slots: slices
+ * padded to a few long rows; clspmv_sell_plan_create), 0 when it takes the
+ * padded read, -1 for a NULL handle. */
+int clspmv_cocktail_sell_planned(const clspmv_cocktail_handle* h);
 /* Kernel of the CSR part under the per-part schedule: 0 (default) nonzero
  * chunks, or CSR-vector with `lanes` (1, 2, 4, 8, 16 or 32) lanes per row,
  * the reference's threads-per-row knob (its CSR-vector driver sweeps the

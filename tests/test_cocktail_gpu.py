@@ -358,3 +358,65 @@ def test_cocktail_flat_part_as_csr(setup, cfg, mname):
     torch.cuda.synchronize()
     y_ref, _, bound = reference_y(coo, x, y0, 1.0, 1.0)
     assert_close(yd.cpu().numpy(), y_ref, bound, f"flat as csr {cfg}/{mname} parts={dev.parts}")
+
+
+def _cocktail_of(pieces, converters, n, seed=8):
+    """CocktailMatrix whose slots hold the given (row, col) key sets
+    (key = row * n + col), converted by `converters`; and the whole matrix."""
+    from clspmv_mic_b200 import _abi
+    rng = np.random.default_rng(seed)
+    st = _abi.Cocktail()
+    st.mat_width = st.mat_height = n
+    keep = []
+    for sl, keys in pieces.items():
+        keys = np.sort(keys)
+        part_coo = F.coo_matrix(n, n, keys // n, keys % n, rng.standard_normal(keys.size).astype(np.float32))
+        host = converters[sl](part_coo)
+        keep.append((part_coo, host))
+        setattr(st, f"ifuse{sl}", True)
+        setattr(st, sl, type(getattr(st, sl)).from_buffer_copy(host.struct))
+    st.mat_nnz = int(sum(k.size for k in pieces.values()))
+    ck = CK.CocktailMatrix(st, owner=None)
+    ck._keep = keep
+    rows = np.concatenate([pc.array("coo_row_id") for pc, _ in keep])
+    cols = np.concatenate([pc.array("coo_col_id") for pc, _ in keep])
+    vals = np.concatenate([pc.array("coo_data") for pc, _ in keep])
+    o = np.lexsort((cols, rows))
+    return F.coo_matrix(n, n, rows[o], cols[o], vals[o]), ck
+
+
+@pytest.mark.parametrize("with_dia", [False, True])
+@pytest.mark.parametrize("sh", [32, 8])
+def test_cocktail_sell_part_planned(with_dia, sh):
+    """A SELL part of uneven rows (24 rows of 500-900 entries among rows of
+    0-3) runs through its length plan, made at upload, alone (its own y
+    update) and beside a DIA part (atomic adds into a y with beta applied
+    first), against the oracle; a SELL part of even rows keeps the padded
+    read."""
+    import torch
+    n = 4096
+    rng = np.random.default_rng(sh + with_dia)
+    r = np.arange(n)
+    band = np.unique(np.concatenate([r * n + r, r[1:] * n + r[1:] - 1, r[:-1] * n + r[:-1] + 1]))
+    keys = []
+    for row in rng.choice(n, 24, replace=False):
+        keys.append(row * n + rng.choice(n, int(rng.integers(500, 900)), replace=False))
+    keys.append(r * n + rng.integers(0, n, n))
+    sell = np.unique(np.concatenate(keys))
+    sell = sell[~np.isin(sell, band)]
+    pieces = {"dia": band, "sell": sell} if with_dia else {"sell": sell}
+    conv = {"dia": F.coo2dia, "sell": lambda c: F.coo2sell(c, sh)}
+    coo, ck = _cocktail_of(pieces, conv, n)
+    dev = ck.to_device()
+    assert dev.sell_planned
+    x = synth.x_vector(n)
+    y0 = np.random.default_rng(2).standard_normal(n).astype(np.float32)
+    for alpha, beta in [(1.0, 0.0), (1.5, -0.5)]:
+        xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y0.copy()).cuda()
+        dev.spmv(xd, yd, alpha, beta)
+        torch.cuda.synchronize()
+        y_ref, _, bound = reference_y(coo, x, y0, alpha, beta)
+        assert_close(yd.cpu().numpy(), y_ref, bound, f"sell{sh} planned, dia={with_dia}")
+    even = np.unique(r * n + (r * 7) % n)
+    _, ck2 = _cocktail_of({"sell": even}, conv, n)
+    assert not ck2.to_device().sell_planned
