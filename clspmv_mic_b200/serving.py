@@ -64,8 +64,7 @@ class Request:
     alpha: float
     future: Future
     t_submit: float
-    ready: object = None          # CUDA event recorded after X was produced
-    stream: int = 0               # the stream `ready` was recorded on
+    stream: object = None         # the stream X was produced on (current at submission)
     t_done: float = 0.0
     nbytes: int = 0               # X and Y bytes the request holds on the device
     keep: bool = True             # False: the future resolves to None
@@ -171,16 +170,13 @@ class SpmvServer:
             raise KeyError(name)
         if X.dim() == 1:
             X = X.view(-1, 1)
-        ev = torch.cuda.Event()
         src = torch.cuda.current_stream(X.device)
         f: Future = Future()
         m, n = self.mats[name].matrix.shape
-        req = Request(name, X, alpha, f, time.perf_counter(), ev, stream=src.cuda_stream,
+        req = Request(name, X, alpha, f, time.perf_counter(), stream=src,
                       nbytes=4 * X.shape[1] * (m + n), keep=keep_result)
         f.request = req     # submission / completion times for latency_stats
         with self._cv:
-            # recorded under the lock: on each stream, queue order is record order
-            ev.record(src)
             self._pending.append(req)
             self._cv.notify()
         return f
@@ -238,12 +234,15 @@ class SpmvServer:
         for r in reqs:
             groups.setdefault(r.name, []).append(r)
         jobs, order, outputs = [], [], []
-        # one wait per source stream: the latest request's event there covers
-        # every earlier one (events of one stream complete in order)
-        latest = {}
+        # one wait per source stream: an event recorded there now follows the
+        # production of every X of this batch made on it (each was queued
+        # before its submission), so no event is made per request
+        sources = {}
         for r in reqs:
-            latest[r.stream] = r.ready
-        for ev in latest.values():
+            sources[(r.stream.device, r.stream.cuda_stream)] = r.stream
+        for src in sources.values():
+            ev = torch.cuda.Event()
+            ev.record(src)
             st.wait_event(ev)
         with torch.cuda.stream(st):
             for name, rs in groups.items():
